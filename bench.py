@@ -1,0 +1,418 @@
+#!/usr/bin/env python3
+"""Transform throughput of the B200 covering engine on its headline cell.
+
+A STEP is the three whole-space transforms of one cell — recount (code ->
+cnt), gain map and loss map — through the plugin ABI.  The headline cell is
+binary Hamming n=26, R=3 (|X| = 67.1M, the larger of the two large
+single-instance cells; 20,830 seeded codewords, ~60% coverage); ternary
+n=16, R=4 is measured after it and reported under "also".
+
+value : model GB/s (the one-axis-per-pass byte model, the same for every
+        implementation, coldcore_b200.metrics) with the code resident on
+        the device; CUDA events on the engine's stream; inputs (1.07 GB of
+        layers) are larger than the 126 MB L2.
+e2e   : the same metric through the public C-ABI with host buffers: every
+        step uploads the code from host memory (dct_set_code) and reads
+        three scalars back (uncovered count, two map maxima).
+roofline : the dominant launch: its algorithmic bytes (cnt / layers read,
+        layers / map / cnt written, from the engine's own launch plan) over
+        its mean CUDA-event duration, against the measured HBM copy peak.
+cpu_baseline : the C restatement of the reference's CPU axis DP on every
+        host thread (oracle/cport), a bounded sample of the same cell.
+
+--impl reference runs that CPU restatement alone (rank 0), on the same
+cell, metric and unit: each step one transform of the cell, rotating
+recount / gain / loss.
+
+Multi-GPU (torchrun): every rank runs its own replica of the cell (the
+transform does not shard into independent pieces without an exchange
+step); value is the sum over ranks of the model bytes over the max time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from coldcore_b200.metrics import model_bytes          # noqa: E402
+from coldcore_b200.workloads import CELLS, code_for     # noqa: E402
+
+METRIC = ("transform GB/s vs HBM peak; LNS time-to-verified-size learned "
+          "vs plain, 1 B200")
+HEADLINE = "H2_26_3"
+ALSO = "H3_16_4"
+
+
+def step_model_bytes(cell):
+    ax, R, p = list(cell.axes), cell.R, cell.problem
+    return (model_bytes(ax, R, p, "recount") + model_bytes(ax, R, p, "gain")
+            + model_bytes(ax, R, p, "loss"))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """Per-launch DRAM bytes from a committed ncu summary, if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- dist
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(
+                seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap")
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU arm
+def cpu_sample(cell, modes, code):
+    """Model GB/s of the C restatement over the given transforms."""
+    from oracle.cport import CPortCell
+    c = CPortCell(list(cell.axes), cell.R, cell.problem)
+    c.recount(code)
+    by, t = 0, 0.0
+    for m in modes:
+        t0 = time.perf_counter()
+        if m == "recount":
+            c.recount(code)
+        elif m == "gain":
+            c.gain_map()
+        else:
+            c.loss_map()
+        t += time.perf_counter() - t0
+        by += model_bytes(list(cell.axes), cell.R, cell.problem, m)
+    return by / t / 1e9, t
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    cell = CELLS[args.cell]
+    code = code_for(cell)
+    from oracle.cport import CPortCell, build
+    build()
+    c = CPortCell(list(cell.axes), cell.R, cell.problem)
+    c.recount(code)
+    modes = ("recount", "gain", "loss")
+    fns = {"recount": lambda: c.recount(code), "gain": c.gain_map,
+           "loss": c.loss_map}
+    for i in range(args.warmup):
+        fns[modes[i % 3]]()
+    by, t = 0, 0.0
+    for i in range(args.steps):
+        m = modes[i % 3]
+        t0 = time.perf_counter()
+        fns[m]()
+        t += time.perf_counter() - t0
+        by += model_bytes(list(cell.axes), cell.R, cell.problem, m)
+    val = by / t / 1e9
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 3),
+        "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic",
+        "config": {"workload": cell.name, "axes": f"{cell.axes[0]}^"
+                   f"{len(cell.axes)}", "R": cell.R, "M": cell.M,
+                   "step": "one transform (recount / gain / loss, rotating)",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(val, 3), "unit": "GB/s",
+                         "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} transforms of {cell.name} "
+                                   "(C restatement, OpenMP, all threads)"},
+        "e2e": {"value": round(val, 3), "unit": "GB/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def measure_cell(cell, args, dist, timed=True):
+    import torch
+
+    from coldcore_b200.gpu import GpuBackend
+    code = code_for(cell)
+    b = GpuBackend(list(cell.axes), cell.R, problem=cell.problem)
+    stream = torch.cuda.ExternalStream(b.stream)
+    lib = b._lib
+    res = {}
+    try:
+        b._set_code(code)
+
+        def step():
+            if lib.dct_transform(0, 2) or lib.dct_transform(1, 1) or \
+                    lib.dct_transform(2, 1):
+                raise RuntimeError("transform failed")
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        clocks = Clocks(dist.local)
+        if timed:
+            clocks.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ms = dist.max(e0.elapsed_time(e1)) / args.steps
+        res["clocks"] = clocks.stop() if timed else None
+        res["ms"] = ms
+        res["value"] = step_model_bytes(cell) * dist.world / (ms * 1e-3) / 1e9
+        res["launches_per_step"] = sum(
+            len(b.plan(i, o)) for i, o in ((0, 2), (1, 1), (2, 1)))
+
+        # ---- e2e through the public API with host buffers
+        host_code = np.ascontiguousarray(code)
+
+        def step_e2e():
+            b.recount(host_code)
+            u = b.uncovered()
+            b.gain_map()
+            m1 = b.map_max()
+            b.loss_map()
+            m2 = b.map_max()
+            return u, m1, m2
+
+        for _ in range(max(1, args.warmup // 2)):
+            step_e2e()
+        torch.cuda.synchronize()
+        dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.steps):
+            step_e2e()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3 / args.steps
+        ms_e2e = dist.max(max(wall, f0.elapsed_time(f1) / args.steps))
+        res["e2e"] = {
+            "value": round(step_model_bytes(cell) * dist.world
+                           / (ms_e2e * 1e-3) / 1e9, 3),
+            "unit": "GB/s", "ms_per_step": round(ms_e2e, 4),
+            "h2d_bytes_per_step": int(code.nbytes),
+            "d2h_bytes_per_step": 24}
+
+        # ---- per-launch timing for the roofline (separate pass)
+        b.set_timing(True)
+        b._set_code(code)
+        per = {}
+        for _ in range(max(3, args.steps // 2)):
+            for (i, o) in ((0, 2), (1, 1), (2, 1)):
+                if lib.dct_transform(i, o):
+                    raise RuntimeError("transform failed")
+                plan = b.plan(i, o)
+                for k, t in enumerate(b.last_timings()):
+                    per.setdefault((i, o, k), []).append(t)
+        b.set_timing(False)
+        rows = []
+        for (i, o, k), ts in per.items():
+            plan = b.plan(i, o)
+            j0, nax, by, kid = (int(v) for v in plan[k])
+            mean = sum(ts) / len(ts)
+            rows.append({"transform": f"({i},{o})", "launch": k,
+                         "axes": f"{j0}..{j0 + nax - 1}", "kernel_id": kid,
+                         "bytes": by, "ms": mean,
+                         "GBps": by / (mean * 1e-3) / 1e9})
+        res["launches"] = rows
+        return res
+    finally:
+        b.close()
+
+
+def run_b200(args, dist):
+    cell = CELLS[args.cell]
+    res = measure_cell(cell, args, dist)
+    also = None
+    if not args.no_also and args.cell == HEADLINE:
+        r2 = measure_cell(CELLS[ALSO], args, dist, timed=False)
+        also = {"workload": ALSO, "value": round(r2["value"], 1),
+                "ms_per_step": round(r2["ms"], 4),
+                "e2e": r2["e2e"]["value"]}
+    if dist.rank != 0:
+        return
+    peak, peak_kind = peaks()
+    rows = res["launches"]
+    total = sum(r["ms"] for r in rows)
+    dom = max(rows, key=lambda r: r["ms"])
+    ach = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
+    tkey = f"{cell.name}:{dom['transform']}:{dom['launch']}"
+    traffic = ncu_traffic(tkey)
+    cpu = None
+    if dist.world == 1 and not args.no_cpu:
+        code = code_for(cell)
+        val, secs = cpu_sample(cell, ("recount", "gain", "loss"), code)
+        cpu = {"value": round(val, 3), "unit": "GB/s",
+               "cores": os.cpu_count(), "kind": "port",
+               "sample": f"one step (recount + gain + loss) of {cell.name}, "
+                         f"{secs:.1f} s, C restatement on all host threads"}
+    line = {
+        "metric": METRIC, "value": round(res["value"], 1), "unit": "GB/s",
+        "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(res["ms"], 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {
+            "workload": cell.name, "axes": f"{cell.axes[0]}^{len(cell.axes)}",
+            "R": cell.R, "M": cell.M, "seed": cell.seed,
+            "step": "recount + gain map + loss map",
+            "bytes_model": "one axis per pass (per-step model bytes "
+                           f"{step_model_bytes(cell)})",
+            "l2": "inputs larger than L2 (layers "
+                  f"{(cell.R + 1) * cell.size * 4 / 1e9:.2f} GB)",
+            "parallelism": f"replicas x{dist.world}",
+            "launch_GBps": {f"{r['transform']}#{r['launch']}":
+                            round(r["GBps"], 1) for r in rows},
+            "launch_ms": {f"{r['transform']}#{r['launch']}":
+                          round(r["ms"], 4) for r in rows},
+        },
+        "clocks": res["clocks"],
+        "e2e": res["e2e"],
+        "gpu_launches": res["launches_per_step"] * args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(ach, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(ach / peak, 4), "peak_kind": peak_kind,
+                     "kernel": f"{dom['transform']} launch {dom['launch']} "
+                               f"(axes {dom['axes']}, kernel id "
+                               f"{dom['kernel_id']})",
+                     "share": round(dom["ms"] / total, 3),
+                     "algorithmic_bytes": dom["bytes"],
+                     "traffic": traffic},
+        "cpu_baseline": cpu,
+    }
+    if also:
+        line["also"] = also
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--cell", default=HEADLINE, choices=sorted(CELLS))
+    ap.add_argument("--no-also", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        # host-only arm: rank 0 measures, the other ranks exit without work
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_reference(args, type("D", (), {"rank": 0})())
+        return
+    dist = Dist()
+    try:
+        run_b200(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

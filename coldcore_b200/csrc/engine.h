@@ -1,0 +1,139 @@
+// engine.h — internal state and launch interfaces of the B200 covering engine.
+//
+// One process-wide cell (the plugin ABI v1 singleton model, coldcore
+// src/include/coldcore/plugin.h:8-10).  Every kernel takes its geometry by
+// value (no __constant__ state shared between translation units), and every
+// launch goes to the engine's own stream, so device work runs in call order.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+namespace cc {
+
+constexpr int kMaxAxes = 40;      // |X| <= 2^40 with every axis >= 2
+constexpr int kMaxLayers = 8;     // R + 1 distance layers (R <= 7)
+constexpr int kMaxSlots = 8;      // changed positions per support pattern
+constexpr int kPlaneAlign = 64;   // plane stride rounded to 64 elements
+
+// problem ids: coldcore src/include/coldcore/plugin.h:45-53
+enum Problem { kHamming = 0, kTorus = 1, kLee = 2, kGrid = 3 };
+
+// cnt predicates (coldcore src/plugins/covering/dctcore_mu.cuh:28-40)
+enum Pred { kPredEq = 0, kPredDef = 1, kPredCrit = 2, kPredIdent = 3 };
+
+struct Geometry {
+  int prob, n, R, mu;
+  long long space;
+  int ax[kMaxAxes];
+  long long pw[kMaxAxes + 1];
+};
+
+__host__ __device__ inline bool cnt_pred(int mode, int c, int target, int mu) {
+  if (mode == kPredDef) return c < mu;
+  if (mode == kPredCrit) return c >= 1 && c <= mu;
+  return c == target;
+}
+
+// ------------------------------------------------------------ transform plan
+// One kernel launch covers a GROUP of consecutive axes [j0, j0+k).  The
+// group's words factor as x = o*(inner*mid) + m*inner + i with
+// inner = pw[j0], mid = prod of the group's axes; a tile is W consecutive
+// inner positions x mid x Bo consecutive outer slabs, staged in shared
+// memory.  Rounds process `rb` axes each in registers (local stride rs in m).
+constexpr int kMaxRounds = 24;
+constexpr int kGroupThreads = 512;   // CTA size cap: 128 registers per thread
+
+enum Src { kSrcLayers = 0, kSrcCnt = 1, kSrcCode = 2 };
+enum Dst { kDstLayers = 0, kDstMap = 1, kDstCnt = 2 };
+
+struct GroupArgs {
+  int32_t *layers;        // plane 0 base; plane d at layers + d*plane
+  long long plane;        // plane stride (elements)
+  uint16_t *cnt;
+  const long long *code;  // sorted code (kSrcCode)
+  long long ncode;
+  long long inner, outer, ntiles, nchunk;
+  int mid, W, Bo, k;
+  int nrounds;
+  int rb[kMaxRounds];     // axes per round
+  int rs[kMaxRounds];     // local stride (in m) of the round's first axis
+  int rq[kMaxRounds];     // axis size of the round (all axes of a round equal)
+  int qax[kMaxRounds];    // per-axis size inside the group (generic kernel)
+  int src, dst, lin, lout;
+  int pmode, ptarget, mu, R;
+  int skew;               // log2 of the shared-memory skew period (0 = none)
+  int prob;
+};
+
+struct GroupPlan {
+  GroupArgs a;
+  int kernel;             // index into the launcher table
+  int threads;
+  size_t smem;
+  int grid;
+};
+
+// launchers (transform_*.cu)
+int launch_group(const GroupPlan &p, cudaStream_t s);
+size_t group_smem_bytes(const GroupArgs &a, int R1);
+int pick_group_kernel(int prob, int q, int R1, int *bm);
+
+// window pass (torus / grid) over one axis, any width, out of place
+struct WindowArgs {
+  const int32_t *src32; const uint16_t *src16; int pmode, ptarget, mu;
+  int32_t *dst32; uint16_t *dst16;
+  long long space, stride; int q, R, grid;
+};
+int launch_window(const WindowArgs &w, cudaStream_t s);
+
+// ------------------------------------------------------------ walks
+// Support table in structure-of-arrays form: slot s of pattern t is
+// tbl[s*len + t] = (pos << 24) | delta, delta a circular shift in
+// 1..ax_pos-1; 0 = unused slot.  Entry 0 is the centre.
+struct WalkArgs {
+  Geometry g;
+  const int32_t *tbl;
+  int slots;
+  long long len;
+  uint16_t *cnt;
+};
+constexpr int kParamWords = 1024;       // words passed by value per launch
+struct WordsParam { long long w[kParamWords]; };
+
+// nb words from `dwords` (device) or, when dwords == nullptr, from `pw`
+int launch_update(const WalkArgs &w, const long long *dwords,
+                  const WordsParam *pw, int nb, int delta,
+                  unsigned long long *trans, cudaStream_t s);
+int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
+                  int mode, int target, int32_t *out, bool zeroed,
+                  cudaStream_t s);
+int pick_split(long long len, int nb);
+
+// ------------------------------------------------------------ reductions
+int launch_cnt_reduce(const uint16_t *cnt, long long N, int mode, int target,
+                      int mu, long long *out, cudaStream_t s);
+int launch_max(const int32_t *A, long long N, long long *out, cudaStream_t s);
+int launch_hist(const int32_t *A, long long N, int nbins, int32_t vmax,
+                int32_t *hist, cudaStream_t s);
+int launch_extract(const int32_t *A, long long N, int32_t thr, void *oidx,
+                   bool wide, int32_t *oval, long long cap, long long *ocount,
+                   cudaStream_t s);
+int launch_read_at(const int32_t *A, const long long *idx, int k,
+                   int32_t *out, cudaStream_t s);
+int launch_scatter(int32_t *A, const long long *idx, long long M,
+                   cudaStream_t s);
+
+int sm_count();
+
+}  // namespace cc
+
+#define CC_CK(x)                                                            \
+  do {                                                                      \
+    cudaError_t e_ = (x);                                                   \
+    if (e_ != cudaSuccess) {                                                \
+      fprintf(stderr, "coldcore_b200: CUDA error %s at %s:%d\n",            \
+              cudaGetErrorString(e_), __FILE__, __LINE__);                  \
+      return -(100 + (int)e_);                                              \
+    }                                                                       \
+  } while (0)

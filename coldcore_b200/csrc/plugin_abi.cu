@@ -1,0 +1,1102 @@
+// plugin_abi.cu — the extern "C" plugin ABI v1 of the B200 covering engine.
+//
+// Host side of every entry point declared in include/coldcore_b200/plugin.h:
+// validation before any mutation, the represented multisets (uploaded /
+// active, coldcore src/plugins/covering/dct_hc.cu:46-56), staging through
+// pinned buffers, the transform planner, and the result copies.  Semantics
+// follow the reference entry points cited per function; the device work is
+// this engine's own (transform_group.cu, transform_window.cu, walks.cu,
+// reduce.cu) and runs in call order on one engine-owned stream.
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/coldcore_b200/plugin.h"
+#include "engine.h"
+
+namespace cc {
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+}  // namespace cc
+
+using namespace cc;
+
+namespace {
+
+constexpr long long kCounterMax = 65535;    // uint16 cnt
+constexpr long long kStageCap = 1 << 16;    // words per staged chunk
+
+struct Plan {
+  std::vector<GroupPlan> groups;   // layered / small-axis path
+  std::vector<WindowArgs> passes;  // wide window path
+  bool window = false;
+  int scatter_plane = -1;          // window recount: plane of the code counts
+};
+
+struct State {
+  bool live = false;
+  Geometry g{};
+  int R1 = 1;                      // planes the transform math uses
+  int nplanes = 0;                 // planes allocated
+  long long plane = 0;
+  int32_t *layers = nullptr;
+  uint16_t *cnt = nullptr;
+  long long cnt_len = 0;
+  uint32_t *owner = nullptr;
+  int use_owner = 0;
+  int layers_mode = 0, cnt_mode = 0;
+  // support tables, SoA slots
+  int32_t *tbl = nullptr, *tbl2 = nullptr;
+  int slots = 0, slots2 = 0;
+  long long len = 0;
+  int fmt = 0;
+  // code
+  long long *d_code = nullptr;
+  long long code_cap = 0, codeM = 0;
+  // staging
+  long long *h_words = nullptr, *d_words = nullptr;
+  int32_t *h_out = nullptr, *d_out = nullptr;
+  long long *h_scalar = nullptr, *d_scalar = nullptr;
+  int32_t *d_hist = nullptr;
+  uint32_t *d_ext32 = nullptr;
+  int64_t *d_ext64 = nullptr;
+  int32_t *d_extv = nullptr;
+  long long extract_cap = 0;
+  // multisets (coldcore dct_hc.cu:46-56) + max multiplicity of `active`
+  std::unordered_map<long long, int> uploaded, active;
+  long long active_size = 0;
+  int up_max = 0;
+  std::vector<int> mult_hist;      // distinct active words per multiplicity
+  int act_max = 0;
+  long long stats[8] = {0};
+  long long bytes_dev = 0, bytes_host = 0;
+  unsigned long long dd_last = 0;
+  bool layered_out = false;        // last transform left N_0..N_R
+  Plan plans[3][4];                // [init_mode][out_mode]
+  bool plan_ok[3][4] = {{false}};
+};
+
+State S;
+cudaStream_t g_stream = nullptr;
+int g_mu = 1;
+
+// per-launch device timing of the last transform (DCT_TIMING=1 in the
+// environment at load, or dct_b200_set_timing(1)): events around every
+// launch, read after the transform's final synchronisation
+constexpr int kMaxTimed = 64;
+int g_timing = -1;
+cudaEvent_t g_ev[kMaxTimed + 1];
+float g_last_ms[kMaxTimed];
+int g_last_n = 0;
+
+bool timing_on() {
+  if (g_timing < 0) g_timing = getenv("DCT_TIMING") ? 1 : 0;
+  return g_timing == 1;
+}
+
+int timing_mark(int i) {
+  if (!timing_on() || i > kMaxTimed) return 0;
+  if (!g_ev[i]) CC_CK(cudaEventCreate(&g_ev[i]));
+  CC_CK(cudaEventRecord(g_ev[i], g_stream));
+  return 0;
+}
+
+long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+int dev_alloc(void **p, size_t bytes, int mode) {
+  cudaError_t e;
+  if (mode == 0) {
+    e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) S.bytes_dev += bytes;
+  } else {
+    // the reference's LPDDR / managed placements (dct_hc.cu alloc_buf):
+    // a B200 host has no coherent C2C memory, so both map to managed
+    // memory that the driver pages in on demand
+    e = cudaMallocManaged(p, bytes);
+    if (e == cudaSuccess) S.bytes_host += bytes;
+  }
+  if (e != cudaSuccess) {
+    fprintf(stderr, "coldcore_b200: allocation of %zu bytes failed: %s\n",
+            bytes, cudaGetErrorString(e));
+    *p = nullptr;
+    return -1;
+  }
+  return 0;
+}
+
+bool valid_words(const long long *w, long long n) {
+  if (n < 0 || (n && !w)) return false;
+  for (long long i = 0; i < n; i++)
+    if (w[i] < 0 || w[i] >= S.g.space) return false;
+  return true;
+}
+
+// exact uint16 bound: no counter can exceed min(total, maxmult * |B|)
+bool within_counter(long long total, long long maxmult) {
+  long long b = maxmult * S.len;
+  if (b > total) b = total;
+  return b <= kCounterMax;
+}
+
+void hist_move(int from, int to) {
+  if (from > 0) S.mult_hist[from]--;
+  if (to > 0) S.mult_hist[to]++;
+  if (to > S.act_max) S.act_max = to;
+  while (S.act_max > 0 && S.mult_hist[S.act_max] == 0) S.act_max--;
+}
+
+void set_active(const std::unordered_map<long long, int> &m, long long sz) {
+  S.active = m;
+  S.active_size = sz;
+  std::fill(S.mult_hist.begin(), S.mult_hist.end(), 0);
+  S.act_max = 0;
+  for (const auto &e : m) {
+    S.mult_hist[e.second]++;
+    if (e.second > S.act_max) S.act_max = e.second;
+  }
+}
+
+void apply_active(const std::unordered_map<long long, int> &batch,
+                  int delta, long long nw) {
+  for (const auto &e : batch) {
+    int &c = S.active[e.first];
+    const int before = c;
+    c += delta * e.second;
+    hist_move(before, c);
+    if (c == 0) S.active.erase(e.first);
+  }
+  S.active_size += delta * nw;
+}
+
+// validate an update batch against `active`; fills `batch`
+int check_update(const long long *words, int nw, int delta,
+                 std::unordered_map<long long, int> &batch) {
+  if (!valid_words(words, nw) || (delta != 1 && delta != -1)) return -1;
+  batch.reserve((size_t)nw * 2 + 1);
+  for (int i = 0; i < nw; i++) ++batch[words[i]];
+  if (delta == -1) {
+    for (const auto &e : batch) {
+      auto it = S.active.find(e.first);
+      if (it == S.active.end() || it->second < e.second) return -1;
+    }
+  } else {
+    long long mx = S.act_max;
+    for (const auto &e : batch) {
+      auto it = S.active.find(e.first);
+      long long m = (it == S.active.end() ? 0 : it->second) + e.second;
+      if (m > mx) mx = m;
+    }
+    if (!within_counter(S.active_size + nw, mx)) return -1;
+  }
+  return 0;
+}
+
+int fetch_scalar(long long *r, int slot = 0) {
+  CC_CK(cudaMemcpyAsync(S.h_scalar + slot, S.d_scalar + slot, 8,
+                        cudaMemcpyDeviceToHost, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));
+  *r = S.h_scalar[slot];
+  return 0;
+}
+
+int stage_words(const long long *words, long long nb) {
+  memcpy(S.h_words, words, (size_t)nb * 8);
+  CC_CK(cudaMemcpyAsync(S.d_words, S.h_words, (size_t)nb * 8,
+                        cudaMemcpyHostToDevice, g_stream));
+  return 0;
+}
+
+WalkArgs walk_args() {
+  WalkArgs w;
+  w.g = S.g;
+  w.g.mu = g_mu;
+  const bool ox = S.fmt == 1 && S.tbl2;
+  w.tbl = ox ? S.tbl2 : S.tbl;
+  w.slots = ox ? S.slots2 : S.slots;
+  w.len = S.len;
+  w.cnt = S.cnt;
+  return w;
+}
+
+void free_all() {
+  if (g_stream) cudaStreamSynchronize(g_stream);
+  auto F = [](void *p) { if (p) cudaFree(p); };
+  auto FH = [](void *p) { if (p) cudaFreeHost(p); };
+  F(S.layers); F(S.cnt); F(S.owner); F(S.tbl); F(S.tbl2); F(S.d_code);
+  F(S.d_words); F(S.d_out); F(S.d_scalar); F(S.d_hist); F(S.d_ext32);
+  F(S.d_ext64); F(S.d_extv);
+  FH(S.h_words); FH(S.h_out); FH(S.h_scalar);
+  S.~State();
+  new (&S) State();
+}
+
+// ------------------------------------------------------------ planner
+// shared-memory budget of one tile (CC_SMEM_BUDGET_KB overrides; read
+// whenever a plan is built, i.e. once per cell and transform kind)
+size_t smem_budget() {
+  const char *e = getenv("CC_SMEM_BUDGET_KB");
+  long long b = e ? atoll(e) * 1024 : 100 * 1024;
+  if (b < 16 * 1024) b = 16 * 1024;
+  if (b > 220 * 1024) b = 220 * 1024;
+  return (size_t)b;
+}
+
+int ipow(int q, int e) { int r = 1; while (e-- > 0) r *= q; return r; }
+
+void set_rounds(GroupArgs &a, int q, int bm) {
+  const int nr = (a.k + bm - 1) / bm;
+  std::vector<int> rb(nr), rs(nr);
+  for (int r = 0; r < nr; r++) {
+    rb[r] = std::min(bm, a.k - r * bm);
+    rs[r] = ipow(q, r * bm);
+  }
+  std::vector<int> order(nr);
+  for (int r = 0; r < nr; r++) order[r] = r;
+  if (a.W == 1 && nr >= 3) {
+    // HBM-facing rounds get the widest strides (coalesced lanes): the
+    // widest round stores every layer, the second widest loads the
+    // 2-byte cnt, the rest exchange through shared memory in between
+    order.clear();
+    order.push_back(nr - 2);
+    for (int r = 0; r < nr - 2; r++) order.push_back(r);
+    order.push_back(nr - 1);
+  }
+  a.nrounds = nr;
+  for (int i = 0; i < nr; i++) {
+    a.rb[i] = rb[order[i]];
+    a.rs[i] = rs[order[i]];
+    a.rq[i] = q;
+  }
+}
+
+int threads_for(const GroupArgs &a, int kid, int bm, int q) {
+  int t;
+  if (kid >= 0) {
+    const long long words = (long long)a.W * a.mid * a.Bo;
+    const int ne = ipow(q, std::min(bm, a.k));
+    t = (int)std::min<long long>(kGroupThreads, words / ne);
+  } else {
+    t = (int)std::min<long long>(256, (long long)a.W * a.mid * a.Bo);
+  }
+  t = (t + 31) / 32 * 32;
+  return t < 32 ? 32 : t;
+}
+
+int occupancy_grid(const GroupPlan &p) {
+  // persistent: as many CTAs as fit, capped by the tile count
+  int per_sm = 1;
+  const size_t budget_sm = 228 * 1024;
+  per_sm = (int)std::max<size_t>(1, budget_sm / (p.smem + 1024));
+  const int by_threads = 2048 / p.threads;
+  if (per_sm > by_threads) per_sm = by_threads;
+  if (per_sm < 1) per_sm = 1;
+  long long grid = (long long)sm_count() * per_sm;
+  if (grid > p.a.ntiles) grid = p.a.ntiles;
+  return (int)std::max<long long>(1, grid);
+}
+
+Plan build_group_plan(int src, int dst) {
+  Plan P;
+  const Geometry &g = S.g;
+  const int R1 = S.R1;
+  const bool layered = R1 > 1;
+  const size_t budget = smem_budget();
+  int j = 0;
+  while (j < g.n) {
+    const int q = g.ax[j];
+    int bm = 1;
+    const int kid = pick_group_kernel(g.prob, q, R1, &bm);
+    GroupArgs a{};
+    a.layers = S.layers;
+    a.plane = S.plane;
+    a.cnt = S.cnt;
+    a.code = S.d_code;
+    a.ncode = S.codeM;
+    a.inner = g.pw[j];
+    a.W = a.inner >= 32 ? 32 : (int)a.inner;
+    a.prob = g.prob;
+    a.R = g.R;
+    a.mu = g_mu;
+    int k = 0;
+    long long mid = 1;
+    for (;;) {
+      if (j + k >= g.n || k >= kMaxRounds) break;
+      const int qn = g.ax[j + k];
+      if (kid >= 0 && qn != q) break;
+      if (kid < 0 && qn > 16) break;
+      const long long mid2 = mid * qn;
+      GroupArgs t = a;
+      t.k = k + 1;
+      t.mid = (int)std::min<long long>(mid2, INT_MAX / 64);
+      const long long outer = g.space / (a.inner * mid2);
+      t.Bo = a.W >= 32 ? 1
+             : (int)std::max<long long>(1, std::min<long long>(
+                   outer, 2048 / (a.W * mid2)));
+      t.skew = 0;
+      if (kid >= 0 && a.W == 1 && (q & (q - 1)) == 0) {
+        int lg = 0;
+        while ((1 << lg) < ipow(q, bm)) lg++;
+        t.skew = lg;
+      }
+      const size_t sm = group_smem_bytes(t, R1);
+      const int th = threads_for(t, kid, bm, q);
+      const long long words = (long long)t.W * t.mid * t.Bo;
+      const bool fits = sm <= budget && mid2 < (1 << 24) &&
+                        (kid < 0 ||
+                         words / ipow(q, std::min(bm, t.k)) <= kGroupThreads);
+      if (k > 0 && !fits) break;
+      a.k = t.k; a.mid = t.mid; a.Bo = t.Bo; a.skew = t.skew;
+      (void)th;
+      mid = mid2;
+      k++;
+    }
+    a.outer = g.space / (a.inner * (long long)a.mid);
+    a.nchunk = (a.inner + a.W - 1) / a.W;
+    a.ntiles = (a.outer + a.Bo - 1) / a.Bo * a.nchunk;
+    for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j + t];
+    if (kid >= 0) set_rounds(a, q, bm);
+    else a.nrounds = 0;
+    const bool first = j == 0, last = j + a.k == g.n;
+    a.src = first ? src : kSrcLayers;
+    a.dst = last ? dst : kDstLayers;
+    a.lin = layered ? std::min(j, g.R) + 1 : 1;
+    a.lout = layered ? std::min(j + a.k, g.R) + 1 : 1;
+    if (last && dst == kDstLayers) a.lout = R1;   // every layer, zeros too
+    a.pmode = kPredEq;
+    a.ptarget = 0;
+    GroupPlan p;
+    p.a = a;
+    p.kernel = kid;
+    p.smem = group_smem_bytes(a, R1);
+    p.threads = threads_for(a, kid, bm, q);
+    p.grid = occupancy_grid(p);
+    P.groups.push_back(p);
+    j += a.k;
+  }
+  return P;
+}
+
+bool any_wide_axis() {
+  for (int j = 0; j < S.g.n; j++)
+    if (S.g.ax[j] > 16) return true;
+  return false;
+}
+
+// window path: pass j reads buf[j] and writes buf[j+1]; buffers are planes
+// 0..2, kSrc from cnt (-1) or a plane, the last one the map / cnt (-2)
+Plan build_window_plan(int init_mode, int out_mode) {
+  Plan P;
+  P.window = true;
+  const Geometry &g = S.g;
+  const int n = g.n;
+  std::vector<int> buf(n + 1);
+  buf[0] = init_mode == 0 ? 2 : -1;
+  P.scatter_plane = init_mode == 0 ? 2 : -1;
+  buf[n] = out_mode == 2 ? -2 : 0;
+  for (int j = n - 1; j >= 1; j--) {
+    const int nxt = buf[j + 1];
+    int pick = 0;
+    while (pick == nxt || (j == 1 && pick == buf[0])) pick++;
+    buf[j] = pick;
+  }
+  for (int j = 0; j < n; j++) {
+    WindowArgs w{};
+    const int s = buf[j], d = buf[j + 1];
+    if (s == -1) w.src16 = S.cnt; else w.src32 = S.layers + s * S.plane;
+    if (d == -2) w.dst16 = S.cnt; else w.dst32 = S.layers + d * S.plane;
+    w.pmode = kPredEq;
+    w.mu = g_mu;
+    w.space = g.space;
+    w.stride = g.pw[j];
+    w.q = g.ax[j];
+    w.R = g.R;
+    w.grid = g.prob == kGrid;
+    P.passes.push_back(w);
+  }
+  return P;
+}
+
+Plan &plan_for(int init_mode, int out_mode) {
+  if (!S.plan_ok[init_mode][out_mode]) {
+    const int src = init_mode == 0 ? kSrcCode : kSrcCnt;
+    const int dst = out_mode == 1 ? kDstMap
+                    : out_mode == 2 ? kDstCnt : kDstLayers;
+    if ((S.g.prob == kTorus || S.g.prob == kGrid) && any_wide_axis())
+      S.plans[init_mode][out_mode] = build_window_plan(init_mode, out_mode);
+    else
+      S.plans[init_mode][out_mode] = build_group_plan(src, dst);
+    S.plan_ok[init_mode][out_mode] = true;
+  }
+  return S.plans[init_mode][out_mode];
+}
+
+void set_predicate(int init_mode, int *pm, int *pt) {
+  *pm = kPredEq;
+  *pt = 0;
+  if (init_mode == 1) {
+    if (g_mu == 1) *pt = 0; else *pm = kPredDef;
+  } else if (init_mode == 2) {
+    if (g_mu == 1) *pt = 1; else *pm = kPredCrit;
+  }
+}
+
+int run_transform(int init_mode, int out_mode) {
+  Plan &P = plan_for(init_mode, out_mode);
+  int pm, pt;
+  set_predicate(init_mode, &pm, &pt);
+  int nt = 0, rc = 0;
+  if (P.window) {
+    if (init_mode == 0) {
+      int32_t *pl = S.layers + P.scatter_plane * S.plane;
+      CC_CK(cudaMemsetAsync(pl, 0, (size_t)S.g.space * 4, g_stream));
+      rc = launch_scatter(pl, S.d_code, S.codeM, g_stream);
+      if (rc) return rc;
+    }
+    if ((rc = timing_mark(nt))) return rc;
+    for (auto &w : P.passes) {
+      WindowArgs x = w;
+      x.pmode = pm;
+      x.ptarget = pt;
+      x.mu = g_mu;
+      if ((rc = launch_window(x, g_stream))) return rc;
+      if ((rc = timing_mark(++nt))) return rc;
+    }
+  } else {
+    if ((rc = timing_mark(nt))) return rc;
+    for (auto &gp : P.groups) {
+      GroupPlan p = gp;
+      p.a.pmode = pm;
+      p.a.ptarget = pt;
+      p.a.mu = g_mu;
+      p.a.code = S.d_code;
+      p.a.ncode = S.codeM;
+      if ((rc = launch_group(p, g_stream))) return rc;
+      if ((rc = timing_mark(++nt))) return rc;
+    }
+  }
+  g_last_n = 0;
+  if (timing_on()) {
+    CC_CK(cudaStreamSynchronize(g_stream));
+    const int m = nt < kMaxTimed ? nt : kMaxTimed;
+    for (int i = 0; i < m; i++)
+      CC_CK(cudaEventElapsedTime(&g_last_ms[i], g_ev[i], g_ev[i + 1]));
+    g_last_n = m;
+    if (getenv("DCT_TIMING"))
+      for (int i = 0; i < m; i++)
+        fprintf(stderr, "DCT_TIMING transform(%d,%d) launch %d: %.4f ms\n",
+                init_mode, out_mode, i, g_last_ms[i]);
+  }
+  return 0;
+}
+
+int ensure_stream() {
+  if (!g_stream)
+    CC_CK(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
+  return 0;
+}
+
+// v1 packed table -> SoA slots; -1 on malformed entries
+int unpack_v1(const uint64_t *pat, long long len, std::vector<int32_t> &out,
+              int *slots) {
+  int w = 1;
+  for (long long t = 0; t < len; t++) {
+    int k = 0;
+    while (k < 8 && ((pat[t] >> (8 * k)) & 255u)) k++;
+    if (k > w) w = k;
+  }
+  out.assign((size_t)w * len, 0);
+  for (long long t = 0; t < len; t++) {
+    for (int k = 0; k < 8; k++) {
+      const unsigned b = (unsigned)(pat[t] >> (8 * k)) & 255u;
+      if (!b) break;
+      const int pos = (int)(b >> 4), dl = (int)(b & 15u);
+      if (pos >= S.g.n || dl < 1 || dl >= S.g.ax[pos]) return -1;
+      out[(size_t)k * len + t] = (pos << 24) | dl;
+    }
+  }
+  *slots = w;
+  return 0;
+}
+
+int init_common(int problem, int n, const int *ax, int R, long long len,
+                int extract_cap, int layers_mode, int cnt_mode,
+                int use_owner) {
+  if (n < 1 || n > kMaxAxes || R < 1 || !ax || len < 1 || len > INT_MAX ||
+      extract_cap < 1)
+    return -1;
+  const bool layered = problem == kHamming || problem == kLee;
+  if (problem < 0 || problem > 3) return -1;
+  if (layered && R + 1 > kMaxLayers) return -1;
+  for (int i = 0; i < n; i++) {
+    if (ax[i] < 2 || ax[i] >= (1 << 24)) return -1;
+    if (problem == kTorus && (ax[i] < 3 || 2 * R + 1 > ax[i])) return -1;
+  }
+  long long space = 1;
+  for (int i = 0; i < n; i++) {
+    if (space > (1LL << 40) / ax[i]) return -2;
+    space *= ax[i];
+  }
+  free_all();
+  int rc = ensure_stream();
+  if (rc) return rc;
+  S.g.prob = problem; S.g.n = n; S.g.R = R; S.g.mu = g_mu;
+  S.g.space = space;
+  S.g.pw[0] = 1;
+  for (int i = 0; i < n; i++) {
+    S.g.ax[i] = ax[i];
+    S.g.pw[i + 1] = S.g.pw[i] * ax[i];
+  }
+  S.R1 = layered ? R + 1 : 1;
+  S.nplanes = layered ? R + 1 : 3;
+  S.plane = round_up(space, kPlaneAlign);
+  S.layers_mode = layers_mode;
+  S.cnt_mode = cnt_mode;
+  S.use_owner = use_owner;
+  S.len = len;
+  if (dev_alloc((void **)&S.layers, (size_t)S.plane * S.nplanes * 4,
+                layers_mode)) { free_all(); return -3; }
+  S.cnt_len = round_up(space, kPlaneAlign);
+  if (dev_alloc((void **)&S.cnt, (size_t)S.cnt_len * 2, cnt_mode)) {
+    free_all(); return -4;
+  }
+  CC_CK(cudaMemsetAsync(S.cnt, 0, (size_t)S.cnt_len * 2, g_stream));
+  if (use_owner) {
+    if (dev_alloc((void **)&S.owner, (size_t)space * 4, cnt_mode)) {
+      free_all(); return -5;
+    }
+  }
+  CC_CK(cudaMalloc(&S.d_words, kStageCap * 8));
+  CC_CK(cudaMalloc(&S.d_out, kStageCap * 4));
+  CC_CK(cudaMalloc(&S.d_scalar, 64 * 8));
+  CC_CK(cudaMalloc(&S.d_hist, 4096 * 4));
+  CC_CK(cudaHostAlloc((void **)&S.h_words, kStageCap * 8,
+                      cudaHostAllocDefault));
+  CC_CK(cudaHostAlloc((void **)&S.h_out, kStageCap * 4,
+                      cudaHostAllocDefault));
+  CC_CK(cudaHostAlloc((void **)&S.h_scalar, 64 * 8, cudaHostAllocDefault));
+  CC_CK(cudaMemsetAsync(S.d_scalar, 0, 64 * 8, g_stream));
+  S.bytes_dev += kStageCap * 12 + 64 * 8 + 4096 * 4;
+  S.extract_cap = extract_cap;
+  CC_CK(cudaMalloc(&S.d_ext32, (size_t)extract_cap * 4));
+  CC_CK(cudaMalloc(&S.d_ext64, (size_t)extract_cap * 8));
+  CC_CK(cudaMalloc(&S.d_extv, (size_t)extract_cap * 4));
+  S.bytes_dev += (long long)extract_cap * 16;
+  S.mult_hist.assign(kCounterMax + 2, 0);
+  S.live = true;
+  return 0;
+}
+
+int upload_table(const std::vector<int32_t> &soa, int slots, int32_t **dst,
+                 int *dslots) {
+  CC_CK(cudaMalloc(dst, soa.size() * 4));
+  CC_CK(cudaMemcpyAsync(*dst, soa.data(), soa.size() * 4,
+                        cudaMemcpyHostToDevice, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));
+  S.bytes_dev += (long long)soa.size() * 4;
+  *dslots = slots;
+  return 0;
+}
+
+int finish_init(long long *bytes) {
+  CC_CK(cudaStreamSynchronize(g_stream));
+  if (bytes) *bytes = S.bytes_dev + S.bytes_host;
+  return 0;
+}
+
+int gather_impl(const long long *words, int nwords, int mode, int target,
+                int32_t *out) {
+  if (nwords <= 0) return 0;
+  if (!out || !valid_words(words, nwords)) return -1;
+  const WalkArgs w = walk_args();
+  for (long long off = 0; off < nwords; off += kStageCap) {
+    const int nb = (int)std::min<long long>(kStageCap, nwords - off);
+    int rc = stage_words(words + off, nb);
+    if (rc) return rc;
+    rc = launch_gather(w, S.d_words, nb, mode, target, S.d_out, false,
+                       g_stream);
+    if (rc) return rc;
+    S.stats[1]++;
+    CC_CK(cudaMemcpyAsync(S.h_out, S.d_out, (size_t)nb * 4,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    memcpy(out + off, S.h_out, (size_t)nb * 4);
+  }
+  return 0;
+}
+
+// cnt += delta over the balls of `words`; trans: running transition counter
+int update_impl(const long long *words, int nwords, int delta,
+                unsigned long long *trans) {
+  const WalkArgs w = walk_args();
+  for (long long off = 0; off < nwords; off += kStageCap) {
+    const int nb = (int)std::min<long long>(kStageCap, nwords - off);
+    int rc;
+    if (nb <= kParamWords) {
+      WordsParam p;
+      memcpy(p.w, words + off, (size_t)nb * 8);
+      rc = launch_update(w, nullptr, &p, nb, delta, trans, g_stream);
+      if (rc) return rc;
+    } else {
+      rc = stage_words(words + off, nb);
+      if (rc) return rc;
+      rc = launch_update(w, S.d_words, nullptr, nb, delta, trans, g_stream);
+      if (rc) return rc;
+      CC_CK(cudaStreamSynchronize(g_stream));   // staging buffer reused
+    }
+  }
+  return 0;
+}
+
+int mode_role(int role, int *mode, int *target) {
+  if (role == 0) { *mode = g_mu == 1 ? kPredEq : kPredDef; *target = 0; }
+  else { *mode = g_mu == 1 ? kPredEq : kPredCrit; *target = 1; }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+long long dct_host_bytes(void) { return S.bytes_host; }
+
+int dct_set_mu(int mu) {
+  if (mu < 1 || mu > 65535) return -1;
+  g_mu = mu;
+  S.g.mu = mu;
+  return 0;
+}
+
+int dct_get_mu(void) { return g_mu; }
+
+int dct_init3(int problem, int n, const int *ax, int R,
+              const uint64_t *ballpat, long long balllen, int extract_cap,
+              long long *bytes, int layers_mode, int cnt_mode,
+              int use_owner) {
+  if (!ballpat || !ax || n < 1 || n > kMaxAxes) return -1;
+  for (int i = 0; i < n; i++)
+    if (ax[i] < 2 || ax[i] > 16) return -1;      // v1 nibble format
+  if (layers_mode < 0 || layers_mode > 2 || cnt_mode < 0 || cnt_mode > 2)
+    return -1;
+  int rc = init_common(problem, n, ax, R, balllen, extract_cap, layers_mode,
+                       cnt_mode, use_owner);
+  if (rc) return rc;
+  std::vector<int32_t> soa;
+  int slots = 0;
+  if (unpack_v1(ballpat, balllen, soa, &slots)) { free_all(); return -1; }
+  rc = upload_table(soa, slots, &S.tbl, &S.slots);
+  if (rc) return rc;
+  return finish_init(bytes);
+}
+
+int dct_init3w(int problem, int n, const int *ax, int R, const int32_t *tbl,
+               int slots, long long len, int extract_cap, long long *bytes) {
+  if (!tbl || slots < 1 || slots > kMaxSlots) return -1;
+  int rc = init_common(problem, n, ax, R, len, extract_cap, 0, 0, 0);
+  if (rc) return rc;
+  std::vector<int32_t> soa((size_t)slots * len, 0);
+  for (long long t = 0; t < len; t++)
+    for (int k = 0; k < slots; k++) {
+      const int32_t c = tbl[t * slots + k];
+      if (!c) continue;
+      const int pos = c >> 24, dl = c & 0xFFFFFF;
+      if (pos < 0 || pos >= n || dl < 1 || dl >= ax[pos]) {
+        free_all();
+        return -1;
+      }
+      soa[(size_t)k * len + t] = c;
+    }
+  rc = upload_table(soa, slots, &S.tbl, &S.slots);
+  if (rc) return rc;
+  return finish_init(bytes);
+}
+
+int dct_init2(int q, int n, int R, const uint64_t *ballpat, long long balllen,
+              int extract_cap, long long *bytes, int layers_mode,
+              int cnt_mode, int use_owner) {
+  int ax[kMaxAxes];
+  if (n < 1 || n > kMaxAxes) return -1;
+  for (int i = 0; i < n; i++) ax[i] = q;
+  return dct_init3(kHamming, n, ax, R, ballpat, balllen, extract_cap, bytes,
+                   layers_mode, cnt_mode, use_owner);
+}
+
+int dct_init(int q, int n, int R, const uint64_t *ballpat, long long balllen,
+             int extract_cap, long long *bytes) {
+  return dct_init2(q, n, R, ballpat, balllen, extract_cap, bytes, 0, 0, 0);
+}
+
+int dct_free(void) {
+  free_all();
+  g_mu = 1;                       // singleton: mu never leaks into a new cell
+  return 0;
+}
+
+int dct_set_tbl2(const uint16_t *mask, const uint64_t *offs, long long len) {
+  if (!S.live || len != S.len || !mask || !offs) return -1;
+  int w = 1;
+  for (long long t = 0; t < len; t++) w = std::max(w, __builtin_popcount(mask[t]));
+  std::vector<int32_t> soa((size_t)w * len, 0);
+  for (long long t = 0; t < len; t++) {
+    unsigned m = mask[t];
+    int k = 0;
+    while (m) {
+      const int p = __builtin_ctz(m);
+      m &= m - 1;
+      const int dl = (int)((offs[t] >> (4 * p)) & 15u);
+      if (p >= S.g.n || dl < 1 || dl >= S.g.ax[p]) return -1;
+      soa[(size_t)k * len + t] = (p << 24) | dl;
+      k++;
+    }
+  }
+  if (S.tbl2) { cudaFree(S.tbl2); S.tbl2 = nullptr; }
+  return upload_table(soa, w, &S.tbl2, &S.slots2);
+}
+
+int dct_use_fmt(int fmt) {
+  if (fmt < 0 || fmt > 1) return -1;
+  if (fmt == 1 && !S.tbl2) return -1;
+  if (fmt == 1 && S.g.prob == kGrid) return -1;   // the ox walk is circulant
+  S.fmt = fmt;
+  return 0;
+}
+
+int dct_set_code(const long long *idx, int M) {
+  if (!S.live || !valid_words(idx, M)) return -1;
+  std::unordered_map<long long, int> up;
+  up.reserve((size_t)M * 2 + 1);
+  int mx = 0;
+  for (int i = 0; i < M; i++) mx = std::max(mx, ++up[idx[i]]);
+  if (!within_counter(M, mx)) return -1;
+  std::vector<long long> sorted(idx, idx + M);
+  std::sort(sorted.begin(), sorted.end());
+  if (M > S.code_cap) {
+    if (S.d_code) cudaFree(S.d_code);
+    S.d_code = nullptr;
+    const long long cap = std::max<long long>(M, 1024);
+    CC_CK(cudaMalloc(&S.d_code, (size_t)cap * 8));
+    S.code_cap = cap;
+  }
+  if (M) {
+    CC_CK(cudaMemcpyAsync(S.d_code, sorted.data(), (size_t)M * 8,
+                          cudaMemcpyHostToDevice, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+  }
+  S.codeM = M;
+  S.uploaded.swap(up);
+  S.up_max = mx;
+  return 0;
+}
+
+int dct_transform(int init_mode, int out_mode) {
+  if (!S.live) return -1;
+  if (init_mode < 0 || init_mode > 2 || out_mode < 1 || out_mode > 3 ||
+      (out_mode == 2 && init_mode != 0))
+    return -1;
+  if (out_mode == 3 && S.R1 == 1) return -1;
+  int rc = run_transform(init_mode, out_mode);
+  if (rc) return rc;
+  CC_CK(cudaStreamSynchronize(g_stream));
+  S.layered_out = out_mode == 3;
+  if (out_mode == 2) set_active(S.uploaded, S.codeM);
+  return 0;
+}
+
+int dct_ball_update(const long long *words, int nwords, int delta) {
+  if (!S.live) return -1;
+  std::unordered_map<long long, int> batch;
+  if (check_update(words, nwords, delta, batch)) return -1;
+  if (nwords == 0) return 0;
+  int rc = update_impl(words, nwords, delta, nullptr);
+  if (rc) return rc;
+  apply_active(batch, delta, nwords);
+  return 0;
+}
+
+int dct_ball_update_delta(const long long *words, int nwords, int delta,
+                          long long *dd) {
+  if (!dd) return -1;
+  *dd = 0;
+  if (!S.live) return -1;
+  std::unordered_map<long long, int> batch;
+  if (check_update(words, nwords, delta, batch)) return -1;
+  if (nwords == 0) return 0;
+  auto *trans = reinterpret_cast<unsigned long long *>(S.d_scalar + 2);
+  int rc = update_impl(words, nwords, delta, trans);
+  if (rc) return rc;
+  long long now;
+  rc = fetch_scalar(&now, 2);
+  if (rc) return rc;
+  const long long tr = (long long)((unsigned long long)now - S.dd_last);
+  S.dd_last = (unsigned long long)now;
+  *dd = delta > 0 ? -tr : tr;
+  apply_active(batch, delta, nwords);
+  return 0;
+}
+
+int dct_ball_gather(const long long *words, int nwords, int target,
+                    int32_t *out) {
+  if (!S.live) return -1;
+  return gather_impl(words, nwords, kPredEq, target, out);
+}
+
+int dct_ball_gather_mu(const long long *words, int nwords, int role,
+                       int32_t *out) {
+  if (!S.live) return -1;
+  if (nwords <= 0) return 0;
+  if (role < 0 || role > 1) return -1;
+  return gather_impl(words, nwords, role == 0 ? kPredDef : kPredCrit, 0, out);
+}
+
+int dct_swap_eval(const long long *drops, int k, const long long *cand,
+                  const long long *off, int32_t *gain, int32_t *loss) {
+  if (!S.live) return -1;
+  if (k <= 0) return 0;
+  if (k > 65535 || !off || off[0] != 0 || !drops || !loss) return -1;
+  for (int i = 0; i < k; i++)
+    if (off[i + 1] < off[i]) return -1;
+  const long long nc = off[k];
+  if (nc > 65535 || (nc && (!cand || !gain))) return -1;
+  if (!valid_words(drops, k) || !valid_words(cand, nc)) return -1;
+  for (int i = 0; i < k; i++)
+    if (S.active.find(drops[i]) == S.active.end()) return -1;
+  // drop / gather / undo per drop word; cnt ends where it started
+  S.stats[5]++;
+  int lm, lt, gm, gt;
+  mode_role(1, &lm, &lt);
+  mode_role(0, &gm, &gt);
+  for (int i = 0; i < k; i++) {
+    int rc = gather_impl(drops + i, 1, lm, lt, loss + i);
+    if (rc) return rc;
+    const long long ni = off[i + 1] - off[i];
+    if (!ni) continue;
+    rc = update_impl(drops + i, 1, -1, nullptr);
+    if (rc) return rc;
+    rc = gather_impl(cand + off[i], (int)ni, gm, gt, gain + off[i]);
+    const int rc2 = update_impl(drops + i, 1, +1, nullptr);
+    if (rc) return rc;
+    if (rc2) return rc2;
+  }
+  return 0;
+}
+
+int dct_loss_owner(const long long *words, int M, int32_t *out) {
+  if (!S.live || !S.owner) return -1;
+  if (!valid_words(words, M) || (M && !out)) return -2;
+  std::unordered_map<long long, int> ms;
+  int mx = 0;
+  for (int i = 0; i < M; i++) mx = std::max(mx, ++ms[words[i]]);
+  if (!within_counter(M, mx)) return -2;
+  CC_CK(cudaMemsetAsync(S.cnt, 0, (size_t)S.cnt_len * 2, g_stream));
+  int rc = update_impl(words, M, +1, nullptr);
+  if (rc) return rc;
+  set_active(ms, M);
+  if (M == 0) return 0;
+  int lm, lt;
+  mode_role(1, &lm, &lt);
+  return gather_impl(words, M, lm, lt, out);
+}
+
+int dct_stats(long long *out, int n) {
+  if (n > 8) n = 8;
+  for (int i = 0; i < n; i++) out[i] = S.stats[i];
+  return n < 0 ? 0 : n;
+}
+
+long long dct_count_eq(int target) {
+  if (!S.live) return -1;
+  CC_CK(cudaMemsetAsync(S.d_scalar, 0, 8, g_stream));
+  int rc = launch_cnt_reduce(S.cnt, S.g.space, kPredEq, target, g_mu,
+                             S.d_scalar, g_stream);
+  if (rc) return rc;
+  long long r;
+  rc = fetch_scalar(&r);
+  return rc ? rc : r;
+}
+
+long long dct_count_deficit(void) {
+  if (!S.live) return -1;
+  CC_CK(cudaMemsetAsync(S.d_scalar, 0, 8, g_stream));
+  int rc = launch_cnt_reduce(S.cnt, S.g.space, kPredDef, 0, g_mu, S.d_scalar,
+                             g_stream);
+  if (rc) return rc;
+  long long r;
+  rc = fetch_scalar(&r);
+  return rc ? rc : r;
+}
+
+int dct_map_max(int32_t *out) {
+  if (!S.live || !out) return -1;
+  CC_CK(cudaMemsetAsync(S.d_scalar, 0, 8, g_stream));
+  int rc = launch_max(S.layers, S.g.space, S.d_scalar, g_stream);
+  if (rc) return rc;
+  long long r;
+  rc = fetch_scalar(&r);
+  if (rc) return rc;
+  *out = (int32_t)r;
+  return 0;
+}
+
+int dct_map_hist(int nbins, int32_t vmax, int32_t *out) {
+  if (!S.live || nbins < 1 || nbins > 4096 || vmax < 1 || !out) return -1;
+  CC_CK(cudaMemsetAsync(S.d_hist, 0, (size_t)nbins * 4, g_stream));
+  int rc = launch_hist(S.layers, S.g.space, nbins, vmax, S.d_hist, g_stream);
+  if (rc) return rc;
+  CC_CK(cudaMemcpyAsync(S.h_out, S.d_hist, (size_t)nbins * 4,
+                        cudaMemcpyDeviceToHost, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));
+  memcpy(out, S.h_out, (size_t)nbins * 4);
+  return 0;
+}
+
+static long long extract_impl(int32_t thr, void *out_idx, bool wide,
+                              int32_t *out_val, int cap) {
+  if (!S.live) return -1;
+  if (cap > S.extract_cap) cap = (int)S.extract_cap;
+  if (cap < 0) cap = 0;
+  CC_CK(cudaMemsetAsync(S.d_scalar, 0, 8, g_stream));
+  void *didx = wide ? (void *)S.d_ext64 : (void *)S.d_ext32;
+  int rc = launch_extract(S.layers, S.g.space, thr, didx, wide, S.d_extv, cap,
+                          S.d_scalar, g_stream);
+  if (rc) return rc;
+  long long found;
+  rc = fetch_scalar(&found);
+  if (rc) return rc;
+  const long long m = found < cap ? found : cap;
+  if (m > 0) {
+    CC_CK(cudaMemcpyAsync(out_idx, didx, (size_t)m * (wide ? 8 : 4),
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaMemcpyAsync(out_val, S.d_extv, (size_t)m * 4,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+  }
+  return found;
+}
+
+long long dct_map_extract(int32_t thr, uint32_t *idx, int32_t *val, int cap) {
+  return extract_impl(thr, idx, false, val, cap);
+}
+
+long long dct_map_extract64(int32_t thr, int64_t *idx, int32_t *val,
+                            int cap) {
+  return extract_impl(thr, idx, true, val, cap);
+}
+
+int dct_map_read_at(const long long *idx, int k, int32_t *out) {
+  if (!S.live) return -1;
+  if (k <= 0) return 0;
+  if (!out || !valid_words(idx, k)) return -1;
+  for (long long off = 0; off < k; off += kStageCap) {
+    const int nb = (int)std::min<long long>(kStageCap, k - off);
+    int rc = stage_words(idx + off, nb);
+    if (rc) return rc;
+    rc = launch_read_at(S.layers, S.d_words, nb, S.d_out, g_stream);
+    if (rc) return rc;
+    CC_CK(cudaMemcpyAsync(S.h_out, S.d_out, (size_t)nb * 4,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    memcpy(out + off, S.h_out, (size_t)nb * 4);
+  }
+  return 0;
+}
+
+int dct_read_cnt(long long off, long long len, uint16_t *out) {
+  if (!S.live || off < 0 || len < 0 || off + len > S.g.space ||
+      (len && !out))
+    return -1;
+  if (len)
+    CC_CK(cudaMemcpyAsync(out, S.cnt + off, (size_t)len * 2,
+                          cudaMemcpyDefault, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));   // async updates were in flight
+  return 0;
+}
+
+long long dct_b200_stream(void) {
+  if (ensure_stream()) return 0;
+  return (long long)(uintptr_t)g_stream;
+}
+
+int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
+  if (!S.live || init_mode < 0 || init_mode > 2 || out_mode < 1 ||
+      out_mode > 3)
+    return -1;
+  Plan &P = plan_for(init_mode, out_mode);
+  const long long X = S.g.space;
+  int n = 0;
+  if (P.window) {
+    for (size_t i = 0; i < P.passes.size(); i++, n++) {
+      const WindowArgs &w = P.passes[i];
+      const long long by = X * ((w.src16 ? 2 : 4) + (w.dst16 ? 2 : 4));
+      if (info && 4 * n + 3 < cap) {
+        info[4 * n] = (long long)i; info[4 * n + 1] = 1;
+        info[4 * n + 2] = by; info[4 * n + 3] = -2;
+      }
+    }
+    return n;
+  }
+  int j = 0;
+  for (const auto &p : P.groups) {
+    long long rd = 0, wr = 0;
+    if (p.a.src == kSrcCnt) rd = 2;
+    else if (p.a.src == kSrcLayers) rd = 4LL * p.a.lin;
+    if (p.a.dst == kDstLayers) wr = 4LL * p.a.lout;
+    else if (p.a.dst == kDstMap) wr = 4;
+    else wr = 2;
+    long long by = X * (rd + wr);
+    if (p.a.src == kSrcCode) by += 8 * S.codeM;
+    if (info && 4 * n + 3 < cap) {
+      info[4 * n] = j; info[4 * n + 1] = p.a.k;
+      info[4 * n + 2] = by; info[4 * n + 3] = p.kernel;
+    }
+    j += p.a.k;
+    n++;
+  }
+  return n;
+}
+
+int dct_b200_set_timing(int on) {
+  g_timing = on ? 1 : 0;
+  return 0;
+}
+
+int dct_b200_last_timings(float *ms, int cap) {
+  const int n = g_last_n < cap ? g_last_n : cap;
+  for (int i = 0; i < n && ms; i++) ms[i] = g_last_ms[i];
+  return g_last_n;
+}
+
+int dct_b200_read_map(long long off, long long len, int32_t *out) {
+  if (!S.live || off < 0 || len < 0 || off + len > S.g.space ||
+      (len && !out))
+    return -1;
+  if (len)
+    CC_CK(cudaMemcpyAsync(out, S.layers + off, (size_t)len * 4,
+                          cudaMemcpyDeviceToHost, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));
+  return 0;
+}
+
+int dct_b200_read_layer(int d, long long off, long long len, int32_t *out) {
+  if (!S.live || !S.layered_out || d < 0 || d >= S.R1 || off < 0 ||
+      len < 0 || off + len > S.g.space || (len && !out))
+    return -1;
+  if (len)
+    CC_CK(cudaMemcpyAsync(out, S.layers + d * S.plane + off,
+                          (size_t)len * 4, cudaMemcpyDeviceToHost, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,236 @@
+// reduce.cu — whole-field reductions and map queries.
+//
+// Semantics of the reference's queries (coldcore
+// src/plugins/covering/dctcore_core.cuh:284-371, dctcore_fast.cuh:191-327,
+// dctcore_mu.cuh:53-73): sum [cnt == t] or sum max(0, mu - cnt) with int64
+// accumulation; the map maximum (0 when every value is <= 0); a histogram of
+// positive values v at bin (v-1)*nbins/vmax clipped to the last bin; the
+// unordered extraction of every map value >= thr, storing at most `cap`
+// entries but counting all of them.
+//
+// These are HBM streaming passes: 16-byte loads (8 counters or 4 map values
+// per load), a grid of 4 x SM-count x 8 warps, warp shuffles then one
+// atomic per block.  Extraction claims output slots with one atomic per warp
+// and, once the output is full, only counts.
+#include "engine.h"
+
+namespace cc {
+
+static int stream_blocks(long long nvec) {
+  long long b = (nvec + 255) / 256;
+  const long long cap = (long long)sm_count() * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+__device__ __forceinline__ long long warp_sum(long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ long long cnt_term(int mode, int c, int target,
+                                              int mu) {
+  if (mode == kPredDef) { int d = mu - c; return d > 0 ? d : 0; }
+  return c == target;
+}
+
+// mode kPredEq: sum [cnt == target]; kPredDef: sum max(0, mu - cnt)
+__global__ void __launch_bounds__(256)
+k_cnt_reduce(const uint16_t *cnt, long long N, int mode, int target, int mu,
+             unsigned long long *out) {
+  const long long nvec = N >> 3;
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  const uint4 *v = reinterpret_cast<const uint4 *>(cnt);
+  long long acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       i < nvec; i += gs) {
+    const uint4 q = v[i];
+    const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int h = 0; h < 8; h++)
+      acc += cnt_term(mode, (int)((w4[h >> 1] >> (16 * (h & 1))) & 0xFFFFu),
+                      target, mu);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (N & 7))
+    acc += cnt_term(mode, (int)cnt[nvec * 8 + threadIdx.x], target, mu);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0 && acc)
+    atomicAdd(out, (unsigned long long)acc);
+}
+
+__global__ void __launch_bounds__(256)
+k_max(const int32_t *A, long long N, long long *out) {
+  const long long nvec = N >> 2;
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  const int4 *v = reinterpret_cast<const int4 *>(A);
+  int32_t m = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       i < nvec; i += gs) {
+    const int4 q = v[i];
+    m = max(m, max(max(q.x, q.y), max(q.z, q.w)));
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (N & 3))
+    m = max(m, A[nvec * 4 + threadIdx.x]);
+  for (int o = 16; o > 0; o >>= 1)
+    m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax((int *)out, m);
+}
+
+__device__ __forceinline__ void hist_one(int32_t v, int nbins, int32_t vmax,
+                                         int32_t *sh) {
+  if (v > 0) {
+    int b = (int)((long long)(v - 1) * nbins / vmax);
+    if (b >= nbins) b = nbins - 1;
+    atomicAdd(&sh[b], 1);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_hist(const int32_t *A, long long N, int nbins, int32_t vmax,
+       int32_t *hist) {
+  extern __shared__ int32_t sh[];
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const long long nvec = N >> 2;
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  const int4 *v = reinterpret_cast<const int4 *>(A);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       i < nvec; i += gs) {
+    const int4 q = v[i];
+    hist_one(q.x, nbins, vmax, sh);
+    hist_one(q.y, nbins, vmax, sh);
+    hist_one(q.z, nbins, vmax, sh);
+    hist_one(q.w, nbins, vmax, sh);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (N & 3))
+    hist_one(A[nvec * 4 + threadIdx.x], nbins, vmax, sh);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// one atomic per warp: slot of this lane's hit, or -1
+__device__ __forceinline__ long long claim_slot(bool hit,
+                                                unsigned long long *ctr) {
+  const unsigned m = __ballot_sync(0xffffffffu, hit);
+  if (!m) return -1;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(ctr, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (!hit) return -1;
+  return (long long)base + __popc(m & ((1u << lane) - 1u));
+}
+
+template <typename IDX>
+__global__ void __launch_bounds__(256)
+k_extract(const int32_t *A, long long N, int32_t thr, IDX *oidx,
+          int32_t *oval, long long cap, unsigned long long *ctr) {
+  const long long nvec = (N + 3) >> 2;          // last vector may be partial
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long trips = (nvec + gs - 1) / gs; // uniform per warp
+  long long tally = 0;
+  for (long long k = 0; k < trips; k++) {
+    const long long i = t0 + k * gs;
+    int32_t e[4] = {0, 0, 0, 0};
+    bool in[4] = {false, false, false, false};
+    if (i < nvec) {
+      if (i * 4 + 3 < N) {
+        const int4 q = reinterpret_cast<const int4 *>(A)[i];
+        e[0] = q.x; e[1] = q.y; e[2] = q.z; e[3] = q.w;
+        in[0] = in[1] = in[2] = in[3] = true;
+      } else {
+        for (int h = 0; h < 4; h++)
+          if (i * 4 + h < N) { e[h] = A[i * 4 + h]; in[h] = true; }
+      }
+    }
+    const bool any = (in[0] && e[0] >= thr) || (in[1] && e[1] >= thr) ||
+                     (in[2] && e[2] >= thr) || (in[3] && e[3] >= thr);
+    if (!__any_sync(0xffffffffu, any)) continue;
+    unsigned long long seen = 0;
+    if ((threadIdx.x & 31) == 0) seen = *(volatile unsigned long long *)ctr;
+    seen = __shfl_sync(0xffffffffu, seen, 0);
+    if ((long long)seen >= cap) {               // full: count only
+      for (int h = 0; h < 4; h++) tally += in[h] && e[h] >= thr;
+      continue;
+    }
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const bool hit = in[h] && e[h] >= thr;
+      const long long s = claim_slot(hit, ctr);
+      if (s >= 0 && s < cap) { oidx[s] = (IDX)(i * 4 + h); oval[s] = e[h]; }
+    }
+  }
+  tally = warp_sum(tally);
+  if ((threadIdx.x & 31) == 0 && tally)
+    atomicAdd(ctr, (unsigned long long)tally);
+}
+
+__global__ void k_read_at(const int32_t *A, const long long *idx, int k,
+                          int32_t *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < k) out[i] = A[idx[i]];
+}
+
+__global__ void k_scatter(int32_t *A, const long long *idx, long long M) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < M) atomicAdd(&A[idx[i]], 1);
+}
+
+int launch_cnt_reduce(const uint16_t *cnt, long long N, int mode, int target,
+                      int mu, long long *out, cudaStream_t s) {
+  k_cnt_reduce<<<stream_blocks(N >> 3), 256, 0, s>>>(
+      cnt, N, mode, target, mu, reinterpret_cast<unsigned long long *>(out));
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_max(const int32_t *A, long long N, long long *out,
+               cudaStream_t s) {
+  k_max<<<stream_blocks(N >> 2), 256, 0, s>>>(A, N, out);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_hist(const int32_t *A, long long N, int nbins, int32_t vmax,
+                int32_t *hist, cudaStream_t s) {
+  k_hist<<<stream_blocks(N >> 2), 256, nbins * 4, s>>>(A, N, nbins, vmax,
+                                                        hist);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_extract(const int32_t *A, long long N, int32_t thr, void *oidx,
+                   bool wide, int32_t *oval, long long cap, long long *ocount,
+                   cudaStream_t s) {
+  const int nb = stream_blocks((N + 3) >> 2);
+  auto *ctr = reinterpret_cast<unsigned long long *>(ocount);
+  if (wide)
+    k_extract<int64_t><<<nb, 256, 0, s>>>(A, N, thr, (int64_t *)oidx, oval,
+                                          cap, ctr);
+  else
+    k_extract<uint32_t><<<nb, 256, 0, s>>>(A, N, thr, (uint32_t *)oidx, oval,
+                                           cap, ctr);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_read_at(const int32_t *A, const long long *idx, int k,
+                   int32_t *out, cudaStream_t s) {
+  if (k <= 0) return 0;
+  k_read_at<<<(k + 255) / 256, 256, 0, s>>>(A, idx, k, out);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_scatter(int32_t *A, const long long *idx, long long M,
+                   cudaStream_t s) {
+  if (M <= 0) return 0;
+  k_scatter<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(A, idx, M);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace cc

@@ -1,0 +1,58 @@
+// transform_window.cu — one window-sum axis pass of any width (torus / grid).
+//
+// Recurrence of the reference's torus and open-grid plugins
+// (coldcore src/plugins/covering/dctcore_torus.cuh:1-12,
+//  dctcore_grid.cuh:1-30): newA[a] = sum of A over the circular (torus) or
+// clamped (grid) window [a-R, a+R] along one axis.  The reference keeps the
+// fibre in a 16-entry register array (axes <= 16); this pass has no width
+// limit (the king 2048x2048 torus), runs out of place, and maps one thread
+// to one output word so that a warp's 2R+1 reads and its write are 128-byte
+// coalesced along the contiguous inner index; the 2R neighbours of a word
+// are re-read from L1/L2, not HBM.
+#include "engine.h"
+
+namespace cc {
+
+template <bool GRID, int SRC16, int DST16>
+__global__ void __launch_bounds__(256) window_axis(const WindowArgs w) {
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       x < w.space; x += gs) {
+    const long long hi = x / w.stride;
+    const int a = (int)(hi % w.q);
+    const long long base = x - (long long)a * w.stride;
+    int lo = a - w.R, up = a + w.R;
+    if (GRID) { if (lo < 0) lo = 0; if (up > w.q - 1) up = w.q - 1; }
+    int32_t s = 0;
+    for (int b = lo; b <= up; b++) {
+      int bb = b;
+      if (!GRID) { if (bb < 0) bb += w.q; else if (bb >= w.q) bb -= w.q; }
+      const long long y = base + (long long)bb * w.stride;
+      if (SRC16) s += cnt_pred(w.pmode, (int)w.src16[y], w.ptarget, w.mu);
+      else s += w.src32[y];
+    }
+    if (DST16) w.dst16[x] = (uint16_t)(s > 65535 ? 65535 : s);
+    else w.dst32[x] = s;
+  }
+}
+
+int launch_window(const WindowArgs &w, cudaStream_t s) {
+  long long nb = (w.space + 255) / 256;
+  const long long cap = (long long)sm_count() * 16;
+  if (nb > cap) nb = cap;
+  if (nb < 1) nb = 1;
+  const bool s16 = w.src16 != nullptr, d16 = w.dst16 != nullptr;
+#define WL(G, A, B) window_axis<G, A, B><<<(int)nb, 256, 0, s>>>(w)
+  if (w.grid) {
+    if (s16 && d16) WL(true, 1, 1); else if (s16) WL(true, 1, 0);
+    else if (d16) WL(true, 0, 1); else WL(true, 0, 0);
+  } else {
+    if (s16 && d16) WL(false, 1, 1); else if (s16) WL(false, 1, 0);
+    else if (d16) WL(false, 0, 1); else WL(false, 0, 0);
+  }
+#undef WL
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace cc

@@ -1,0 +1,171 @@
+// walks.cu — exact incremental updates and per-candidate queries over a
+// word's support set (its metric ball).
+//
+// Semantics of the reference's support walks
+// (coldcore src/plugins/covering/dctcore_core.cuh:158-273, dctcore_grid.cuh
+// :239-342, dctcore_mu.cuh:75-105, dctcore_fast.cuh:360-389): the ball of a
+// centre w is the support table's patterns applied to w's digits, each
+// pattern a set of (position, circular shift) pairs; the open grid rejects a
+// pattern whose shift wraps past a board edge.  cnt is a uint16 plane,
+// updated with packed 32-bit atomics on the aligned counter pair (the plane
+// is padded, so the partner of the last counter exists and stays 0).
+//
+// The table is held as 32-bit (position, delta) slots instead of the v1
+// nibble bytes, so axes of any width walk (the v1 format stops at 16).  A
+// block owns one word (or a slice of its ball when the ball is large): the
+// word's digits, axis sizes and strides sit in shared memory, and each
+// thread resolves one pattern at a time with a few integer ops per slot.
+#include "engine.h"
+
+namespace cc {
+
+struct WordSmem {
+  int dig[kMaxAxes];
+  int ax[kMaxAxes];
+  long long pw[kMaxAxes];
+};
+
+__device__ __forceinline__ void word_setup(const Geometry &g, long long w,
+                                           WordSmem &s) {
+  for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
+    s.dig[j] = (int)((w / g.pw[j]) % g.ax[j]);
+    s.ax[j] = g.ax[j];
+    s.pw[j] = g.pw[j];
+  }
+  __syncthreads();
+}
+
+// word index of pattern t around w; -1 when the open grid rejects it
+template <bool GRID>
+__device__ __forceinline__ long long walk_word(const WalkArgs &a, long long w,
+                                               long long t, const WordSmem &s) {
+  long long x = w;
+#pragma unroll 1
+  for (int k = 0; k < a.slots; k++) {
+    const int code = a.tbl[(long long)k * a.len + t];
+    if (!code) break;
+    const int p = code >> 24, dl = code & 0xFFFFFF;
+    const int dg = s.dig[p];
+    int nd = dg + dl;
+    if (nd >= s.ax[p]) nd -= s.ax[p];
+    const int sh = nd - dg;
+    if (GRID && (sh > a.g.R || sh < -a.g.R)) return -1;
+    x += (long long)sh * s.pw[p];
+  }
+  return x;
+}
+
+__device__ __forceinline__ long long block_sum(long long v) {
+  __shared__ long long red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();                      // red may be in use by a prior call
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  v = threadIdx.x < (blockDim.x >> 5) ? red[lane] : 0;
+  if (wid == 0)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;                             // valid in thread 0
+}
+
+// cnt[x] += delta over each word's support set.  trans != nullptr also
+// counts the deficit transitions read off the atomics' old values (an
+// increment from c < mu, a decrement from c <= mu).
+template <bool GRID, bool PARAM>
+__global__ void __launch_bounds__(256)
+k_update(const WalkArgs a, const long long *words, const WordsParam pw,
+         int split, int delta, unsigned long long *trans) {
+  __shared__ WordSmem s;
+  const int wi = blockIdx.x / split, seg = blockIdx.x % split;
+  const long long w = PARAM ? pw.w[wi] : words[wi];
+  word_setup(a.g, w, s);
+  long long acc = 0;
+  const long long step = (long long)split * blockDim.x;
+  for (long long t = (long long)seg * blockDim.x + threadIdx.x; t < a.len;
+       t += step) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x < 0) continue;
+    uint32_t *cell = reinterpret_cast<uint32_t *>(a.cnt + (x & ~1LL));
+    const int sh = (x & 1) ? 16 : 0;
+    const uint32_t add = 1u << sh;
+    const uint32_t old = delta > 0 ? atomicAdd(cell, add) : atomicSub(cell, add);
+    if (trans) {
+      const int c = (int)((old >> sh) & 0xFFFFu);
+      acc += delta > 0 ? (c < a.g.mu) : (c <= a.g.mu);
+    }
+  }
+  if (trans) {
+    acc = block_sum(acc);
+    if (threadIdx.x == 0 && acc) atomicAdd(trans, (unsigned long long)acc);
+  }
+}
+
+// out[wi] = #{x in B(w_i) : pred(cnt[x])}; split blocks per word add up
+template <bool GRID>
+__global__ void __launch_bounds__(256)
+k_gather(const WalkArgs a, const long long *words, int split, int mode,
+         int target, int32_t *out) {
+  __shared__ WordSmem s;
+  const int wi = blockIdx.x / split, seg = blockIdx.x % split;
+  const long long w = words[wi];
+  word_setup(a.g, w, s);
+  long long acc = 0;
+  const long long step = (long long)split * blockDim.x;
+  for (long long t = (long long)seg * blockDim.x + threadIdx.x; t < a.len;
+       t += step) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x >= 0) acc += cnt_pred(mode, (int)a.cnt[x], target, a.g.mu);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) {
+    if (split == 1) out[wi] = (int32_t)acc;
+    else if (acc) atomicAdd(&out[wi], (int32_t)acc);
+  }
+}
+
+// blocks per word so that single-word walks still fill the GPU
+int pick_split(long long len, int nb) {
+  long long cover = (len + 255) / 256;
+  long long split = (long long)sm_count() * 64 / (nb > 0 ? nb : 1);
+  if (split < 1) split = 1;
+  if (split > cover) split = cover;
+  if (split > 65535) split = 65535;
+  return (int)split;
+}
+
+int launch_update(const WalkArgs &w, const long long *dwords,
+                  const WordsParam *pw, int nb, int delta,
+                  unsigned long long *trans, cudaStream_t s) {
+  if (nb <= 0) return 0;
+  const int split = pick_split(w.len, nb);
+  const dim3 grid((unsigned)nb * split);
+  const bool grid_prob = w.g.prob == kGrid;
+  static WordsParam empty;
+  if (dwords) {
+    if (grid_prob) k_update<true, false><<<grid, 256, 0, s>>>(w, dwords, empty, split, delta, trans);
+    else k_update<false, false><<<grid, 256, 0, s>>>(w, dwords, empty, split, delta, trans);
+  } else {
+    if (grid_prob) k_update<true, true><<<grid, 256, 0, s>>>(w, nullptr, *pw, split, delta, trans);
+    else k_update<false, true><<<grid, 256, 0, s>>>(w, nullptr, *pw, split, delta, trans);
+  }
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
+                  int mode, int target, int32_t *out, bool zeroed,
+                  cudaStream_t s) {
+  if (nb <= 0) return 0;
+  const int split = pick_split(w.len, nb);
+  if (split > 1 && !zeroed)
+    CC_CK(cudaMemsetAsync(out, 0, (size_t)nb * 4, s));
+  const dim3 grid((unsigned)nb * split);
+  if (w.g.prob == kGrid)
+    k_gather<true><<<grid, 256, 0, s>>>(w, dwords, split, mode, target, out);
+  else
+    k_gather<false><<<grid, 256, 0, s>>>(w, dwords, split, mode, target, out);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace cc

@@ -1,0 +1,452 @@
+"""ctypes binding of the B200 covering engine (plugin ABI v1).
+
+Mirrors coldcore's ``src/coldcore/gpu.py`` (``GpuBackend``,
+``load_plugin``, ``default_plugin_path``, ``locality_order`` and the two
+``*_generic`` reference forms): same constructor arguments, method names,
+return types and ``RuntimeError`` on a negative return code, so a search
+core written against the reference's backend runs on this one unchanged.
+The library is ``coldcore_b200/libcoldcore_covering.so`` (built by
+``python -m coldcore_b200.build``); there is no fallback — a missing or
+unloadable library raises.
+
+Additions: cells with axes wider than 16 (king 2048x2048) go through
+``dct_init3w`` with the engine's wide support table; ``layer(d)`` reads
+the exact distance layers after ``layers_map()``; ``stream`` is the
+engine's CUDA stream handle for host-side timing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .patterns import PROBLEM_IDS, locality_key, v1_table, wide_table
+from .space import ProductSpace
+
+_libs = {}
+
+_LL = ctypes.c_longlong
+_I32P = ctypes.POINTER(ctypes.c_int32)
+_LLP = ctypes.POINTER(_LL)
+
+REQUIRED = ("dct_init3", "dct_free", "dct_set_code", "dct_transform",
+            "dct_ball_update", "dct_ball_gather", "dct_count_eq",
+            "dct_map_max", "dct_map_extract", "dct_map_extract64",
+            "dct_map_read_at", "dct_read_cnt")
+
+
+def _rc_msg(rc):
+    if rc <= -100:
+        return f"rc={rc} (CUDA error {-(rc + 100)})"
+    return f"rc={rc}"
+
+
+def _check(name, rc):
+    if rc != 0:
+        raise RuntimeError(f"{name} {_rc_msg(rc)}")
+
+
+def _bind(path):
+    lib = ctypes.CDLL(path)
+    missing = [f for f in REQUIRED if not hasattr(lib, f)]
+    if missing:
+        raise RuntimeError(f"{path} lacks required symbols {missing}")
+    I, P64 = ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)
+    sig = {
+        "dct_init3": (I, [I, I, ctypes.POINTER(I), I, P64, _LL, I, _LLP, I, I,
+                          I]),
+        "dct_init3w": (I, [I, I, ctypes.POINTER(I), I, _I32P, I, _LL, I,
+                           _LLP]),
+        "dct_init2": (I, [I, I, I, P64, _LL, I, _LLP, I, I, I]),
+        "dct_init": (I, [I, I, I, P64, _LL, I, _LLP]),
+        "dct_free": (I, []),
+        "dct_host_bytes": (_LL, []),
+        "dct_set_code": (I, [_LLP, I]),
+        "dct_transform": (I, [I, I]),
+        "dct_set_mu": (I, [I]),
+        "dct_get_mu": (I, []),
+        "dct_ball_update": (I, [_LLP, I, I]),
+        "dct_ball_gather": (I, [_LLP, I, I, _I32P]),
+        "dct_ball_gather_mu": (I, [_LLP, I, I, _I32P]),
+        "dct_loss_owner": (I, [_LLP, I, _I32P]),
+        "dct_ball_update_delta": (I, [_LLP, I, I, _LLP]),
+        "dct_swap_eval": (I, [_LLP, I, _LLP, _LLP, _I32P, _I32P]),
+        "dct_stats": (I, [_LLP, I]),
+        "dct_count_eq": (_LL, [I]),
+        "dct_count_deficit": (_LL, []),
+        "dct_map_max": (I, [_I32P]),
+        "dct_map_hist": (I, [I, ctypes.c_int32, _I32P]),
+        "dct_map_extract": (_LL, [ctypes.c_int32,
+                                  ctypes.POINTER(ctypes.c_uint32), _I32P, I]),
+        "dct_map_extract64": (_LL, [ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_int64), _I32P, I]),
+        "dct_map_read_at": (I, [_LLP, I, _I32P]),
+        "dct_read_cnt": (I, [_LL, _LL, ctypes.POINTER(ctypes.c_uint16)]),
+        "dct_set_tbl2": (I, [ctypes.POINTER(ctypes.c_uint16), P64, _LL]),
+        "dct_use_fmt": (I, [I]),
+        "dct_b200_stream": (_LL, []),
+        "dct_b200_plan": (I, [I, I, _LLP, I]),
+        "dct_b200_read_layer": (I, [I, _LL, _LL, _I32P]),
+        "dct_b200_read_map": (I, [_LL, _LL, _I32P]),
+        "dct_b200_set_timing": (I, [I]),
+        "dct_b200_last_timings": (I, [ctypes.POINTER(ctypes.c_float), I]),
+    }
+    for name, (res, args) in sig.items():
+        if hasattr(lib, name):
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+    return lib
+
+
+def default_plugin_path():
+    """``COLDCORE_PLUGIN_PATH`` if set, else the in-tree library."""
+    env = os.environ.get("COLDCORE_PLUGIN_PATH")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        "libcoldcore_covering.so")
+
+
+def load_plugin(path=None):
+    """Load (and cache) the engine library; raises when it is missing."""
+    path = os.path.abspath(path or default_plugin_path())
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"engine library not built: {path} "
+                "(run `python -m coldcore_b200.build`)")
+        _libs[path] = _bind(path)
+    return _libs[path]
+
+
+def locality_order(pats, axes):
+    """Sort a v1 table by unwrapped offset so that neighbouring walk threads
+    touch neighbouring words (coldcore ``gpu.py:106-129``); order-free walks
+    make this a pure traffic optimisation.  Entry 0 stays the centre."""
+    pats = np.ascontiguousarray(pats, dtype=np.uint64)
+    n = len(axes)
+    pos = np.zeros((len(pats), 8), dtype=np.int64)
+    dlt = np.zeros((len(pats), 8), dtype=np.int64)
+    for k in range(8):
+        b = ((pats >> np.uint64(8 * k)) & np.uint64(255)).astype(np.int64)
+        pos[:, k] = np.minimum(b >> 4, n - 1)
+        dlt[:, k] = b & 15
+    return np.ascontiguousarray(
+        pats[np.argsort(locality_key(pos, dlt, axes), kind="stable")])
+
+
+def swap_eval_generic(backend, drops, cands):
+    """Reference form of ``swap_eval`` for any backend (coldcore
+    ``gpu.py:132-164``): gather role 1 of each drop, then with that drop
+    removed the role-0 gathers of its candidates; cnt is restored."""
+    drops = np.atleast_1d(np.asarray(drops, dtype=np.int64))
+    shared = not isinstance(cands, (list, tuple))
+    parts = ([np.atleast_1d(np.asarray(cands, dtype=np.int64))] * len(drops)
+             if shared else
+             [np.atleast_1d(np.asarray(c, dtype=np.int64)) for c in cands])
+    loss = np.empty(len(drops), dtype=np.int32)
+    gains = []
+    for i, w in enumerate(drops.tolist()):
+        wa = np.array([w], dtype=np.int64)
+        loss[i] = int(backend.ball_gather(wa, 1)[0])
+        if len(parts[i]):
+            backend.ball_update(wa, -1)
+            gains.append(np.asarray(backend.ball_gather(parts[i], 0),
+                                    dtype=np.int32))
+            backend.ball_update(wa, +1)
+        else:
+            gains.append(np.zeros(0, dtype=np.int32))
+    if shared:
+        return loss, (np.stack(gains) if len(gains) else
+                      np.zeros((0, len(parts[0]) if parts else 0),
+                               dtype=np.int32))
+    return loss, gains
+
+
+def ball_update_delta_generic(backend, idx, delta):
+    """Update plus the change of ``uncovered()`` (coldcore ``gpu.py:167``)."""
+    u0 = backend.uncovered()
+    backend.ball_update(idx, delta)
+    return backend.uncovered() - u0
+
+
+def _p(a, t=_LL):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+class GpuBackend:
+    """One problem cell resident on the B200 (coldcore ``gpu.py:207-537``).
+
+    problem: "hamming", "torus_linf", "lee" or "grid_linf"; mu: covering
+    multiplicity; layers_mode / cnt_mode: 0 = HBM, 1 / 2 = managed memory
+    (None = HBM).
+    """
+
+    def __init__(self, axes, R, problem="hamming", plugin_path=None,
+                 extract_cap=1 << 22, layers_mode=None, cnt_mode=None,
+                 use_owner=False, mu=1):
+        if problem not in PROBLEM_IDS:
+            raise ValueError(f"unknown problem {problem!r}")
+        self.problem = problem
+        self.R = int(R)
+        self.mu = mu = int(mu)
+        if not 1 <= mu <= 65535:
+            raise ValueError("mu must be in 1..65535")
+        self.space = ProductSpace(axes)
+        self.extract_cap = int(extract_cap)
+        self.indep_dist = 2 * R if problem in ("hamming", "lee") else None
+        self.supports_hist = True
+        self._lib = lib = load_plugin(plugin_path)
+        self._ext_bufs = None
+        self._closed = True
+        axes = self.space.axes
+        by = _LL(0)
+        ax = (ctypes.c_int * self.space.n)(*axes)
+        pid = PROBLEM_IDS[problem]
+        if max(axes) <= 16 and (problem in ("hamming", "lee")
+                                or self.space.n <= 8):
+            pats = v1_table(axes, R, problem)
+            self.ball_len = len(pats)
+            rc = lib.dct_init3(pid, self.space.n, ax, self.R,
+                               _p(pats, ctypes.c_uint64), len(pats),
+                               self.extract_cap, ctypes.byref(by),
+                               layers_mode or 0, cnt_mode or 0,
+                               1 if use_owner else 0)
+        else:
+            tbl = wide_table(axes, R, problem)
+            self.ball_len = len(tbl)
+            rc = lib.dct_init3w(pid, self.space.n, ax, self.R,
+                                _p(tbl, ctypes.c_int32), tbl.shape[1],
+                                len(tbl), self.extract_cap, ctypes.byref(by))
+        _check("init", rc)
+        self._closed = False
+        _check("set_mu", lib.dct_set_mu(mu))
+        self.gpu_bytes = by.value
+        self.host_bytes = int(lib.dct_host_bytes())
+
+    # ---------------- lifecycle
+    def close(self):
+        if not self._closed:
+            self._lib.dct_free()
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def word_index(self, words):
+        return self.space.word_index(words)
+
+    def index_word(self, idx):
+        return self.space.index_word(idx)
+
+    @property
+    def stream(self):
+        return int(self._lib.dct_b200_stream())
+
+    # ---------------- fields
+    def _set_code(self, idx):
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        _check("set_code", self._lib.dct_set_code(_p(idx), len(idx)))
+
+    def recount(self, idx):
+        self._set_code(idx)
+        _check("transform(code->cnt)", self._lib.dct_transform(0, 2))
+
+    def gain_map(self):
+        _check("transform(uncov->gain)", self._lib.dct_transform(1, 1))
+
+    def loss_map(self):
+        _check("transform(cnt1->loss)", self._lib.dct_transform(2, 1))
+
+    def layers_map(self, init_mode=0):
+        """Transform into the exact distance layers N_0..N_R (Hamming, Lee):
+        init_mode 0 = the staged code, 1 = deficient words, 2 = critical."""
+        _check("transform(layers)", self._lib.dct_transform(init_mode, 3))
+
+    def layer(self, d, off=0, length=None):
+        length = self.space.size - off if length is None else length
+        out = np.empty(length, dtype=np.int32)
+        _check("read_layer", self._lib.dct_b200_read_layer(
+            d, off, length, _p(out, ctypes.c_int32)))
+        return out
+
+    def set_timing(self, on):
+        self._lib.dct_b200_set_timing(1 if on else 0)
+
+    def last_timings(self):
+        """Device milliseconds of each launch of the last transform."""
+        buf = (ctypes.c_float * 64)()
+        n = self._lib.dct_b200_last_timings(buf, 64)
+        return [float(buf[i]) for i in range(min(n, 64))]
+
+    def plan(self, init_mode, out_mode):
+        """Launches of one transform: rows (first axis, axes, bytes, kernel)."""
+        buf = np.zeros(4 * 64, dtype=np.int64)
+        n = self._lib.dct_b200_plan(init_mode, out_mode, _p(buf), len(buf))
+        if n < 0:
+            _check("plan", n)
+        return buf[:4 * n].reshape(n, 4)
+
+    # ---------------- incremental / exact
+    def ball_update(self, idx, delta):
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        _check("ball_update", self._lib.dct_ball_update(
+            _p(idx), len(idx), int(delta)))
+
+    def ball_gather(self, idx, target):
+        """Exact per-candidate count of ball words by coverage role:
+        0 deficient (cnt < mu), 1 critical (1 <= cnt <= mu), else the
+        literal cnt == target (coldcore ``gpu.py:323-348``)."""
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        out = np.empty(len(idx), dtype=np.int32)
+        if not len(idx):
+            return out
+        if self.mu == 1 or target not in (0, 1):
+            _check("ball_gather", self._lib.dct_ball_gather(
+                _p(idx), len(idx), int(target), _p(out, ctypes.c_int32)))
+        else:
+            _check("ball_gather_mu", self._lib.dct_ball_gather_mu(
+                _p(idx), len(idx), int(target), _p(out, ctypes.c_int32)))
+        return out
+
+    def ball_update_delta(self, idx, delta):
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        dd = _LL(0)
+        _check("ball_update_delta", self._lib.dct_ball_update_delta(
+            _p(idx), len(idx), int(delta), ctypes.byref(dd)))
+        return int(dd.value)
+
+    def swap_eval(self, drops, cands):
+        """Exact costs of many swaps without changing state (coldcore
+        ``gpu.py:368-440``): ``(loss, gains)``."""
+        drops = np.ascontiguousarray(np.atleast_1d(drops), dtype=np.int64)
+        k = len(drops)
+        shared = not isinstance(cands, (list, tuple))
+        cap = (1 << 16) - 1
+        if shared:
+            c1 = np.ascontiguousarray(np.atleast_1d(cands), dtype=np.int64)
+            parts = [c1] * k
+        else:
+            if len(cands) != k:
+                raise ValueError("need one candidate array per drop")
+            parts = [np.ascontiguousarray(np.atleast_1d(c), dtype=np.int64)
+                     for c in cands]
+        loss = np.empty(k, dtype=np.int32)
+        gains = [None] * k
+        i = 0
+        while i < k:
+            j, tot = i, 0
+            while j < k and j - i < cap and tot + len(parts[j]) <= cap:
+                tot += len(parts[j])
+                j += 1
+            if j == i:
+                raise ValueError(f"over {cap} candidates for one drop")
+            cat = (np.concatenate(parts[i:j]) if tot
+                   else np.zeros(1, dtype=np.int64))
+            off = np.zeros(j - i + 1, dtype=np.int64)
+            off[1:] = np.cumsum([len(p) for p in parts[i:j]])
+            g = np.empty(max(tot, 1), dtype=np.int32)
+            lo = np.empty(j - i, dtype=np.int32)
+            sub = np.ascontiguousarray(drops[i:j])
+            _check("swap_eval", self._lib.dct_swap_eval(
+                _p(sub), j - i, _p(cat), _p(off), _p(g, ctypes.c_int32),
+                _p(lo, ctypes.c_int32)))
+            loss[i:j] = lo
+            for t in range(j - i):
+                gains[i + t] = g[off[t]:off[t + 1]].copy()
+            i = j
+        if shared:
+            return loss, (np.stack(gains) if k
+                          else np.zeros((0, len(c1)), dtype=np.int32))
+        return loss, gains
+
+    def loss_owner(self, idx):
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        out = np.empty(len(idx), dtype=np.int32)
+        _check("loss_owner", self._lib.dct_loss_owner(
+            _p(idx), len(idx), _p(out, ctypes.c_int32)))
+        return out
+
+    def gpu_stats(self):
+        buf = (_LL * 8)()
+        self._lib.dct_stats(buf, 8)
+        keys = ("gather_set_side", "gather_walk", "set_scans",
+                "set_overflows", "swap_eval_fast", "swap_eval_fallback",
+                "count_eq0_listed", "gather_set_tiled")
+        return {k: int(v) for k, v in zip(keys, buf)}
+
+    # ---------------- queries
+    def count_eq(self, target):
+        r = int(self._lib.dct_count_eq(int(target)))
+        if r < 0:
+            _check("count_eq", r)
+        return r
+
+    def uncovered(self):
+        """Total deficit sum_x max(0, mu - cnt(x)) (mu = 1: uncovered)."""
+        if self.mu == 1:
+            return self.count_eq(0)
+        r = int(self._lib.dct_count_deficit())
+        if r < 0:
+            _check("count_deficit", r)
+        return r
+
+    def map_max(self):
+        v = ctypes.c_int32(0)
+        _check("map_max", self._lib.dct_map_max(ctypes.byref(v)))
+        return int(v.value)
+
+    def map_hist(self, nbins, vmax):
+        out = np.zeros(nbins, dtype=np.int32)
+        _check("map_hist", self._lib.dct_map_hist(
+            int(nbins), int(vmax), _p(out, ctypes.c_int32)))
+        return out
+
+    def map_extract(self, thr, cap=None):
+        cap = min(cap or self.extract_cap, self.extract_cap)
+        wide = self.space.size > 2 ** 32 - 2
+        oi = np.empty(max(cap, 1), dtype=np.int64 if wide else np.uint32)
+        ov = np.empty(max(cap, 1), dtype=np.int32)
+        if wide:
+            found = self._lib.dct_map_extract64(
+                int(thr), _p(oi, ctypes.c_int64), _p(ov, ctypes.c_int32), cap)
+        else:
+            found = self._lib.dct_map_extract(
+                int(thr), _p(oi, ctypes.c_uint32), _p(ov, ctypes.c_int32), cap)
+        if found < 0:
+            _check("map_extract", int(found))
+        m = min(int(found), cap)
+        return oi[:m].astype(np.int64), ov[:m].copy(), int(found)
+
+    def map_all(self):
+        """The whole map field in one device-to-host copy."""
+        out = np.empty(self.space.size, dtype=np.int32)
+        _check("read_map", self._lib.dct_b200_read_map(
+            0, self.space.size, _p(out, ctypes.c_int32)))
+        return out
+
+    def map_read_at(self, idx):
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        out = np.empty(len(idx), dtype=np.int32)
+        if len(idx):
+            _check("map_read_at", self._lib.dct_map_read_at(
+                _p(idx), len(idx), _p(out, ctypes.c_int32)))
+        return out
+
+    def read_cnt(self, off=0, length=None):
+        length = self.space.size - off if length is None else length
+        out = np.empty(length, dtype=np.uint16)
+        _check("read_cnt", self._lib.dct_read_cnt(
+            off, length, _p(out, ctypes.c_uint16)))
+        return out
+
+
+class GpuCoveringBackend(GpuBackend):
+    """Homogeneous covering-code cell K_q(n,R)."""
+
+    def __init__(self, q, n, R, **kw):
+        super().__init__([q] * n, R, problem="hamming", **kw)
+        self.q, self.n = q, n

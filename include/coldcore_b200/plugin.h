@@ -1,0 +1,162 @@
+/* coldcore_b200/plugin.h — C ABI of the B200 covering engine
+ * (libcoldcore_covering.so, built for sm_100a).
+ *
+ * Drop-in for coldcore's plugin ABI v1: the same flat `dct_*` symbols with
+ * the same signatures, return codes and validation, so coldcore's ctypes
+ * binding (src/coldcore/gpu.py:52-103) loads this library unchanged through
+ * COLDCORE_PLUGIN_PATH.  Each declaration cites the reference declaration
+ * it replaces (coldcore src/include/coldcore/plugin.h) and the reference
+ * implementation whose behaviour it keeps (src/plugins/covering/dct_hc.cu).
+ *
+ * Conventions kept from the reference (plugin.h:7-17):
+ *  - singleton context: one cell per process per loaded library;
+ *  - 0 = ok, negative = engine error, -100-e = CUDA error e (message on
+ *    stderr);
+ *  - caller-allocated outputs; input arrays are read before the call returns;
+ *  - invalid indices, update signs other than +-1, over-removals and
+ *    counter overflow are rejected before any state changes.
+ *
+ * Differences (additive or relaxed, never narrowing):
+ *  - up to 40 axes, R <= 7, Hamming/Lee/grid axes up to 2^24, torus axes
+ *    up to 2^24 with 2R+1 <= axis; the v1 table still caps packed patterns
+ *    at 16-wide axes, so wider cells use dct_init3w;
+ *  - the occurrence limit is exact instead of global: a multiset is
+ *    accepted while min(total occurrences, max multiplicity x |B|) <= 65535
+ *    (no uint16 counter can then exceed 65535), which admits every cell
+ *    the reference's 65,535 global cap admits;
+ *  - all device work runs, in call order, on one stream owned by the
+ *    engine (dct_b200_stream) instead of the legacy default stream.
+ */
+#ifndef COLDCORE_B200_PLUGIN_H
+#define COLDCORE_B200_PLUGIN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COLDCORE_PLUGIN_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define CCP_API __attribute__((visibility("default")))
+#else
+#define CCP_API
+#endif
+
+/* problem ids — plugin.h:45-53 */
+#define CCP_PROB_HAMMING    0
+#define CCP_PROB_TORUS_LINF 1
+#define CCP_PROB_LEE        2
+#define CCP_PROB_GRID_LINF  3
+
+/* ---- lifecycle ---- */
+/* plugin.h:62-65; dct_hc.cu:230-374.  ballpat: v1 packed table, byte k =
+ * pos<<4 | delta, zero byte terminates, entry 0 the centre. */
+CCP_API int  dct_init3(int problem, int n, const int *ax, int R,
+               const uint64_t *ballpat, long long balllen, int extract_cap,
+               long long *bytes, int layers_mode, int cnt_mode,
+               int use_owner);
+/* plugin.h:70-72; dct_hc.cu:377-385 (homogeneous Hamming) */
+CCP_API int  dct_init2(int q, int n, int R, const uint64_t *ballpat,
+               long long balllen, int extract_cap, long long *bytes,
+               int layers_mode, int cnt_mode, int use_owner);
+/* plugin.h:73-74; dct_hc.cu:387-391 */
+CCP_API int  dct_init (int q, int n, int R, const uint64_t *ballpat,
+               long long balllen, int extract_cap, long long *bytes);
+/* plugin.h:66; dct_hc.cu:393-428 (also resets mu to 1) */
+CCP_API int  dct_free(void);
+/* plugin.h:67; dct_hc.cu:208 — bytes outside HBM (managed modes) */
+CCP_API long long dct_host_bytes(void);
+
+/* ---- solution / transforms ---- */
+/* plugin.h:81; dct_hc.cu:452-459 — stages the code multiset */
+CCP_API int  dct_set_code(const long long *idx, int M);
+/* plugin.h:82; dct_hc.cu:465-521 — pairs (0,1) (0,2) (1,1) (2,1).
+ * Additive: out_mode 3 (Hamming / Lee) leaves the exact distance layers
+ * N_0..N_R of the transform in the planes instead of their sum, for
+ * dct_b200_read_layer. */
+CCP_API int  dct_transform(int init_mode, int out_mode);
+
+/* ---- mu-fold multiple covering ---- */
+CCP_API int  dct_set_mu(int mu);             /* plugin.h:91; dct_hc.cu:214-220 */
+CCP_API int  dct_get_mu(void);               /* plugin.h:92; dct_hc.cu:222 */
+
+/* ---- incremental / exact per-candidate ---- */
+/* plugin.h:95; dct_hc.cu:567-587 (batches <= 1024 words return before the
+ * device finishes; the next data-returning call waits) */
+CCP_API int  dct_ball_update(const long long *words, int nwords, int delta);
+/* plugin.h:96-97; dct_hc.cu:785-788 */
+CCP_API int  dct_ball_gather(const long long *words, int nwords, int target,
+                     int32_t *out);
+/* plugin.h:100-101; dct_hc.cu:794-799 (role 0 deficient, 1 critical) */
+CCP_API int  dct_ball_gather_mu(const long long *words, int nwords, int role,
+                        int32_t *out);
+/* plugin.h:102; dct_hc.cu:997-1022 — needs use_owner at init */
+CCP_API int  dct_loss_owner(const long long *words, int M, int32_t *out);
+
+/* ---- v0.3 optional ---- */
+/* plugin.h:111-112; dct_hc.cu:826-866 */
+CCP_API int  dct_ball_update_delta(const long long *words, int nwords, int delta,
+                           long long *dd);
+/* plugin.h:113-115; dct_hc.cu:882-977 */
+CCP_API int  dct_swap_eval(const long long *drops, int k, const long long *cand,
+                   const long long *off, int32_t *gain, int32_t *loss);
+/* plugin.h:116; dct_hc.cu:779-783 — counters: [0] gathers served by the
+ * set side, [1] by the walk, [2] predicate-set scans, [3] scans that
+ * overflowed, [4] swap_eval fast path, [5] swap_eval fallback, [6]
+ * count_eq(0) answered by the listing pass, [7] tiled set gathers */
+CCP_API int  dct_stats(long long *out, int n);
+
+/* ---- reductions / map queries ---- */
+CCP_API long long dct_count_eq(int target);          /* plugin.h:122; dct_hc.cu:1024 */
+CCP_API long long dct_count_deficit(void);           /* plugin.h:125; dct_hc.cu:981 */
+CCP_API int  dct_map_max(int32_t *out);              /* plugin.h:126; dct_hc.cu:1056 */
+CCP_API int  dct_map_hist(int nbins, int32_t vmax,   /* plugin.h:127; dct_hc.cu:1071 */
+                  int32_t *out);
+CCP_API long long dct_map_extract  (int32_t thr,     /* plugin.h:128; dct_hc.cu:1093 */
+                            uint32_t *idx, int32_t *val, int cap);
+CCP_API long long dct_map_extract64(int32_t thr,     /* plugin.h:130; dct_hc.cu:1114 */
+                            int64_t *idx, int32_t *val, int cap);
+CCP_API int  dct_map_read_at(const long long *idx,   /* plugin.h:132; dct_hc.cu:1136 */
+                     int k, int32_t *out);
+CCP_API int  dct_read_cnt(long long off,             /* plugin.h:133; dct_hc.cu:1153 */
+                  long long len, uint16_t *out);
+
+/* ---- alternative support-table format (ox) ---- */
+/* plugin.h:136-138; dct_hc.cu:431-450 */
+CCP_API int  dct_set_tbl2(const uint16_t *mask, const uint64_t *offs,
+                  long long len);
+CCP_API int  dct_use_fmt(int fmt);
+
+/* ---- additive symbols of this engine (no reference counterpart) ---- */
+/* dct_init3 with a wide support table: `slots` int32 per pattern, each
+ * (pos << 24) | delta with delta a circular shift in 1..ax[pos]-1, 0 =
+ * unused slot; row 0 the centre.  Lifts the 16-wide axis limit of the v1
+ * nibble format (king 2048x2048 needs it).  Replaces the table argument of
+ * plugin.h:62-65 only. */
+CCP_API int  dct_init3w(int problem, int n, const int *ax, int R,
+                const int32_t *tbl, int slots, long long len,
+                int extract_cap, long long *bytes);
+/* the engine's CUDA stream (cudaStream_t as an integer), for host timing */
+CCP_API long long dct_b200_stream(void);
+/* describe the launches of one dct_transform(init_mode, out_mode) without
+ * running it: per launch 4 values (first axis, axes in the launch,
+ * algorithmic HBM bytes read + written, kernel id); returns the number of
+ * launches (at most cap/4 described) or a negative error. */
+CCP_API int  dct_b200_plan(int init_mode, int out_mode, long long *info, int cap);
+/* per-launch device timing of transforms (events around every launch;
+ * DCT_TIMING=1 in the environment turns it on too and prints each time to
+ * stderr, the reference's DCT_TIMING, dctcore_hamming.cuh:464-511) */
+CCP_API int  dct_b200_set_timing(int on);
+/* milliseconds of each launch of the last transform; returns the count */
+CCP_API int  dct_b200_last_timings(float *ms, int cap);
+/* words [off, off+len) of the map (the last transform's out_mode 1 field) */
+CCP_API int  dct_b200_read_map(long long off, long long len, int32_t *out);
+/* after dct_transform(init, 3): words [off, off+len) of distance layer d */
+CCP_API int  dct_b200_read_layer(int d, long long off, long long len, int32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COLDCORE_B200_PLUGIN_H */
