@@ -308,6 +308,15 @@ int occupancy_grid(const GroupPlan &p) {
   return (int)std::max<long long>(1, grid);
 }
 
+// Distance layers that can be nonzero after axes 0..j-1: each Hamming axis
+// adds at most 1 to the distance, each Lee axis at most floor(a/2).
+int live_layers(int j) {
+  long long reach = 0;
+  for (int i = 0; i < j; i++)
+    reach += S.g.prob == kLee ? S.g.ax[i] / 2 : 1;
+  return (int)std::min<long long>(reach, S.g.R) + 1;
+}
+
 Plan build_group_plan(int src, int dst) {
   Plan P;
   const Geometry &g = S.g;
@@ -372,8 +381,8 @@ Plan build_group_plan(int src, int dst) {
     const bool first = j == 0, last = j + a.k == g.n;
     a.src = first ? src : kSrcLayers;
     a.dst = last ? dst : kDstLayers;
-    a.lin = layered ? std::min(j, g.R) + 1 : 1;
-    a.lout = layered ? std::min(j + a.k, g.R) + 1 : 1;
+    a.lin = layered ? live_layers(j) : 1;
+    a.lout = layered ? live_layers(j + a.k) : 1;
     if (last && dst == kDstLayers) a.lout = R1;   // every layer, zeros too
     a.pmode = kPredEq;
     a.ptarget = 0;
@@ -542,6 +551,7 @@ int init_common(int problem, int n, const int *ax, int R, long long len,
   if (layered && R + 1 > kMaxLayers) return -1;
   for (int i = 0; i < n; i++) {
     if (ax[i] < 2 || ax[i] >= (1 << 24)) return -1;
+    if (layered && ax[i] > 16) return -1;        // register / tile kernels
     if (problem == kTorus && (ax[i] < 3 || 2 * R + 1 > ax[i])) return -1;
   }
   long long space = 1;
@@ -685,9 +695,11 @@ int dct_init3(int problem, int n, const int *ax, int R,
               const uint64_t *ballpat, long long balllen, int extract_cap,
               long long *bytes, int layers_mode, int cnt_mode,
               int use_owner) {
-  if (!ballpat || !ax || n < 1 || n > kMaxAxes) return -1;
+  // the v1 table packs position and delta in one nibble each: n <= 16,
+  // axes <= 16 (wider cells use dct_init3w)
+  if (!ballpat || !ax || n < 1 || n > 16) return -1;
   for (int i = 0; i < n; i++)
-    if (ax[i] < 2 || ax[i] > 16) return -1;      // v1 nibble format
+    if (ax[i] < 2 || ax[i] > 16) return -1;
   if (layers_mode < 0 || layers_mode > 2 || cnt_mode < 0 || cnt_mode > 2)
     return -1;
   int rc = init_common(problem, n, ax, R, balllen, extract_cap, layers_mode,

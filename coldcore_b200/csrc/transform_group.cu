@@ -425,13 +425,15 @@ size_t group_smem_bytes(const GroupArgs &a, int R1) {
 
 int launch_group(const GroupPlan &p, cudaStream_t s) {
   GroupFn fn = p.kernel >= 0 ? kTable[p.kernel].fn : group_generic;
-  static bool attr_set[64 + 1];
+  // opt in to the dynamic shared memory this launch needs (the per-block
+  // limit counts the kernel's static shared memory too)
+  static size_t attr_set[64 + 1];
   const int slot = p.kernel >= 0 ? p.kernel : 64;
-  if (!attr_set[slot]) {
+  if (p.smem > 48 * 1024 && p.smem > attr_set[slot]) {
     CC_CK(cudaFuncSetAttribute((const void *)fn,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               227 * 1024));
-    attr_set[slot] = true;
+                               (int)p.smem));
+    attr_set[slot] = p.smem;
   }
   fn<<<p.grid, p.threads, p.smem, s>>>(p.a);
   CC_CK(cudaGetLastError());

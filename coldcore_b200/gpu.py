@@ -203,8 +203,8 @@ class GpuBackend:
         by = _LL(0)
         ax = (ctypes.c_int * self.space.n)(*axes)
         pid = PROBLEM_IDS[problem]
-        if max(axes) <= 16 and (problem in ("hamming", "lee")
-                                or self.space.n <= 8):
+        if max(axes) <= 16 and self.space.n <= 16 and (
+                problem in ("hamming", "lee") or self.space.n <= 8):
             pats = v1_table(axes, R, problem)
             self.ball_len = len(pats)
             rc = lib.dct_init3(pid, self.space.n, ax, self.R,

@@ -94,8 +94,9 @@ def wide_table(axes, R, problem, order=True):
 
 def v1_table(axes, R, problem, order=True):
     """Reference v1 packed table (uint64 per pattern)."""
-    if max(axes) > 16:
-        raise ValueError("the v1 table packs deltas in nibbles: axes <= 16")
+    if max(axes) > 16 or len(axes) > 16:
+        raise ValueError("the v1 table packs positions and deltas in "
+                         "nibbles: at most 16 axes of size <= 16")
     pos, dlt = enumerate_ball(axes, R, problem)
     if pos.shape[1] > 8:
         raise ValueError("the v1 table holds at most 8 changed positions")

@@ -17,9 +17,10 @@
  *    counter overflow are rejected before any state changes.
  *
  * Differences (additive or relaxed, never narrowing):
- *  - up to 40 axes, R <= 7, Hamming/Lee/grid axes up to 2^24, torus axes
- *    up to 2^24 with 2R+1 <= axis; the v1 table still caps packed patterns
- *    at 16-wide axes, so wider cells use dct_init3w;
+ *  - up to 40 axes, R <= 7, Hamming / Lee axes up to 16, torus / grid axes
+ *    up to 2^24 (torus: 2R+1 <= axis); the v1 table packs positions and
+ *    deltas in nibbles (n <= 16, axes <= 16), so larger cells — binary
+ *    Hamming n = 26, the king 2048x2048 torus — use dct_init3w;
  *  - the occurrence limit is exact instead of global: a multiset is
  *    accepted while min(total occurrences, max multiplicity x |B|) <= 65535
  *    (no uint16 counter can then exceed 65535), which admits every cell

@@ -19,7 +19,7 @@ _lib = None
 def build():
     if (not os.path.exists(LIB)
             or os.path.getmtime(LIB) < os.path.getmtime(SRC)):
-        subprocess.run(["gcc", "-O3", "-march=native", "-fopenmp", "-fPIC",
+        subprocess.run(["gcc", "-O3", "-march=x86-64-v2", "-fopenmp", "-fPIC",
                         "-shared", "-o", LIB, SRC], check=True)
     return LIB
 
