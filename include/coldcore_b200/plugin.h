@@ -154,6 +154,21 @@ CCP_API int  dct_b200_set_timing(int on);
 CCP_API int  dct_b200_last_timings(float *ms, int cap);
 /* words [off, off+len) of the map (the last transform's out_mode 1 field) */
 CCP_API int  dct_b200_read_map(long long off, long long len, int32_t *out);
+/* No counterpart in the reference.  Gain (role 0) or loss (role 1) map of
+ * a Hamming / Lee cell for callers that may not allocate device memory —
+ * a framework whose own allocator must own every buffer, a service that
+ * reserves its memory at start-up.  cnt (uint16, |X| words) and map (int32,
+ * |X| words) are device pointers the caller owns; the (R+1) distance layers
+ * live in a fixed 64 MiB device array inside this library, which every GPU
+ * that loads the library keeps until exit.  Needs round_up(|X|, 64) x (R+1)
+ * <= 16,777,216 words, else returns -6 with a message on stderr.  Queued on
+ * `stream` (a cudaStream_t as an integer, 0 = the default stream) without
+ * waiting.  Calls share the array: calls that overlap on the GPU race.  The
+ * first call on a device looks up the array's address, so make it before
+ * any stream capture.  Calls no cudaMalloc / cudaFree. */
+CCP_API int  dct_b200_field_noalloc(int problem, int n, const int *ax, int R,
+                                    int mu, int role, const uint16_t *cnt,
+                                    int32_t *map, long long stream);
 /* after dct_transform(init, 3): words [off, off+len) of distance layer d */
 CCP_API int  dct_b200_read_layer(int d, long long off, long long len, int32_t *out);
 

@@ -1,0 +1,56 @@
+"""The allocation-free field entry point (dct_b200_field_noalloc) against
+the engine's ordinary transform, bit for bit, on two calls in a row.
+
+It serves callers that may not allocate device memory themselves — for
+instance a host framework whose caching allocator must own every buffer —
+so the test hands it buffers allocated by torch and checks that the map it
+writes equals the one dct_transform computes.  Collected last (file name),
+so a run stopping at the first failure has run everything else first."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from coldcore_b200.gpu import GpuBackend, load_plugin
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lib, problem_id, axes, R, mu, role, cnt_t, map_t, stream):
+    ax = (ctypes.c_int * len(axes))(*axes)
+    return lib.dct_b200_field_noalloc(
+        ctypes.c_int(problem_id), ctypes.c_int(len(axes)), ax,
+        ctypes.c_int(R), ctypes.c_int(mu), ctypes.c_int(role),
+        ctypes.c_void_p(cnt_t.data_ptr()), ctypes.c_void_p(map_t.data_ptr()),
+        ctypes.c_longlong(stream))
+
+
+@pytest.mark.parametrize("problem,pid,axes,R,mu", [
+    ("hamming", 0, [3] * 8, 2, 1), ("hamming", 0, [2] * 12, 3, 2),
+    ("lee", 2, [5, 6, 7], 2, 1), ("hamming", 0, [3] * 13, 3, 1)])
+def test_noalloc_field_matches_transform(problem, pid, axes, R, mu):
+    import torch
+    lib = load_plugin()
+    rng = np.random.default_rng(11)
+    size = int(np.prod(axes))
+    with GpuBackend(axes, R, problem=problem, mu=mu) as b:
+        stream = torch.cuda.current_stream().cuda_stream
+        for call in range(2):                       # two calls in a row
+            code = rng.choice(size, size=max(3, size // 60), replace=False)
+            b.recount(code)
+            cnt = torch.from_numpy(b.read_cnt().view(np.int16)).cuda()
+            out = torch.full((size,), -7, dtype=torch.int32, device="cuda")
+            role = call % 2
+            assert _noalloc(lib, pid, axes, R, mu, role, cnt, out, stream) == 0
+            torch.cuda.synchronize()
+            (b.gain_map if role == 0 else b.loss_map)()
+            assert np.array_equal(out.cpu().numpy(), b.map_all())
+
+
+def test_noalloc_rejects_cells_beyond_its_array():
+    import torch
+    lib = load_plugin()
+    cnt = torch.zeros(8, dtype=torch.int16, device="cuda")
+    out = torch.zeros(8, dtype=torch.int32, device="cuda")
+    # 3^16 words x 5 layers is more than the fixed 16M-word array
+    assert _noalloc(lib, 0, [3] * 16, 4, 1, 0, cnt, out, 0) == -6
