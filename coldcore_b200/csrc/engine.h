@@ -53,6 +53,7 @@ struct GroupArgs {
   uint16_t *cnt;
   const long long *code;  // sorted code (kSrcCode)
   long long ncode;
+  const long long *code_bounds;  // per-tile slice of the code (kSrcCode)
   long long inner, outer, ntiles, nchunk;
   int mid, W, Bo, k;
   int nrounds;
@@ -64,6 +65,7 @@ struct GroupArgs {
   int pmode, ptarget, mu, R;
   int skew;               // log2 of the shared-memory skew period (0 = none)
   int prob;
+  int pipe;               // prefetch the next tile while computing (cp.async)
 };
 
 struct GroupPlan {
@@ -78,6 +80,9 @@ struct GroupPlan {
 int launch_group(const GroupPlan &p, cudaStream_t s);
 size_t group_smem_bytes(const GroupArgs &a, int R1);
 int pick_group_kernel(int prob, int q, int R1, int *bm);
+int launch_code_bounds(const long long *code, long long ncode,
+                       long long tile_words, long long ntiles,
+                       long long *bounds, cudaStream_t s);
 
 // window pass (torus / grid) over one axis, any width, out of place
 struct WindowArgs {

@@ -66,6 +66,8 @@ struct State {
   // code
   long long *d_code = nullptr;
   long long code_cap = 0, codeM = 0;
+  long long *d_bounds = nullptr;   // per-tile code slices of a recount
+  long long bounds_cap = 0;
   // staging
   long long *h_words = nullptr, *d_words = nullptr;
   int32_t *h_out = nullptr, *d_out = nullptr;
@@ -87,6 +89,8 @@ struct State {
   bool layered_out = false;        // last transform left N_0..N_R
   Plan plans[3][4];                // [init_mode][out_mode]
   bool plan_ok[3][4] = {{false}};
+  bool tuned[3][4] = {{false}};
+  float tune_ms[3][4] = {{0}};
 };
 
 State S;
@@ -236,6 +240,7 @@ void free_all() {
   auto F = [](void *p) { if (p) cudaFree(p); };
   auto FH = [](void *p) { if (p) cudaFreeHost(p); };
   F(S.layers); F(S.cnt); F(S.owner); F(S.tbl); F(S.tbl2); F(S.d_code);
+  F(S.d_bounds);
   F(S.d_words); F(S.d_out); F(S.d_scalar); F(S.d_hist); F(S.d_ext32);
   F(S.d_ext64); F(S.d_extv);
   FH(S.h_words); FH(S.h_out); FH(S.h_scalar);
@@ -292,6 +297,8 @@ int threads_for(const GroupArgs &a, int kid, int bm, int q) {
     t = (int)std::min<long long>(256, (long long)a.W * a.mid * a.Bo);
   }
   t = (t + 31) / 32 * 32;
+  const char *cap = getenv("CC_THREADS");          // tuning cap
+  if (cap && atoi(cap) >= 32 && t > atoi(cap)) t = atoi(cap) / 32 * 32;
   return t < 32 ? 32 : t;
 }
 
@@ -317,60 +324,85 @@ int live_layers(int j) {
   return (int)std::min<long long>(reach, S.g.R) + 1;
 }
 
-Plan build_group_plan(int src, int dst) {
+// Schedule knobs of a group plan: the shared-memory budget of a tile and
+// which groups prefetch their next tile (pipe 0 none, 1 the cnt-reading
+// first group, 2 every group).  CC_SMEM_BUDGET_KB / CC_PIPE override the
+// defaults; the autotuner tries several.
+struct Knobs { size_t budget; int pipe; };
+
+Knobs default_knobs() {
+  const char *pe = getenv("CC_PIPE");
+  return {smem_budget(), pe ? atoi(pe) : 1};
+}
+
+Plan build_group_plan(int src, int dst, Knobs kn) {
   Plan P;
   const Geometry &g = S.g;
   const int R1 = S.R1;
   const bool layered = R1 > 1;
-  const size_t budget = smem_budget();
+  const size_t budget = kn.budget;
   int j = 0;
   while (j < g.n) {
     const int q = g.ax[j];
     int bm = 1;
     const int kid = pick_group_kernel(g.prob, q, R1, &bm);
-    GroupArgs a{};
-    a.layers = S.layers;
-    a.plane = S.plane;
-    a.cnt = S.cnt;
-    a.code = S.d_code;
-    a.ncode = S.codeM;
-    a.inner = g.pw[j];
-    a.W = a.inner >= 32 ? 32 : (int)a.inner;
-    a.prob = g.prob;
-    a.R = g.R;
-    a.mu = g_mu;
-    int k = 0;
-    long long mid = 1;
-    for (;;) {
-      if (j + k >= g.n || k >= kMaxRounds) break;
-      const int qn = g.ax[j + k];
-      if (kid >= 0 && qn != q) break;
-      if (kid < 0 && qn > 16) break;
-      const long long mid2 = mid * qn;
-      GroupArgs t = a;
-      t.k = k + 1;
-      t.mid = (int)std::min<long long>(mid2, INT_MAX / 64);
-      const long long outer = g.space / (a.inner * mid2);
-      t.Bo = a.W >= 32 ? 1
-             : (int)std::max<long long>(1, std::min<long long>(
-                   outer, 2048 / (a.W * mid2)));
-      t.skew = 0;
-      if (kid >= 0 && a.W == 1 && (q & (q - 1)) == 0) {
-        int lg = 0;
-        while ((1 << lg) < ipow(q, bm)) lg++;
-        t.skew = lg;
+    GroupArgs base{};
+    base.layers = S.layers;
+    base.plane = S.plane;
+    base.cnt = S.cnt;
+    base.code = S.d_code;
+    base.ncode = S.codeM;
+    base.inner = g.pw[j];
+    base.prob = g.prob;
+    base.R = g.R;
+    base.mu = g_mu;
+    base.src = j == 0 ? src : kSrcLayers;
+    // pipe 1 and 3 prefetch the cnt-reading first group; 3 also the last
+    // group when it writes the 4-byte map (reads every layer, writes one
+    // plane), decided below; 2 prefetches every group
+    base.pipe = kid >= 0 && base.src != kSrcCode &&
+                (kn.pipe == 2 || ((kn.pipe == 1 || kn.pipe == 3) &&
+                                  base.src == kSrcCnt));
+    // the most axes that fit one tile of W inner words
+    auto grow = [&](int W) {
+      GroupArgs a = base;
+      a.W = W;
+      long long mid = 1;
+      for (;;) {
+        if (j + a.k >= g.n || a.k >= kMaxRounds) break;
+        const int qn = g.ax[j + a.k];
+        if (kid >= 0 && qn != q) break;
+        if (kid < 0 && qn > 16) break;
+        const long long mid2 = mid * qn;
+        GroupArgs t = a;
+        t.k = a.k + 1;
+        t.mid = (int)std::min<long long>(mid2, INT_MAX / 64);
+        const long long outer = g.space / (a.inner * mid2);
+        t.Bo = W >= 16 ? 1
+               : (int)std::max<long long>(1, std::min<long long>(
+                     outer, 2048 / (W * mid2)));
+        t.skew = 0;
+        if (kid >= 0 && W == 1 && (q & (q - 1)) == 0) {
+          int lg = 0;
+          while ((1 << lg) < ipow(q, bm)) lg++;
+          t.skew = lg;
+        }
+        const bool fits = group_smem_bytes(t, R1) <= budget &&
+                          mid2 < (1 << 24);
+        if (a.k > 0 && !fits) break;
+        a = t;
+        mid = mid2;
       }
-      const size_t sm = group_smem_bytes(t, R1);
-      const int th = threads_for(t, kid, bm, q);
-      const long long words = (long long)t.W * t.mid * t.Bo;
-      const bool fits = sm <= budget && mid2 < (1 << 24) &&
-                        (kid < 0 ||
-                         words / ipow(q, std::min(bm, t.k)) <= kGroupThreads);
-      if (k > 0 && !fits) break;
-      a.k = t.k; a.mid = t.mid; a.Bo = t.Bo; a.skew = t.skew;
-      (void)th;
-      mid = mid2;
-      k++;
+      return a;
+    };
+    GroupArgs a;
+    if (base.inner >= 32) {
+      // 128-byte rows, or 64-byte rows when that fits more axes
+      a = grow(32);
+      GroupArgs b16 = grow(16);
+      if (b16.k > a.k) a = b16;
+    } else {
+      a = grow((int)base.inner);
     }
     a.outer = g.space / (a.inner * (long long)a.mid);
     a.nchunk = (a.inner + a.W - 1) / a.W;
@@ -378,9 +410,15 @@ Plan build_group_plan(int src, int dst) {
     for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j + t];
     if (kid >= 0) set_rounds(a, q, bm);
     else a.nrounds = 0;
-    const bool first = j == 0, last = j + a.k == g.n;
-    a.src = first ? src : kSrcLayers;
+    const bool last = j + a.k == g.n;
     a.dst = last ? dst : kDstLayers;
+    if (kn.pipe == 3 && kid >= 0 && last && dst != kDstLayers &&
+        a.src == kSrcLayers) {
+      // read-heavy last group: prefetch its tiles too (if they still fit)
+      GroupArgs t = a;
+      t.pipe = 1;
+      if (group_smem_bytes(t, R1) <= budget) a.pipe = 1;
+    }
     a.lin = layered ? live_layers(j) : 1;
     a.lout = layered ? live_layers(j + a.k) : 1;
     if (last && dst == kDstLayers) a.lout = R1;   // every layer, zeros too
@@ -438,15 +476,19 @@ Plan build_window_plan(int init_mode, int out_mode) {
   return P;
 }
 
+Plan make_plan(int init_mode, int out_mode, Knobs kn) {
+  const int src = init_mode == 0 ? kSrcCode : kSrcCnt;
+  const int dst = out_mode == 1 ? kDstMap
+                  : out_mode == 2 ? kDstCnt : kDstLayers;
+  if ((S.g.prob == kTorus || S.g.prob == kGrid) && any_wide_axis())
+    return build_window_plan(init_mode, out_mode);
+  return build_group_plan(src, dst, kn);
+}
+
 Plan &plan_for(int init_mode, int out_mode) {
   if (!S.plan_ok[init_mode][out_mode]) {
-    const int src = init_mode == 0 ? kSrcCode : kSrcCnt;
-    const int dst = out_mode == 1 ? kDstMap
-                    : out_mode == 2 ? kDstCnt : kDstLayers;
-    if ((S.g.prob == kTorus || S.g.prob == kGrid) && any_wide_axis())
-      S.plans[init_mode][out_mode] = build_window_plan(init_mode, out_mode);
-    else
-      S.plans[init_mode][out_mode] = build_group_plan(src, dst);
+    S.plans[init_mode][out_mode] = make_plan(init_mode, out_mode,
+                                             default_knobs());
     S.plan_ok[init_mode][out_mode] = true;
   }
   return S.plans[init_mode][out_mode];
@@ -484,6 +526,20 @@ int run_transform(int init_mode, int out_mode) {
       if ((rc = timing_mark(++nt))) return rc;
     }
   } else {
+    if (init_mode == 0) {
+      const GroupArgs &a0 = P.groups[0].a;
+      const long long need = a0.ntiles + 1;
+      if (need > S.bounds_cap) {
+        if (S.d_bounds) cudaFree(S.d_bounds);
+        S.d_bounds = nullptr;
+        CC_CK(cudaMalloc(&S.d_bounds, (size_t)need * 8));
+        S.bounds_cap = need;
+      }
+      rc = launch_code_bounds(S.d_code, S.codeM,
+                              (long long)a0.Bo * a0.mid, a0.ntiles,
+                              S.d_bounds, g_stream);
+      if (rc) return rc;
+    }
     if ((rc = timing_mark(nt))) return rc;
     for (auto &gp : P.groups) {
       GroupPlan p = gp;
@@ -492,6 +548,7 @@ int run_transform(int init_mode, int out_mode) {
       p.a.mu = g_mu;
       p.a.code = S.d_code;
       p.a.ncode = S.codeM;
+      p.a.code_bounds = S.d_bounds;
       if ((rc = launch_group(p, g_stream))) return rc;
       if ((rc = timing_mark(++nt))) return rc;
     }
@@ -508,6 +565,51 @@ int run_transform(int init_mode, int out_mode) {
         fprintf(stderr, "DCT_TIMING transform(%d,%d) launch %d: %.4f ms\n",
                 init_mode, out_mode, i, g_last_ms[i]);
   }
+  return 0;
+}
+
+// Autotuner: on the first transform of a kind on a large cell, time each
+// candidate schedule twice (CUDA events on the engine stream) and keep the
+// fastest plan.  Every schedule computes the same integers, so tuning runs
+// are ordinary transforms.  CC_TUNE=0 turns it off; explicit CC_PIPE /
+// CC_SMEM_BUDGET_KB settings also pin the schedule.
+int autotune(int init_mode, int out_mode) {
+  if (S.tuned[init_mode][out_mode]) return 0;
+  S.tuned[init_mode][out_mode] = true;
+  const char *te = getenv("CC_TUNE");
+  if ((te && atoi(te) == 0) || getenv("CC_PIPE") ||
+      getenv("CC_SMEM_BUDGET_KB") || S.g.space < (1LL << 22) ||
+      ((S.g.prob == kTorus || S.g.prob == kGrid) && any_wide_axis()))
+    return 0;
+  static const Knobs cands[] = {{100 << 10, 1}, {160 << 10, 1},
+                                {64 << 10, 1}, {200 << 10, 1},
+                                {100 << 10, 2}, {100 << 10, 3},
+                                {200 << 10, 3}};
+  cudaEvent_t e0, e1;
+  CC_CK(cudaEventCreate(&e0));
+  CC_CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  Plan keep;
+  for (const Knobs &kn : cands) {
+    S.plans[init_mode][out_mode] = make_plan(init_mode, out_mode, kn);
+    S.plan_ok[init_mode][out_mode] = true;
+    int rc = run_transform(init_mode, out_mode);      // warm
+    if (rc) return rc;
+    CC_CK(cudaEventRecord(e0, g_stream));
+    for (int r = 0; r < 2; r++) {
+      rc = run_transform(init_mode, out_mode);
+      if (rc) return rc;
+    }
+    CC_CK(cudaEventRecord(e1, g_stream));
+    CC_CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CC_CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) { best = ms; keep = S.plans[init_mode][out_mode]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  S.plans[init_mode][out_mode] = keep;
+  S.tune_ms[init_mode][out_mode] = best / 2;
   return 0;
 }
 
@@ -818,7 +920,9 @@ int dct_transform(int init_mode, int out_mode) {
       (out_mode == 2 && init_mode != 0))
     return -1;
   if (out_mode == 3 && S.R1 == 1) return -1;
-  int rc = run_transform(init_mode, out_mode);
+  int rc = autotune(init_mode, out_mode);
+  if (rc) return rc;
+  rc = run_transform(init_mode, out_mode);
   if (rc) return rc;
   CC_CK(cudaStreamSynchronize(g_stream));
   S.layered_out = out_mode == 3;

@@ -24,6 +24,7 @@
 //
 // Integer arithmetic is exactly the reference's, so every field is bit-exact.
 #include <algorithm>
+#include <cstdlib>
 
 #include "engine.h"
 
@@ -37,25 +38,37 @@ struct IPow<Q, 0> { static constexpr int v = 1; };
 enum Op { kOpHamming = 0, kOpLee = 1, kOpTorus = 2, kOpGrid = 3 };
 
 // ---------------------------------------------------------------- axis ops
-// Hamming: newA_d[a] = A_d[a] + T_{d-1} - A_{d-1}[a], T = fibre sum
+// Hamming: newA_d[a] = A_d[a] + T_{d-1} - A_{d-1}[a], T = fibre sum.
+// T_{d-1} - A_{d-1}[a] is the sum of the fibre's OTHER entries of layer
+// d-1, which is how it is formed here: one add per entry for Q = 2, two for
+// Q = 3, and T minus the entry above.  Descending d reads layer d-1 before
+// it is rewritten, so every term is the old value, as in the recurrence.
 template <int Q, int R1, int QB, int ST>
 __device__ __forceinline__ void axis_hamming(int32_t (&v)[R1][QB]) {
 #pragma unroll
   for (int e = 0; e < QB; e++) {
     if ((e / ST) % Q != 0) continue;
-    int32_t T[R1];
 #pragma unroll
-    for (int d = 0; d + 1 < R1; d++) {
-      int32_t s = 0;
+    for (int d = R1 - 1; d >= 1; d--) {
+      if (Q == 2) {
+        const int32_t a0 = v[d - 1][e], a1 = v[d - 1][e + ST];
+        v[d][e] += a1;
+        v[d][e + ST] += a0;
+      } else if (Q == 3) {
+        const int32_t a0 = v[d - 1][e], a1 = v[d - 1][e + ST],
+                      a2 = v[d - 1][e + 2 * ST];
+        v[d][e] += a1 + a2;
+        v[d][e + ST] += a0 + a2;
+        v[d][e + 2 * ST] += a0 + a1;
+      } else {
+        int32_t T = 0;
 #pragma unroll
-      for (int a = 0; a < Q; a++) s += v[d][e + a * ST];
-      T[d] = s;
+        for (int a = 0; a < Q; a++) T += v[d - 1][e + a * ST];
+#pragma unroll
+        for (int a = 0; a < Q; a++)
+          v[d][e + a * ST] += T - v[d - 1][e + a * ST];
+      }
     }
-#pragma unroll
-    for (int d = R1 - 1; d >= 1; d--)
-#pragma unroll
-      for (int a = 0; a < Q; a++)
-        v[d][e + a * ST] += T[d - 1] - v[d - 1][e + a * ST];
   }
 }
 
@@ -69,20 +82,17 @@ __device__ __forceinline__ void axis_lee(int32_t (&v)[R1][QB]) {
     if ((e / ST) % Q != 0) continue;
 #pragma unroll
     for (int d = R1 - 1; d >= 1; d--) {
-      int32_t nv[Q];
 #pragma unroll
       for (int a = 0; a < Q; a++) {
-        int32_t s = v[d][e + a * ST];
+        int32_t s = 0;
 #pragma unroll
         for (int w = 1; w <= (d < H ? d : H); w++) {
           const int am = (a - w + Q) % Q, ap = (a + w) % Q;
           s += v[d - w][e + am * ST];
           if (ap != am) s += v[d - w][e + ap * ST];
         }
-        nv[a] = s;
+        v[d][e + a * ST] += s;       // only lower layers are read
       }
-#pragma unroll
-      for (int a = 0; a < Q; a++) v[d][e + a * ST] = nv[a];
     }
   }
 }
@@ -136,125 +146,360 @@ __device__ __forceinline__ int skewed(int p, int skew) {
   return skew ? p + (p >> skew) : p;
 }
 
-// Fill layer 0 of the tile (shared memory) with the code multiplicities
-// of the contiguous range [x0, x0 + len); other layers are implicit zeros.
+// Fill layer 0 of tile `tile` (shared memory) with the code multiplicities
+// of its contiguous range [x0, x0 + len); other layers are implicit zeros.
+// The tile's slice of the sorted code is code[bounds[tile], bounds[tile+1])
+// (k_code_bounds, one binary search per tile boundary).
 __device__ __forceinline__ void stage_code(const GroupArgs &g, int32_t *sm,
-                                           long long x0, int len) {
-  __shared__ long long s_lo, s_hi;
+                                           long long tile, long long x0,
+                                           int len) {
   for (int p = threadIdx.x; p < len; p += blockDim.x)
     sm[skewed(p, g.skew)] = 0;
-  if (threadIdx.x == 0) {
-    long long lo = 0, hi = g.ncode;     // lower_bound(x0)
-    while (lo < hi) {
-      long long md = (lo + hi) >> 1;
-      if (g.code[md] < x0) lo = md + 1; else hi = md;
-    }
-    long long a = lo;
-    hi = g.ncode;                       // lower_bound(x0 + len)
-    while (lo < hi) {
-      long long md = (lo + hi) >> 1;
-      if (g.code[md] < x0 + len) lo = md + 1; else hi = md;
-    }
-    s_lo = a;
-    s_hi = lo;
-  }
   __syncthreads();
-  for (long long t = s_lo + threadIdx.x; t < s_hi; t += blockDim.x)
+  const long long lo = g.code_bounds[tile], hi = g.code_bounds[tile + 1];
+  for (long long t = lo + threadIdx.x; t < hi; t += blockDim.x)
     atomicAdd(&sm[skewed((int)(g.code[t] - x0), g.skew)], 1);
   __syncthreads();
 }
 
+// bounds[t] = lower_bound(code, t * tile_words) for t = 0..ntiles
+__global__ void k_code_bounds(const long long *code, long long ncode,
+                              long long tile_words, long long ntiles,
+                              long long *bounds) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles) return;
+  const long long x = t * tile_words;
+  long long lo = 0, hi = ncode;
+  while (lo < hi) {
+    const long long md = (lo + hi) >> 1;
+    if (code[md] < x) lo = md + 1; else hi = md;
+  }
+  bounds[t] = lo;
+}
+
+int launch_code_bounds(const long long *code, long long ncode,
+                       long long tile_words, long long ntiles,
+                       long long *bounds, cudaStream_t s) {
+  k_code_bounds<<<(unsigned)((ntiles + 1 + 255) / 256), 256, 0, s>>>(
+      code, ncode, tile_words, ntiles, bounds);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
 // ------------------------------------------------------------------ kernel
+// Where a round's block comes from and goes to: the first round reads HBM
+// (layers, the cnt predicate) or the staged code, the last writes HBM
+// (layers, map, cnt); every other side is shared memory.
+enum RoundIo { kIoSmem = 0, kIoLayers = 1, kIoCnt = 2, kIoCode = 3,
+               kIoMap = 4, kIoCntOut = 5, kIoCntSmem = 6 };
+
+// One round over the whole tile: every thread takes register blocks of
+// ne = Q^rb words (all layers), rb of the group's axes at local stride S.
+// FULL: rb == BM (no per-word bound checks).  Addresses step linearly with
+// the block word e: in HBM by S*inner words, in shared memory by sstep —
+// the skew (one pad word per 2^skew) keeps that linear, because a round's
+// stride S is 1 or a multiple of 2^skew and S == 1 blocks start on a
+// multiple of 2^skew.
+template <int OP, int Q, int R1, int BM, bool FULL>
+__device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
+                                          int SD, long long o0, long long i0,
+                                          int rb, int S, int src, int dst,
+                                          int nl = R1,
+                                          const uint16_t *cs = nullptr) {
+  constexpr int QB = IPow<Q, BM>::v;
+  int ne = QB;
+  if (!FULL) { ne = 1; for (int t = 0; t < rb; t++) ne *= Q; }
+  const int W = g.W;
+  const int nh = g.mid / (S * ne);
+  const int nblk = W * S * nh * g.Bo;
+  const long long imid = g.inner * (long long)g.mid;
+  const long long gstep = (long long)S * g.inner;      // HBM word step of e
+  const int sstep = g.skew == 0 ? S * W
+                    : (S == 1 ? W : (S + (S >> g.skew)) * W);
+  // predicate as a range: lo <= cnt <= hi
+  const int plo = g.pmode == kPredDef ? 0 : g.pmode == kPredCrit ? 1
+                  : g.ptarget;
+  const int phi = g.pmode == kPredDef ? g.mu - 1 : g.pmode == kPredCrit
+                  ? g.mu : g.ptarget;
+  const unsigned pspan = (unsigned)(phi - plo);
+  for (int blk = threadIdx.x; blk < nblk; blk += blockDim.x) {
+    const int w = blk % W;
+    int rest = blk / W;
+    const int mlo = rest % S;
+    rest /= S;
+    const int mhi = rest % nh;
+    const int ob = rest / nh;
+    const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
+    const int pb = ob * g.mid + mlo + S * ne * mhi;      // tile word, e = 0
+    const int sp0 = skewed(pb, g.skew) * W + w;
+    const long long xb = (o0 + ob) * imid + (long long)(mlo + S * ne * mhi)
+                         * g.inner + i0 + w;
+    int32_t v[R1][QB];
+#pragma unroll
+    for (int d = 0; d < R1; d++)
+#pragma unroll
+      for (int e = 0; e < QB; e++) v[d][e] = 0;
+    // -------- load
+    if (src == kIoCntSmem) {                     // prefetched cnt window
+      const uint16_t *p = cs + pb;
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        if (!FULL && e >= ne) break;
+        v[0][e] = (unsigned)((int)p[e * S] - plo) <= pspan;
+      }
+    } else if (src == kIoSmem || src == kIoCode) {
+      if (src == kIoCode) nl = 1;
+#pragma unroll
+      for (int d = 0; d < R1; d++) {
+        if (d >= nl) break;
+        const int32_t *p = sm + d * SD + sp0;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          v[d][e] = p[e * sstep];
+        }
+      }
+    } else if (valid) {
+      if (src == kIoLayers) {
+#pragma unroll
+        for (int d = 0; d < R1; d++) {
+          if (d >= g.lin) break;
+          const int32_t *p = g.layers + d * g.plane + xb;
+#pragma unroll
+          for (int e = 0; e < QB; e++) {
+            if (!FULL && e >= ne) break;
+            v[d][e] = __ldcs(p);
+            p += gstep;
+          }
+        }
+      } else {                                   // kIoCnt
+        const uint16_t *p = g.cnt + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          v[0][e] = (unsigned)((int)__ldcs(p) - plo) <= pspan;
+          p += gstep;
+        }
+      }
+    }
+    // -------- rb axis recurrences in registers
+    if (FULL) AxisLoop<OP, Q, R1, BM, 0>::run(v, BM, g.R);
+    else AxisLoop<OP, Q, R1, BM, 0>::run(v, rb, g.R);
+    // -------- store
+    if (dst == kIoSmem) {
+#pragma unroll
+      for (int d = 0; d < R1; d++) {
+        int32_t *p = sm + d * SD + sp0;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          p[e * sstep] = v[d][e];
+        }
+      }
+    } else if (valid) {
+      if (dst == kIoLayers) {
+#pragma unroll
+        for (int d = 0; d < R1; d++) {
+          if (d >= g.lout) break;
+          int32_t *p = g.layers + d * g.plane + xb;
+#pragma unroll
+          for (int e = 0; e < QB; e++) {
+            if (!FULL && e >= ne) break;
+            __stcs(p, v[d][e]);
+            p += gstep;
+          }
+        }
+      } else if (dst == kIoMap) {
+        int32_t *p = g.layers + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          int32_t s = 0;
+#pragma unroll
+          for (int d = 0; d < R1; d++) s += v[d][e];
+          __stcs(p, s);
+          p += gstep;
+        }
+      } else {
+        uint16_t *p = g.cnt + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          int32_t s = 0;
+#pragma unroll
+          for (int d = 0; d < R1; d++) s += v[d][e];
+          *p = (uint16_t)(s > 65535 ? 65535 : s);
+          p += gstep;
+        }
+      }
+    }
+  }
+}
+
 template <int OP, int Q, int R1, int BM>
 __global__ void __launch_bounds__(kGroupThreads)
 group_kernel(const GroupArgs g) {
-  constexpr int QB = IPow<Q, BM>::v;
   extern __shared__ int32_t sm[];
-  const long long imid = g.inner * (long long)g.mid;
   const int W = g.W;
   const int tile_words = g.Bo * g.mid;
   const int SD = (skewed(tile_words, g.skew) + 1) * W;   // layer stride
+  const int first_src = g.src == kSrcLayers ? kIoLayers
+                        : g.src == kSrcCnt ? kIoCnt : kIoCode;
+  const int last_dst = g.dst == kDstLayers ? kIoLayers
+                       : g.dst == kDstMap ? kIoMap : kIoCntOut;
   for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
     const long long o0 = (tile / g.nchunk) * g.Bo;
     const long long i0 = (tile % g.nchunk) * W;
     if (g.src == kSrcCode) {
       // first group only: W == 1, inner == 1, the tile is contiguous
       long long len = (g.outer - o0) * (long long)g.mid;
-      stage_code(g, sm, o0 * g.mid, (int)(len < tile_words ? len : tile_words));
+      stage_code(g, sm, tile, o0 * g.mid,
+                 (int)(len < tile_words ? len : tile_words));
     }
     for (int r = 0; r < g.nrounds; r++) {
-      const int rb = g.rb[r], S = g.rs[r];
-      int ne = 1;
-      for (int t = 0; t < rb; t++) ne *= Q;
-      const int nh = g.mid / (S * ne);
-      const int nblk = W * S * nh * g.Bo;
-      const bool first = r == 0, last = r == g.nrounds - 1;
-      for (int blk = threadIdx.x; blk < nblk; blk += blockDim.x) {
-        const int w = blk % W;
-        int rest = blk / W;
-        const int mlo = rest % S;
-        rest /= S;
-        const int mhi = rest % nh;
-        const int ob = rest / nh;
-        const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
-        const long long xb = (o0 + ob) * imid + i0 + w;
-        const int pb = ob * g.mid + mlo + S * ne * mhi;   // tile word of e=0
-        int32_t v[R1][QB];
-        // -------- load
-#pragma unroll
-        for (int e = 0; e < QB; e++) {
-          const int m = mlo + S * e + S * ne * mhi;
-          const long long x = xb + (long long)m * g.inner;
-          const int sp = skewed(pb + S * e, g.skew) * W + w;
-#pragma unroll
-          for (int d = 0; d < R1; d++) v[d][e] = 0;
-          if (e >= ne) continue;
-          if (first && g.src == kSrcLayers) {
-            if (valid) {
-#pragma unroll
-              for (int d = 0; d < R1; d++)
-                if (d < g.lin) v[d][e] = g.layers[d * g.plane + x];
-            }
-          } else if (first && g.src == kSrcCnt) {
-            if (valid)
-              v[0][e] = cnt_pred(g.pmode, (int)g.cnt[x], g.ptarget, g.mu);
-          } else if (first) {                       // kSrcCode: layer 0 only
-            v[0][e] = sm[sp];
-          } else {
-#pragma unroll
-            for (int d = 0; d < R1; d++) v[d][e] = sm[d * SD + sp];
-          }
-        }
-        // -------- rb axis recurrences in registers
-        AxisLoop<OP, Q, R1, BM, 0>::run(v, rb, g.R);
-        // -------- store
-#pragma unroll
-        for (int e = 0; e < QB; e++) {
-          if (e >= ne) continue;
-          const int m = mlo + S * e + S * ne * mhi;
-          const long long x = xb + (long long)m * g.inner;
-          const int sp = skewed(pb + S * e, g.skew) * W + w;
-          if (!last) {
-#pragma unroll
-            for (int d = 0; d < R1; d++) sm[d * SD + sp] = v[d][e];
-          } else if (valid) {
-            if (g.dst == kDstLayers) {
-#pragma unroll
-              for (int d = 0; d < R1; d++)
-                if (d < g.lout) g.layers[d * g.plane + x] = v[d][e];
-            } else {
-              int32_t s = 0;
-#pragma unroll
-              for (int d = 0; d < R1; d++) s += v[d][e];
-              if (g.dst == kDstMap) g.layers[x] = s;
-              else g.cnt[x] = (uint16_t)(s > 65535 ? 65535 : s);
-            }
-          }
-        }
-      }
+      const int src = r == 0 ? first_src : kIoSmem;
+      const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
+      if (g.rb[r] == BM)
+        run_round<OP, Q, R1, BM, true>(g, sm, SD, o0, i0, BM, g.rs[r], src,
+                                       dst);
+      else
+        run_round<OP, Q, R1, BM, false>(g, sm, SD, o0, i0, g.rb[r], g.rs[r],
+                                        src, dst);
       __syncthreads();
     }
   }
+}
+
+// --------------------------------------------------------- pipelined kernel
+// The same rounds, with the next tile's input prefetched into a second
+// shared-memory buffer by cp.async while the current tile computes, so the
+// HBM reads of one tile overlap the register work and the HBM writes of the
+// previous one.  Layer sources copy (lin layers) x tile words, 16 bytes at a
+// time where the rows allow; a cnt source (the first group: a contiguous
+// range) copies the 16-byte-aligned window of 2-byte counters around it.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void cp_wait_prev() {
+  asm volatile("cp.async.wait_group 1;\n" ::);
+}
+__device__ __forceinline__ void cp_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+__device__ __forceinline__ void prefetch_layers(const GroupArgs &g,
+                                                int32_t *buf, int SD,
+                                                long long tile) {
+  const long long o0 = (tile / g.nchunk) * g.Bo;
+  const long long i0 = (tile % g.nchunk) * g.W;
+  const long long imid = g.inner * (long long)g.mid;
+  const int W = g.W, tw = g.Bo * g.mid;
+  if (W % 4 == 0 && g.inner % 4 == 0) {        // 16-byte rows of 4 words
+    const int W4 = W / 4, n = tw * W4;
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+      const int w = (idx % W4) * 4, p = idx / W4;
+      const int ob = p / g.mid, m = p % g.mid;
+      if (o0 + ob >= g.outer || i0 + w >= g.inner) continue;
+      const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
+      const int sp = skewed(p, g.skew) * W + w;
+      for (int d = 0; d < g.lin; d++)
+        cp_async16(buf + d * SD + sp, g.layers + d * g.plane + x);
+    }
+  } else {
+    const int n = tw * W;
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+      const int w = idx % W, p = idx / W;
+      const int ob = p / g.mid, m = p % g.mid;
+      if (o0 + ob >= g.outer || i0 + w >= g.inner) continue;
+      const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
+      const int sp = skewed(p, g.skew) * W + w;
+      for (int d = 0; d < g.lin; d++)
+        cp_async4(buf + d * SD + sp, g.layers + d * g.plane + x);
+    }
+  }
+}
+
+// first group (inner == 1): the tile is the contiguous range
+// [x0, x0 + len); copy the aligned 8-counter window around it and return
+// the offset of x0 inside the window
+__device__ __forceinline__ int prefetch_cnt(const GroupArgs &g, uint16_t *cs,
+                                            long long tile) {
+  const long long x0 = (tile / g.nchunk) * g.Bo * (long long)g.mid;
+  long long len = g.outer * (long long)g.mid - x0;
+  if (len > (long long)g.Bo * g.mid) len = (long long)g.Bo * g.mid;
+  const long long a0 = x0 & ~7LL, a1 = (x0 + len + 7) & ~7LL;
+  const int nch = (int)((a1 - a0) >> 3);
+  for (int c = threadIdx.x; c < nch; c += blockDim.x)
+    cp_async16(cs + 8 * c, g.cnt + a0 + 8 * c);
+  return (int)(x0 - a0);
+}
+
+template <int OP, int Q, int R1, int BM>
+__global__ void __launch_bounds__(kGroupThreads)
+group_kernel_pipe(const GroupArgs g) {
+  extern __shared__ __align__(16) int32_t sm[];
+  const int W = g.W;
+  const int tile_words = g.Bo * g.mid;
+  const int SD = (skewed(tile_words, g.skew) + 1) * W;   // layer stride
+  const bool from_cnt = g.src == kSrcCnt;
+  const int cbw = (tile_words + 16 + 7) & ~7;            // cnt window words
+  // every buffer starts on a 16-byte boundary (cp.async 16-byte copies)
+  const int lay_words = (R1 * SD + 3) & ~3;
+  int32_t *const buf0 = sm;
+  int32_t *const buf1 = from_cnt ? sm : sm + lay_words;
+  uint16_t *const cb0 = reinterpret_cast<uint16_t *>(sm + lay_words);
+  uint16_t *const cb1 = cb0 + cbw;
+  const int last_dst = g.dst == kDstLayers ? kIoLayers
+                       : g.dst == kDstMap ? kIoMap : kIoCntOut;
+  int off0 = 0, off1 = 0;
+  long long tile = blockIdx.x;
+  if (tile < g.ntiles) {
+    if (from_cnt) off0 = prefetch_cnt(g, cb0, tile);
+    else prefetch_layers(g, buf0, SD, tile);
+  }
+  cp_commit();
+  for (int i = 0; tile < g.ntiles; i++, tile += gridDim.x) {
+    const bool odd = i & 1;
+    const long long next = tile + gridDim.x;
+    if (next < g.ntiles) {
+      if (from_cnt) {
+        const int o = prefetch_cnt(g, odd ? cb0 : cb1, next);
+        if (odd) off0 = o; else off1 = o;
+      } else {
+        prefetch_layers(g, odd ? buf0 : buf1, SD, next);
+      }
+    }
+    cp_commit();
+    cp_wait_prev();                 // this thread's copies of `tile` landed
+    __syncthreads();                // ... and everyone else's
+    const long long o0 = (tile / g.nchunk) * g.Bo;
+    const long long i0 = (tile % g.nchunk) * W;
+    int32_t *buf = odd ? buf1 : buf0;
+    const uint16_t *cs = odd ? cb1 + off1 : cb0 + off0;
+    for (int r = 0; r < g.nrounds; r++) {
+      const int src = r > 0 ? kIoSmem : from_cnt ? kIoCntSmem : kIoSmem;
+      const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
+      const int nl = r > 0 ? R1 : g.lin;
+      if (g.rb[r] == BM)
+        run_round<OP, Q, R1, BM, true>(g, buf, SD, o0, i0, BM, g.rs[r], src,
+                                       dst, nl, cs);
+      else
+        run_round<OP, Q, R1, BM, false>(g, buf, SD, o0, i0, g.rb[r],
+                                        g.rs[r], src, dst, nl, cs);
+      __syncthreads();
+    }
+  }
+  cp_wait_all();
 }
 
 // ------------------------------------------------------------ generic kernel
@@ -275,7 +520,8 @@ __global__ void __launch_bounds__(512) group_generic(const GroupArgs g) {
     const long long i0 = (tile % g.nchunk) * W;
     if (g.src == kSrcCode) {
       long long len = (g.outer - o0) * (long long)g.mid;
-      stage_code(g, sm, o0 * g.mid, (int)(len < tile_words ? len : tile_words));
+      stage_code(g, sm, tile, o0 * g.mid,
+                 (int)(len < tile_words ? len : tile_words));
     }
     // -------- load the tile
     for (int t = threadIdx.x; t < nel; t += blockDim.x) {
@@ -377,17 +623,21 @@ __global__ void __launch_bounds__(512) group_generic(const GroupArgs g) {
 
 // ------------------------------------------------------------ dispatch table
 typedef void (*GroupFn)(const GroupArgs);
-struct KernelEntry { int op, q, r1, bm; GroupFn fn; };
+struct KernelEntry { int op, q, r1, bm; GroupFn fn, fn_pipe; };
 
-#define KE(OP, Q, R1, BM) {OP, Q, R1, BM, group_kernel<OP, Q, R1, BM>}
+#define KE(OP, Q, R1, BM)                                                   \
+  {OP, Q, R1, BM, group_kernel<OP, Q, R1, BM>,                              \
+   group_kernel_pipe<OP, Q, R1, BM>}
 static const KernelEntry kTable[] = {
     // Hamming, binary: 16-word blocks up to 4 layers, 8-word above
     KE(kOpHamming, 2, 2, 4), KE(kOpHamming, 2, 3, 4), KE(kOpHamming, 2, 4, 4),
+    KE(kOpHamming, 2, 4, 3),   // 8-word blocks: fewer registers per thread
     KE(kOpHamming, 2, 5, 3), KE(kOpHamming, 2, 6, 3), KE(kOpHamming, 2, 7, 3),
     KE(kOpHamming, 2, 8, 3),
-    // Hamming, ternary: 9-word blocks
+    // Hamming, ternary: 9-word blocks; 3-word blocks for wider CTAs
     KE(kOpHamming, 3, 2, 2), KE(kOpHamming, 3, 3, 2), KE(kOpHamming, 3, 4, 2),
     KE(kOpHamming, 3, 5, 2), KE(kOpHamming, 3, 6, 2), KE(kOpHamming, 3, 7, 2),
+    KE(kOpHamming, 3, 4, 1), KE(kOpHamming, 3, 5, 1),
     // Hamming, quaternary
     KE(kOpHamming, 4, 2, 2), KE(kOpHamming, 4, 3, 2), KE(kOpHamming, 4, 4, 2),
     KE(kOpHamming, 4, 5, 1),
@@ -408,8 +658,12 @@ static int op_of(int prob) {
 // Kernel id for a group whose axes all have size q; -1 = generic kernel.
 int pick_group_kernel(int prob, int q, int R1, int *bm) {
   const int op = op_of(prob);
+  // CC_BLOCK_AXES caps the axes of one register block (tuning)
+  const char *cap_env = getenv("CC_BLOCK_AXES");
+  const int cap = cap_env ? atoi(cap_env) : 99;
   for (int i = 0; i < kTableLen; i++)
-    if (kTable[i].op == op && kTable[i].q == q && kTable[i].r1 == R1) {
+    if (kTable[i].op == op && kTable[i].q == q && kTable[i].r1 == R1 &&
+        kTable[i].bm <= cap) {
       *bm = kTable[i].bm;
       return i;
     }
@@ -420,15 +674,21 @@ int pick_group_kernel(int prob, int q, int R1, int *bm) {
 size_t group_smem_bytes(const GroupArgs &a, int R1) {
   const int tile_words = a.Bo * a.mid;
   const int skw = a.skew ? tile_words + (tile_words >> a.skew) : tile_words;
-  return (size_t)(skw + 1) * a.W * R1 * sizeof(int32_t);
+  const size_t lay = (size_t)(skw + 1) * a.W * R1;          // words
+  const size_t tile = ((lay + 3) & ~(size_t)3) * sizeof(int32_t);
+  if (!a.pipe) return tile;
+  if (a.src == kSrcCnt)                     // one tile + two cnt windows
+    return tile + 2 * (size_t)((tile_words + 16 + 7) & ~7) * 2;
+  return 2 * tile;                          // two tiles
 }
 
 int launch_group(const GroupPlan &p, cudaStream_t s) {
-  GroupFn fn = p.kernel >= 0 ? kTable[p.kernel].fn : group_generic;
+  GroupFn fn = p.kernel < 0 ? group_generic
+               : p.a.pipe ? kTable[p.kernel].fn_pipe : kTable[p.kernel].fn;
   // opt in to the dynamic shared memory this launch needs (the per-block
   // limit counts the kernel's static shared memory too)
-  static size_t attr_set[64 + 1];
-  const int slot = p.kernel >= 0 ? p.kernel : 64;
+  static size_t attr_set[2 * 64 + 1];
+  const int slot = p.kernel < 0 ? 128 : p.kernel + (p.a.pipe ? 64 : 0);
   if (p.smem > 48 * 1024 && p.smem > attr_set[slot]) {
     CC_CK(cudaFuncSetAttribute((const void *)fn,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
