@@ -326,6 +326,60 @@ def measure_cell(cell, args, dist, timed=True):
         b.close()
 
 
+def measure_batch(args, dist):
+    """Batched campaign: 256 seeded cells of uneven size (q in 2..6, q^n
+    log-uniform in 10^3..10^7, R in 1..4, 80% Hamming / 20% Lee, codes
+    covering ~half of each space).  One step = every cell's recount,
+    deficit, gain map + max, loss map + max.  Persistent graph launch
+    against one launch per pass per cell (same engine)."""
+    import torch
+
+    from coldcore_b200.batch import BatchEngine
+    from coldcore_b200.workloads import batch_cells
+    cells = batch_cells(256, seed=7)
+    out = {}
+    with BatchEngine() as b:
+        for p, a, R, code in cells:
+            b.add(p, a, R, code)
+        t0 = time.perf_counter()
+        b.build(0)
+        out["build_s"] = round(time.perf_counter() - t0, 2)
+        out.update(b.info())
+        for mode, key in ((0, "persistent"), (1, "per_pass_launches")):
+            for _ in range(2):
+                b.run(mode)
+            torch.cuda.synchronize()
+            reps = max(3, args.steps // 4)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                b.run(mode)
+            dt = (time.perf_counter() - t0) / reps
+            out[key] = {"ms_per_step": round(1e3 * dt, 3),
+                        "instances_per_s": round(len(cells) / dt, 1)}
+    # the campaign as coldcore runs it: one singleton cell context per
+    # instance (init, code upload, three transforms, two scalars, free)
+    from coldcore_b200.gpu import GpuBackend
+    t0 = time.perf_counter()
+    for p, a, R, code in cells:
+        with GpuBackend(list(a), R, problem=p) as g:
+            g.recount(code)
+            g.uncovered()
+            g.gain_map()
+            g.map_max()
+            g.loss_map()
+            g.map_max()
+    dt = time.perf_counter() - t0
+    out["singleton_per_cell"] = {"ms_per_step": round(1e3 * dt, 3),
+                                 "instances_per_s": round(len(cells) / dt, 1)}
+    out["speedup"] = round(out["persistent"]["instances_per_s"]
+                           / out["per_pass_launches"]["instances_per_s"], 2)
+    out["speedup_vs_singleton"] = round(
+        out["persistent"]["instances_per_s"]
+        / out["singleton_per_cell"]["instances_per_s"], 2)
+    out["words"] = int(sum(int(np.prod(a)) for _, a, _, _ in cells))
+    return out
+
+
 def run_b200(args, dist):
     cell = CELLS[args.cell]
     res = measure_cell(cell, args, dist)
@@ -388,6 +442,8 @@ def run_b200(args, dist):
     }
     if also:
         line["also"] = also
+    if not args.no_batch:
+        line["batched"] = measure_batch(args, dist)
     print(json.dumps(line), flush=True)
 
 
@@ -400,6 +456,7 @@ def main():
     ap.add_argument("--cell", default=HEADLINE, choices=sorted(CELLS))
     ap.add_argument("--no-also", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

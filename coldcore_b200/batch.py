@@ -1,0 +1,121 @@
+"""Batched campaign engine: many independent cells, one persistent launch.
+
+The reference's campaign runs one process per cell (coldcore
+``src/coldcore/campaign.py:186-221``) because its plugin ABI is a
+per-process singleton.  ``BatchEngine`` holds many cells in one device
+arena and computes, for every cell, cnt from its code, the deficit
+(uncovered count at mu = 1), the gain map and its maximum and the loss map
+and its maximum, in one persistent kernel launch replayed from a CUDA graph
+(``dct_batch_*`` in ``include/coldcore_b200/plugin.h``).
+"""
+import ctypes
+
+import numpy as np
+
+from .gpu import _check, load_plugin
+from .patterns import PROBLEM_IDS
+
+_LL = ctypes.c_longlong
+
+
+def _bind(lib):
+    if getattr(lib, "_batch_bound", False):
+        return lib
+    I = ctypes.c_int
+    lib.dct_batch_create.restype = _LL
+    lib.dct_batch_create.argtypes = []
+    lib.dct_batch_add.restype = I
+    lib.dct_batch_add.argtypes = [_LL, I, I, ctypes.POINTER(I), I, I,
+                                  ctypes.POINTER(_LL), I]
+    lib.dct_batch_build.restype = I
+    lib.dct_batch_build.argtypes = [_LL, I]
+    lib.dct_batch_run.restype = I
+    lib.dct_batch_run.argtypes = [_LL, I]
+    lib.dct_batch_read.restype = I
+    lib.dct_batch_read.argtypes = [_LL, I, I, _LL, _LL, ctypes.c_void_p]
+    lib.dct_batch_scalars.restype = I
+    lib.dct_batch_scalars.argtypes = [_LL, ctypes.POINTER(_LL), I]
+    lib.dct_batch_info.restype = I
+    lib.dct_batch_info.argtypes = [_LL, ctypes.POINTER(_LL), I]
+    lib.dct_batch_free.restype = I
+    lib.dct_batch_free.argtypes = [_LL]
+    lib._batch_bound = True
+    return lib
+
+
+class BatchEngine:
+    """Cells are added, then ``build()`` allocates and schedules them (tile
+    size autotuned unless ``tile_kb`` is given); each ``run()`` recomputes
+    every cell's fields."""
+
+    def __init__(self, plugin_path=None):
+        self._lib = _bind(load_plugin(plugin_path))
+        self.h = int(self._lib.dct_batch_create())
+        if self.h <= 0:
+            raise RuntimeError("dct_batch_create failed")
+        self.cells = []
+
+    def add(self, problem, axes, R, code, mu=1):
+        axes = [int(a) for a in axes]
+        code = np.ascontiguousarray(np.atleast_1d(code), dtype=np.int64)
+        ax = (ctypes.c_int * len(axes))(*axes)
+        rc = self._lib.dct_batch_add(
+            self.h, PROBLEM_IDS[problem], len(axes), ax, int(R), int(mu),
+            code.ctypes.data_as(ctypes.POINTER(_LL)), len(code))
+        if rc < 0:
+            _check("batch_add", rc)
+        self.cells.append((problem, tuple(axes), int(R), int(mu)))
+        return rc
+
+    def build(self, tile_kb=0):
+        _check("batch_build", self._lib.dct_batch_build(self.h, int(tile_kb)))
+
+    def run(self, mode=0):
+        _check("batch_run", self._lib.dct_batch_run(self.h, int(mode)))
+
+    def run_rc(self, mode):
+        return int(self._lib.dct_batch_run(self.h, int(mode)))
+
+    def read(self, cell, field):
+        size = int(np.prod(self.cells[cell][1]))
+        out = np.empty(size, dtype=np.uint16 if field == 0 else np.int32)
+        _check("batch_read", self._lib.dct_batch_read(
+            self.h, int(cell), int(field), 0, size,
+            out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def cnt(self, cell):
+        return self.read(cell, 0)
+
+    def gain(self, cell):
+        return self.read(cell, 1)
+
+    def loss(self, cell):
+        return self.read(cell, 2)
+
+    def scalars(self):
+        """(cells, 3) int64: deficit, gain maximum, loss maximum."""
+        buf = np.zeros(3 * len(self.cells), dtype=np.int64)
+        n = self._lib.dct_batch_scalars(
+            self.h, buf.ctypes.data_as(ctypes.POINTER(_LL)), len(buf))
+        if n < 0:
+            _check("batch_scalars", n)
+        return buf.reshape(-1, 3)
+
+    def info(self):
+        buf = (_LL * 6)()
+        _check("batch_info", 0 if self._lib.dct_batch_info(self.h, buf, 6) == 6
+               else -1)
+        keys = ("cells", "passes", "items", "tile_kb", "grid", "tuned_us")
+        return {k: int(v) for k, v in zip(keys, buf)}
+
+    def close(self):
+        if self.h > 0:
+            self._lib.dct_batch_free(self.h)
+            self.h = 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,647 @@
+// batch.cu — the batched campaign engine: many independent cells (Hamming,
+// Lee, torus, grid; any sizes) resident at once, and their count, gain and
+// loss transforms run as ONE persistent launch captured in a CUDA graph.
+//
+// The reference runs a campaign as one process per cell, each with its own
+// singleton plugin context (coldcore src/coldcore/campaign.py:186-221,
+// src/include/coldcore/plugin.h:8-10), so every cell pays its own context,
+// allocations and per-axis launches.  Here a batch owns one device arena;
+// each cell's transforms are split into passes (one per axis group) and
+// passes into tiles, and the whole step — for every cell: recount from its
+// code, the uncovered/deficit count, gain map + maximum, loss map + maximum
+// — is one launch of batch_kernel (transform_group.cu) over a level-ordered
+// work table.  Handles, not the v1 singleton: batches never touch the
+// dct_* cell.
+//
+// Tile size is the one schedule knob (shared memory per tile); the
+// autotuner times a few and keeps the fastest.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/coldcore_b200/plugin.h"
+#include "engine.h"
+
+using namespace cc;
+
+namespace {
+
+struct Cell {
+  Geometry g;
+  int R1 = 1;
+  long long plane = 0;
+  std::vector<long long> code;       // sorted
+  // device pointers into the arena
+  int32_t *layers = nullptr, *gain = nullptr, *loss = nullptr;
+  uint16_t *cnt = nullptr;
+  long long *dcode = nullptr, *bounds = nullptr;
+  long long nbounds = 0;
+  int first_pass = 0, npass = 0;     // global pass range (small cells)
+  bool big = false;                  // own register-blocked launches
+  std::vector<GroupPlan> fast[3];    // recount, gain, loss (big cells)
+};
+
+// Cells of at least 2^16 words whose axes all have one size with a
+// register-blocked kernel run as their own launches (captured on forked
+// streams of the same graph); smaller cells share the persistent kernel.
+constexpr long long kBigCell = 1LL << 16;
+constexpr long long kItemWords = 32768;   // words per work item (at least)
+constexpr int kSideStreams = 4;
+
+struct Batch {
+  std::vector<Cell> cells;
+  bool built = false;
+  char *arena = nullptr;
+  size_t arena_bytes = 0;
+  std::vector<GroupArgs> passes;
+  std::vector<int> dep;
+  std::vector<unsigned> need;
+  GroupArgs *d_passes = nullptr;
+  int *d_dep = nullptr;
+  unsigned *d_need = nullptr;
+  int4 *d_items = nullptr;
+  long long nitems = 0;
+  unsigned *d_done = nullptr;
+  unsigned long long *d_next = nullptr;
+  int *d_err = nullptr;
+  long long *d_scal = nullptr;       // per cell: deficit, gain max, loss max
+  long long *d_bounds = nullptr;     // per-tile code slices of every cell
+  long long bounds_cap = 0;
+  size_t tile_budget = 48 * 1024;
+  size_t smem = 0;
+  int grid = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t side[kSideStreams] = {nullptr};
+  cudaEvent_t fork = nullptr, join[kSideStreams] = {nullptr};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  float tuned_ms = 0;
+};
+
+std::unordered_map<long long, Batch *> g_batches;
+long long g_next_handle = 1;
+
+Batch *get(long long h) {
+  auto it = g_batches.find(h);
+  return it == g_batches.end() ? nullptr : it->second;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Groups of consecutive axes whose tile fits `budget` bytes of shared
+// memory (runtime-size tile kernel: any axis size up to 16).
+std::vector<GroupArgs> plan_cell(const Cell &c, size_t budget) {
+  std::vector<GroupArgs> out;
+  const Geometry &g = c.g;
+  long long reach = 0;
+  int j = 0;
+  while (j < g.n) {
+    GroupArgs a{};
+    a.layers = c.layers;
+    a.plane = c.plane;
+    a.cnt = c.cnt;
+    a.inner = g.pw[j];
+    a.W = a.inner >= 32 ? 32 : (int)a.inner;
+    a.prob = g.prob;
+    a.R = g.R;
+    a.mu = g.mu;
+    long long mid = 1;
+    while (j + a.k < g.n && a.k < kMaxRounds) {
+      GroupArgs t = a;
+      const long long mid2 = mid * g.ax[j + a.k];
+      const long long outer = g.space / (a.inner * mid2);
+      t.k = a.k + 1;
+      t.mid = (int)mid2;
+      t.Bo = a.W >= 32 ? 1
+             : (int)std::max<long long>(1, std::min<long long>(
+                   outer, 1024 / (a.W * mid2)));
+      if (a.k > 0 && group_smem_bytes(t, c.R1) > budget) break;
+      a = t;
+      mid = mid2;
+    }
+    for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j + t];
+    a.outer = g.space / (a.inner * (long long)a.mid);
+    a.nchunk = (a.inner + a.W - 1) / a.W;
+    a.ntiles = (a.outer + a.Bo - 1) / a.Bo * a.nchunk;
+    long long reach2 = reach;
+    for (int t = 0; t < a.k; t++)
+      reach2 += g.prob == kLee ? g.ax[j + t] / 2 : 1;
+    const bool layered = c.R1 > 1;
+    a.lin = layered ? (int)std::min<long long>(reach, g.R) + 1 : 1;
+    a.lout = layered ? (int)std::min<long long>(reach2, g.R) + 1 : 1;
+    out.push_back(a);
+    reach = reach2;
+    j += a.k;
+  }
+  return out;
+}
+
+// |B| of the metric ball (the most words one codeword covers): the
+// coefficient sum up to R of prod_j (per-axis weight enumerator) for the
+// sum metrics, prod_j min(2R+1, a_j) for the L-infinity families
+long long ball_cardinality(const Geometry &g) {
+  if (g.prob == kTorus || g.prob == kGrid) {
+    long long b = 1;
+    for (int j = 0; j < g.n; j++) b *= std::min(2 * g.R + 1, g.ax[j]);
+    return b;
+  }
+  std::vector<long long> poly(g.R + 1, 0);
+  poly[0] = 1;
+  for (int j = 0; j < g.n; j++) {
+    std::vector<long long> nx(g.R + 1, 0);
+    const int a = g.ax[j];
+    for (int w = 0; w <= g.R; w++) {
+      if (!poly[w]) continue;
+      for (int d = 0; d < a; d++) {
+        const int c = d < a - d ? d : a - d;       // circular weight
+        const int e = g.prob == kHamming ? (d ? 1 : 0) : c;
+        if (w + e <= g.R) nx[w + e] += poly[w];
+      }
+    }
+    poly = nx;
+  }
+  long long t = 0;
+  for (long long v : poly) t += v;
+  return t;
+}
+
+void release(Batch *b) {
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  auto F = [](void *p) { if (p) cudaFree(p); };
+  F(b->arena); F(b->d_passes); F(b->d_dep); F(b->d_need); F(b->d_items);
+  F(b->d_done); F(b->d_next); F(b->d_err); F(b->d_scal); F(b->d_bounds);
+  b->d_bounds = nullptr;
+  b->bounds_cap = 0;
+  b->arena = nullptr; b->d_passes = nullptr; b->d_dep = nullptr;
+  b->d_need = nullptr; b->d_items = nullptr; b->d_done = nullptr;
+  b->d_next = nullptr; b->d_err = nullptr; b->d_scal = nullptr;
+  b->built = false;
+}
+
+// passes + level-ordered work table for the current tile budget
+int make_schedule(Batch *b) {
+  b->passes.clear();
+  b->dep.clear();
+  b->need.clear();
+  std::vector<std::vector<int>> by_level;
+  size_t smem = 0;
+  for (size_t i = 0; i < b->cells.size(); i++) {
+    Cell &c = b->cells[i];
+    c.first_pass = (int)b->passes.size();
+    c.npass = 0;
+    if (c.big) {
+      const Knobs kn{100 * 1024, 1};
+      for (int t = 0; t < 3; t++) {
+        PlanPtrs ptr{c.layers, c.plane, c.cnt, c.dcode,
+                     (long long)c.code.size(), t == 1 ? c.gain : c.loss};
+        const int src = t == 0 ? kSrcCode : kSrcCnt;
+        const int dst = t == 0 ? kDstCnt : kDstMap;
+        c.fast[t] = plan_groups(c.g, c.R1, ptr, src, dst, kn);
+        for (auto &gp : c.fast[t]) {
+          if (prepare_group(gp)) return -1;
+          gp.a.pmode = kPredEq;
+          gp.a.ptarget = t == 1 ? 0 : 1;
+          if (c.g.mu > 1) gp.a.pmode = t == 1 ? kPredDef : kPredCrit;
+        }
+      }
+      continue;
+    }
+    const std::vector<GroupArgs> groups = plan_cell(c, b->tile_budget);
+    const int G = (int)groups.size();
+    for (int t = 0; t < 3; t++) {            // recount, gain, loss
+      for (int k = 0; k < G; k++) {
+        GroupArgs a = groups[k];
+        const bool first = k == 0, last = k == G - 1;
+        a.src = !first ? kSrcLayers : t == 0 ? kSrcCode : kSrcCnt;
+        a.dst = !last ? kDstLayers : t == 0 ? kDstCnt : kDstMap;
+        a.code = c.dcode;
+        a.ncode = (long long)c.code.size();
+        a.code_bounds = c.bounds;
+        a.pmode = kPredEq;
+        a.ptarget = t == 1 ? 0 : 1;
+        if (c.g.mu > 1) a.pmode = t == 1 ? kPredDef : kPredCrit;
+        a.map = t == 1 ? c.gain : c.loss;
+        a.red = b->d_scal + 3 * i + t;
+        a.red_mode = last ? (t == 0 ? 1 : 2) : 0;
+        const int pid = (int)b->passes.size();
+        b->passes.push_back(a);
+        b->dep.push_back(pid == c.first_pass ? -1 : pid - 1);
+        b->need.push_back((unsigned)a.ntiles);
+        const int level = pid - c.first_pass;
+        if ((int)by_level.size() <= level) by_level.resize(level + 1);
+        by_level[level].push_back(pid);
+        smem = std::max(smem, group_smem_bytes(a, c.R1));
+      }
+    }
+    c.npass = (int)b->passes.size() - c.first_pass;
+  }
+  // tile slices of each cell's code for this schedule's first groups
+  auto first_tiles = [&](const Cell &c) {
+    return c.big ? c.fast[0][0].a.ntiles : b->passes[c.first_pass].ntiles;
+  };
+  long long nb = 0;
+  for (const Cell &c : b->cells) nb += first_tiles(c) + 1;
+  if (nb > b->bounds_cap) {
+    if (b->d_bounds) cudaFree(b->d_bounds);
+    b->d_bounds = nullptr;
+    CC_CK(cudaMalloc(&b->d_bounds, (size_t)nb * 8));
+    b->bounds_cap = nb;
+  }
+  nb = 0;
+  for (Cell &c : b->cells) {
+    c.bounds = b->d_bounds + nb;
+    c.nbounds = first_tiles(c) + 1;
+    nb += c.nbounds;
+    for (int p = c.first_pass; p < c.first_pass + c.npass; p++)
+      b->passes[p].code_bounds = c.bounds;
+    if (c.big)
+      for (int t = 0; t < 3; t++)
+        for (auto &gp : c.fast[t]) gp.a.code_bounds = c.bounds;
+  }
+  std::vector<int4> items;
+  for (auto &lv : by_level) {
+    // largest passes first inside a level: long tails start early
+    std::stable_sort(lv.begin(), lv.end(), [&](int x, int y) {
+      return b->passes[x].ntiles > b->passes[y].ntiles;
+    });
+    for (int pid : lv) {
+      const GroupArgs &a = b->passes[pid];
+      const long long tw = (long long)a.Bo * a.mid * a.W;
+      const long long per = std::max<long long>(1, kItemWords / tw);
+      for (long long t = 0; t < a.ntiles; t += per)
+        items.push_back(make_int4(pid, (int)t,
+                                  (int)std::min<long long>(per, a.ntiles - t),
+                                  0));
+    }
+  }
+  b->nitems = (long long)items.size();
+  b->smem = smem;
+  b->grid = batch_grid(smem);
+  auto F = [](void *p) { if (p) cudaFree(p); };
+  F(b->d_passes); F(b->d_dep); F(b->d_need); F(b->d_items); F(b->d_done);
+  const size_t np = b->passes.size();
+  const size_t npa = std::max<size_t>(1, np);
+  CC_CK(cudaMalloc(&b->d_passes, npa * sizeof(GroupArgs)));
+  CC_CK(cudaMalloc(&b->d_dep, npa * sizeof(int)));
+  CC_CK(cudaMalloc(&b->d_need, npa * sizeof(unsigned)));
+  CC_CK(cudaMalloc(&b->d_done, npa * sizeof(unsigned)));
+  CC_CK(cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) *
+                                    sizeof(int4)));
+  if (np) {
+    CC_CK(cudaMemcpyAsync(b->d_passes, b->passes.data(),
+                          np * sizeof(GroupArgs), cudaMemcpyHostToDevice,
+                          b->stream));
+    CC_CK(cudaMemcpyAsync(b->d_dep, b->dep.data(), np * sizeof(int),
+                          cudaMemcpyHostToDevice, b->stream));
+    CC_CK(cudaMemcpyAsync(b->d_need, b->need.data(), np * sizeof(unsigned),
+                          cudaMemcpyHostToDevice, b->stream));
+  }
+  if (!items.empty())
+    CC_CK(cudaMemcpyAsync(b->d_items, items.data(), items.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+// one big cell's step on stream s: code bounds, recount, deficit, gain,
+// gain max, loss, loss max (register-blocked group kernels)
+int run_big_cell(Batch *b, size_t i, cudaStream_t s) {
+  Cell &c = b->cells[i];
+  const GroupArgs &a0 = c.fast[0][0].a;
+  int rc = launch_code_bounds(c.dcode, (long long)c.code.size(),
+                              (long long)a0.Bo * a0.mid, a0.ntiles, c.bounds,
+                              s);
+  if (rc) return rc;
+  for (int t = 0; t < 3; t++) {
+    for (const auto &gp : c.fast[t])
+      if ((rc = launch_group(gp, s))) return rc;
+    long long *slot = b->d_scal + 3 * i + t;
+    rc = t == 0 ? launch_cnt_reduce(c.cnt, c.g.space, kPredDef, 0, c.g.mu,
+                                    slot, s)
+                : launch_max(t == 1 ? c.gain : c.loss, c.g.space, slot, s);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int capture_graph(Batch *b) {
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  const size_t np = std::max<size_t>(1, b->passes.size());
+  CC_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  auto ck = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && !rc) {
+      fprintf(stderr, "coldcore_b200: batch capture: %s: %s\n", what,
+              cudaGetErrorString(e));
+      rc = -(100 + (int)e);
+    }
+  };
+  ck(cudaMemsetAsync(b->d_next, 0, 8, b->stream), "memset next");
+  ck(cudaMemsetAsync(b->d_err, 0, 4, b->stream), "memset err");
+  ck(cudaMemsetAsync(b->d_done, 0, np * sizeof(unsigned), b->stream),
+     "memset done");
+  ck(cudaMemsetAsync(b->d_scal, 0, b->cells.size() * 3 * 8, b->stream),
+     "memset scalars");
+  // big cells fork onto side streams, small cells share one persistent
+  // launch on the main stream, and everything joins before the end
+  ck(cudaEventRecord(b->fork, b->stream), "fork record");
+  for (int k = 0; k < kSideStreams; k++)
+    ck(cudaStreamWaitEvent(b->side[k], b->fork, 0), "fork wait");
+  int nbig = 0;
+  for (size_t i = 0; i < b->cells.size() && !rc; i++)
+    if (b->cells[i].big)
+      rc = run_big_cell(b, i, b->side[nbig++ % kSideStreams]);
+  if (!rc && b->nitems) {
+    BatchLaunch L{b->d_passes, b->d_dep, b->d_need, b->d_items, b->nitems,
+                  b->d_done, b->d_next, b->d_err, b->smem, b->grid};
+    rc = launch_batch(L, b->stream);
+  }
+  for (int k = 0; k < kSideStreams; k++) {
+    ck(cudaEventRecord(b->join[k], b->side[k]), "join record");
+    ck(cudaStreamWaitEvent(b->stream, b->join[k], 0), "join wait");
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  CC_CK(e);
+  b->graph = graph;
+  CC_CK(cudaGraphInstantiate(&b->exec, graph, 0));
+  return 0;
+}
+
+int run_persistent(Batch *b) {
+  CC_CK(cudaGraphLaunch(b->exec, b->stream));
+  int err = 0;
+  CC_CK(cudaMemcpyAsync(&err, b->d_err, 4, cudaMemcpyDeviceToHost,
+                        b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return err ? -7 : 0;
+}
+
+// One launch sequence per cell, cell after cell, synchronising after every
+// transform as the singleton dct_transform does — how a campaign of
+// single-cell contexts runs today; the baseline of the persistent launch.
+int run_per_cell(Batch *b) {
+  CC_CK(cudaMemsetAsync(b->d_scal, 0, b->cells.size() * 3 * 8, b->stream));
+  for (size_t i = 0; i < b->cells.size(); i++) {
+    const Cell &c = b->cells[i];
+    if (c.big) {
+      const int rc = run_big_cell(b, i, b->stream);
+      if (rc) return rc;
+      CC_CK(cudaStreamSynchronize(b->stream));
+      continue;
+    }
+    const int per_t = c.npass / 3;
+    for (int p = c.first_pass; p < c.first_pass + c.npass; p++) {
+      GroupPlan gp;
+      gp.a = b->passes[p];
+      gp.kernel = -1;
+      gp.threads = 256;
+      gp.smem = group_smem_bytes(gp.a, c.R1);
+      gp.grid = (int)std::min<long long>(gp.a.ntiles,
+                                         (long long)sm_count() * 4);
+      int rc = launch_group(gp, b->stream);
+      if (rc) return rc;
+      if ((p - c.first_pass + 1) % per_t == 0)
+        CC_CK(cudaStreamSynchronize(b->stream));
+    }
+  }
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+long long dct_batch_create(void) {
+  Batch *b = new Batch();
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) ==
+                cudaSuccess &&
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) ==
+                cudaSuccess;
+  for (int k = 0; k < kSideStreams && ok; k++)
+    ok = cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking) ==
+             cudaSuccess &&
+         cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) ==
+             cudaSuccess;
+  if (!ok) {
+    delete b;
+    return -1;
+  }
+  const long long h = g_next_handle++;
+  g_batches[h] = b;
+  return h;
+}
+
+int dct_batch_add(long long h, int problem, int n, const int *ax, int R,
+                  int mu, const long long *code, int M) {
+  Batch *b = get(h);
+  if (!b || b->built || problem < 0 || problem > 3 || n < 1 ||
+      n > kMaxAxes || !ax || R < 1 || mu < 1 || mu > 65535 || M < 0 ||
+      (M && !code))
+    return -1;
+  const bool layered = problem == kHamming || problem == kLee;
+  if (layered && R + 1 > kMaxLayers) return -1;
+  Cell c;
+  c.g.prob = problem; c.g.n = n; c.g.R = R; c.g.mu = mu;
+  c.g.pw[0] = 1;
+  for (int i = 0; i < n; i++) {
+    if (ax[i] < 2 || ax[i] > 16) return -1;          // tile kernel fibres
+    if (problem == kTorus && 2 * R + 1 > ax[i]) return -1;
+    if (c.g.pw[i] > (1LL << 40) / ax[i]) return -2;
+    c.g.ax[i] = ax[i];
+    c.g.pw[i + 1] = c.g.pw[i] * ax[i];
+  }
+  c.g.space = c.g.pw[n];
+  c.R1 = layered ? R + 1 : 1;
+  c.plane = (c.g.space + kPlaneAlign - 1) / kPlaneAlign * kPlaneAlign;
+  c.code.assign(code, code + M);
+  for (long long w : c.code)
+    if (w < 0 || w >= c.g.space) return -1;
+  std::sort(c.code.begin(), c.code.end());
+  // the exact uint16 bound of the singleton engine: no counter exceeds
+  // min(total occurrences, max multiplicity x |B|)
+  long long maxmult = 0, run = 0;
+  for (size_t i = 0; i < c.code.size(); i++) {
+    run = (i && c.code[i] == c.code[i - 1]) ? run + 1 : 1;
+    if (run > maxmult) maxmult = run;
+  }
+  if (std::min<long long>(M, maxmult * ball_cardinality(c.g)) > 65535)
+    return -1;
+  bool homog = true;
+  for (int i = 1; i < n; i++) homog &= ax[i] == ax[0];
+  int bm = 0;
+  c.big = c.g.space >= kBigCell && homog &&
+          pick_group_kernel(problem, ax[0], c.R1, &bm) >= 0;
+  b->cells.push_back(std::move(c));
+  return (int)b->cells.size() - 1;
+}
+
+int dct_batch_build(long long h, int tile_kb) {
+  Batch *b = get(h);
+  if (!b || b->built || b->cells.empty()) return -1;
+  if (tile_kb > 0) b->tile_budget = (size_t)std::max(16, tile_kb) * 1024;
+  // arena: per cell layers, cnt, gain, loss, code
+  size_t total = 0;
+  std::vector<size_t> off(b->cells.size());
+  for (size_t i = 0; i < b->cells.size(); i++) {
+    const Cell &c = b->cells[i];
+    off[i] = total;
+    total += align256((size_t)c.plane * c.R1 * 4) + align256(c.plane * 2) +
+             2 * align256((size_t)c.plane * 4) +
+             align256(std::max<size_t>(1, c.code.size()) * 8);
+  }
+  CC_CK(cudaMalloc(&b->arena, total));
+  b->arena_bytes = total;
+  CC_CK(cudaMalloc(&b->d_next, 8));
+  CC_CK(cudaMalloc(&b->d_err, 4));
+  CC_CK(cudaMalloc(&b->d_scal, b->cells.size() * 3 * 8));
+  for (size_t i = 0; i < b->cells.size(); i++) {
+    Cell &c = b->cells[i];
+    char *p = b->arena + off[i];
+    c.layers = reinterpret_cast<int32_t *>(p);
+    p += align256((size_t)c.plane * c.R1 * 4);
+    c.cnt = reinterpret_cast<uint16_t *>(p);
+    p += align256(c.plane * 2);
+    c.gain = reinterpret_cast<int32_t *>(p);
+    p += align256((size_t)c.plane * 4);
+    c.loss = reinterpret_cast<int32_t *>(p);
+    p += align256((size_t)c.plane * 4);
+    c.dcode = reinterpret_cast<long long *>(p);
+    if (!c.code.empty())
+      CC_CK(cudaMemcpyAsync(c.dcode, c.code.data(), c.code.size() * 8,
+                            cudaMemcpyHostToDevice, b->stream));
+  }
+  b->built = true;
+  // tile bounds depend on the tile size: computed per schedule
+  auto schedule = [&]() -> int {
+    int rc = make_schedule(b);
+    if (rc) return rc;
+    for (size_t i = 0; i < b->cells.size(); i++) {
+      const Cell &c = b->cells[i];
+      if (c.big) continue;             // bounds computed inside the graph
+      const GroupArgs &a0 = b->passes[c.first_pass];
+      rc = launch_code_bounds(c.dcode, (long long)c.code.size(),
+                              (long long)a0.Bo * a0.mid, a0.ntiles, c.bounds,
+                              b->stream);
+      if (rc) return rc;
+    }
+    return capture_graph(b);
+  };
+  int rc;
+  if (tile_kb > 0) return schedule();
+  // autotune the tile budget: time one graph launch per candidate
+  static const int cand_kb[] = {24, 48, 96};
+  cudaEvent_t e0, e1;
+  CC_CK(cudaEventCreate(&e0));
+  CC_CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_kb = 48;
+  for (int kb : cand_kb) {
+    b->tile_budget = (size_t)kb * 1024;
+    if ((rc = schedule())) return rc;
+    if ((rc = run_persistent(b))) return rc;               // warm
+    CC_CK(cudaEventRecord(e0, b->stream));
+    if ((rc = run_persistent(b))) return rc;
+    CC_CK(cudaEventRecord(e1, b->stream));
+    CC_CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CC_CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) { best = ms; best_kb = kb; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->tile_budget = (size_t)best_kb * 1024;
+  b->tuned_ms = best;
+  return schedule();
+}
+
+int dct_batch_run(long long h, int mode) {
+  Batch *b = get(h);
+  if (!b || !b->built) return -1;
+  if (mode == 0) return run_persistent(b);
+  if (mode == 1) return run_per_cell(b);
+  if (mode == 2) {
+    // self-test of the bounded dependency wait: one launch in which the
+    // first pass needs one more tile than it has, so its dependents time
+    // out; the launch must end with an error status, not hang
+    if (b->passes.size() < 2) return -1;
+    std::vector<unsigned> poisoned = b->need;
+    poisoned[0] += 1;
+    CC_CK(cudaMemcpyAsync(b->d_need, poisoned.data(),
+                          poisoned.size() * sizeof(unsigned),
+                          cudaMemcpyHostToDevice, b->stream));
+    const int rc = run_persistent(b);
+    CC_CK(cudaMemcpyAsync(b->d_need, b->need.data(),
+                          b->need.size() * sizeof(unsigned),
+                          cudaMemcpyHostToDevice, b->stream));
+    CC_CK(cudaStreamSynchronize(b->stream));
+    return rc;
+  }
+  return -1;
+}
+
+int dct_batch_read(long long h, int cell, int field, long long off,
+                   long long len, void *out) {
+  Batch *b = get(h);
+  if (!b || !b->built || cell < 0 || cell >= (int)b->cells.size() ||
+      field < 0 || field > 2 || off < 0 || len < 0 || (len && !out))
+    return -1;
+  const Cell &c = b->cells[cell];
+  if (off + len > c.g.space) return -1;
+  const void *src = field == 0 ? (const void *)(c.cnt + off)
+                    : field == 1 ? (const void *)(c.gain + off)
+                                 : (const void *)(c.loss + off);
+  if (len)
+    CC_CK(cudaMemcpyAsync(out, src, (size_t)len * (field == 0 ? 2 : 4),
+                          cudaMemcpyDeviceToHost, b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+int dct_batch_scalars(long long h, long long *out, int cap) {
+  Batch *b = get(h);
+  if (!b || !b->built || !out) return -1;
+  const int n = (int)std::min<long long>(cap, (long long)b->cells.size() * 3);
+  CC_CK(cudaMemcpyAsync(out, b->d_scal, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                        b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return n;
+}
+
+int dct_batch_info(long long h, long long *out, int cap) {
+  Batch *b = get(h);
+  if (!b || !out || cap < 6) return -1;
+  out[0] = (long long)b->cells.size();
+  out[1] = (long long)b->passes.size();
+  out[2] = b->nitems;
+  out[3] = (long long)(b->tile_budget / 1024);
+  out[4] = b->grid;
+  out[5] = (long long)(b->tuned_ms * 1000.0f);
+  return 6;
+}
+
+int dct_batch_free(long long h) {
+  Batch *b = get(h);
+  if (!b) return -1;
+  release(b);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  for (int k = 0; k < kSideStreams; k++) {
+    if (b->side[k]) cudaStreamDestroy(b->side[k]);
+    if (b->join[k]) cudaEventDestroy(b->join[k]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  g_batches.erase(h);
+  delete b;
+  return 0;
+}
+
+}  // extern "C"

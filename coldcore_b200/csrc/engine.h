@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
+#include <vector>
 
 namespace cc {
 
@@ -66,6 +67,9 @@ struct GroupArgs {
   int skew;               // log2 of the shared-memory skew period (0 = none)
   int prob;
   int pipe;               // prefetch the next tile while computing (cp.async)
+  int32_t *map;           // kDstMap target (nullptr: plane 0 of layers)
+  long long *red;         // epilogue reduction target (generic tiles)
+  int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
 };
 
 struct GroupPlan {
@@ -76,13 +80,40 @@ struct GroupPlan {
   int grid;
 };
 
+// planner.cu: schedule knobs and the group plan of one transform
+struct Knobs { size_t budget; int pipe; };   // pipe: see plan_groups
+struct PlanPtrs {
+  int32_t *layers; long long plane; uint16_t *cnt;
+  const long long *code; long long ncode; int32_t *map;
+};
+std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
+                                   const PlanPtrs &ptr, int src, int dst,
+                                   Knobs kn);
+
 // launchers (transform_*.cu)
 int launch_group(const GroupPlan &p, cudaStream_t s);
+int prepare_group(const GroupPlan &p);
 size_t group_smem_bytes(const GroupArgs &a, int R1);
 int pick_group_kernel(int prob, int q, int R1, int *bm);
 int launch_code_bounds(const long long *code, long long ncode,
                        long long tile_words, long long ntiles,
                        long long *bounds, cudaStream_t s);
+
+// batched engine: one persistent launch over (pass, tile) work items
+struct BatchLaunch {
+  const GroupArgs *passes;
+  const int *dep;
+  const unsigned *need;
+  const int4 *items;            // (pass, first tile, tiles, 0)
+  long long nitems;
+  unsigned *done;
+  unsigned long long *next;
+  int *err;
+  size_t smem;
+  int grid;
+};
+int launch_batch(const BatchLaunch &b, cudaStream_t s);
+int batch_grid(size_t smem);
 
 // window pass (torus / grid) over one axis, any width, out of place
 struct WindowArgs {

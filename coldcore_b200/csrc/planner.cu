@@ -1,0 +1,189 @@
+// planner.cu — transform schedules: which axes each launch covers, its
+// tile, rounds, CTA size and grid (used by the singleton cell and by the
+// large cells of a batch).
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+#include <vector>
+
+#include "engine.h"
+
+namespace cc {
+namespace {
+
+int ipow(int q, int e) { int r = 1; while (e-- > 0) r *= q; return r; }
+
+void set_rounds(GroupArgs &a, int q, int bm) {
+  const int nr = (a.k + bm - 1) / bm;
+  std::vector<int> rb(nr), rs(nr);
+  for (int r = 0; r < nr; r++) {
+    rb[r] = std::min(bm, a.k - r * bm);
+    rs[r] = ipow(q, r * bm);
+  }
+  std::vector<int> order(nr);
+  for (int r = 0; r < nr; r++) order[r] = r;
+  if (a.W == 1 && nr >= 3) {
+    // HBM-facing rounds get the widest strides (coalesced lanes): the
+    // widest round stores every layer, the second widest loads the
+    // 2-byte cnt, the rest exchange through shared memory in between
+    order.clear();
+    order.push_back(nr - 2);
+    for (int r = 0; r < nr - 2; r++) order.push_back(r);
+    order.push_back(nr - 1);
+  }
+  a.nrounds = nr;
+  for (int i = 0; i < nr; i++) {
+    a.rb[i] = rb[order[i]];
+    a.rs[i] = rs[order[i]];
+    a.rq[i] = q;
+  }
+}
+
+int threads_for(const GroupArgs &a, int kid, int bm, int q) {
+  int t;
+  if (kid >= 0) {
+    const long long words = (long long)a.W * a.mid * a.Bo;
+    const int ne = ipow(q, std::min(bm, a.k));
+    t = (int)std::min<long long>(kGroupThreads, words / ne);
+  } else {
+    t = (int)std::min<long long>(256, (long long)a.W * a.mid * a.Bo);
+  }
+  t = (t + 31) / 32 * 32;
+  const char *cap = getenv("CC_THREADS");          // tuning cap
+  if (cap && atoi(cap) >= 32 && t > atoi(cap)) t = atoi(cap) / 32 * 32;
+  return t < 32 ? 32 : t;
+}
+
+int occupancy_grid(const GroupPlan &p) {
+  // persistent: as many CTAs as fit, capped by the tile count
+  int per_sm = 1;
+  const size_t budget_sm = 228 * 1024;
+  per_sm = (int)std::max<size_t>(1, budget_sm / (p.smem + 1024));
+  const int by_threads = 2048 / p.threads;
+  if (per_sm > by_threads) per_sm = by_threads;
+  if (per_sm < 1) per_sm = 1;
+  long long grid = (long long)sm_count() * per_sm;
+  if (grid > p.a.ntiles) grid = p.a.ntiles;
+  return (int)std::max<long long>(1, grid);
+}
+
+// Distance layers that can be nonzero after axes 0..j-1: each Hamming axis
+// adds at most 1 to the distance, each Lee axis at most floor(a/2).
+int live_layers(const Geometry &g, int j) {
+  long long reach = 0;
+  for (int i = 0; i < j; i++)
+    reach += g.prob == kLee ? g.ax[i] / 2 : 1;
+  return (int)std::min<long long>(reach, g.R) + 1;
+}
+
+}  // namespace
+
+// Groups of consecutive axes for one transform of cell `g`: the most axes
+// per launch whose tile fits kn.budget bytes of shared memory, the
+// register-blocked kernel where one exists for the axis size and layer
+// count, 128- or 64-byte rows on strided groups, rounds ordered so the
+// HBM-facing ones have the widest strides.
+std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
+                                   const PlanPtrs &ptr, int src, int dst,
+                                   Knobs kn) {
+  std::vector<GroupPlan> out;
+  const bool layered = R1 > 1;
+  const size_t budget = kn.budget;
+  int j = 0;
+  while (j < g.n) {
+    const int q = g.ax[j];
+    int bm = 1;
+    const int kid = pick_group_kernel(g.prob, q, R1, &bm);
+    GroupArgs base{};
+    base.layers = ptr.layers;
+    base.plane = ptr.plane;
+    base.cnt = ptr.cnt;
+    base.code = ptr.code;
+    base.ncode = ptr.ncode;
+    base.map = ptr.map;
+    base.inner = g.pw[j];
+    base.prob = g.prob;
+    base.R = g.R;
+    base.mu = g.mu;
+    base.src = j == 0 ? src : kSrcLayers;
+    // pipe 1 and 3 prefetch the cnt-reading first group; 3 also the last
+    // group when it writes the 4-byte map (reads every layer, writes one
+    // plane), decided below; 2 prefetches every group
+    base.pipe = kid >= 0 && base.src != kSrcCode &&
+                (kn.pipe == 2 || ((kn.pipe == 1 || kn.pipe == 3) &&
+                                  base.src == kSrcCnt));
+    // the most axes that fit one tile of W inner words
+    auto grow = [&](int W) {
+      GroupArgs a = base;
+      a.W = W;
+      long long mid = 1;
+      for (;;) {
+        if (j + a.k >= g.n || a.k >= kMaxRounds) break;
+        const int qn = g.ax[j + a.k];
+        if (kid >= 0 && qn != q) break;
+        if (kid < 0 && qn > 16) break;
+        const long long mid2 = mid * qn;
+        GroupArgs t = a;
+        t.k = a.k + 1;
+        t.mid = (int)std::min<long long>(mid2, INT_MAX / 64);
+        const long long outer = g.space / (a.inner * mid2);
+        t.Bo = W >= 16 ? 1
+               : (int)std::max<long long>(1, std::min<long long>(
+                     outer, 2048 / (W * mid2)));
+        t.skew = 0;
+        if (kid >= 0 && W == 1 && (q & (q - 1)) == 0) {
+          int lg = 0;
+          while ((1 << lg) < ipow(q, bm)) lg++;
+          t.skew = lg;
+        }
+        const bool fits = group_smem_bytes(t, R1) <= budget &&
+                          mid2 < (1 << 24);
+        if (a.k > 0 && !fits) break;
+        a = t;
+        mid = mid2;
+      }
+      return a;
+    };
+    GroupArgs a;
+    if (base.inner >= 32) {
+      // 128-byte rows, or 64-byte rows when that fits more axes
+      a = grow(32);
+      GroupArgs b16 = grow(16);
+      if (b16.k > a.k) a = b16;
+    } else {
+      a = grow((int)base.inner);
+    }
+    a.outer = g.space / (a.inner * (long long)a.mid);
+    a.nchunk = (a.inner + a.W - 1) / a.W;
+    a.ntiles = (a.outer + a.Bo - 1) / a.Bo * a.nchunk;
+    for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j + t];
+    if (kid >= 0) set_rounds(a, q, bm);
+    else a.nrounds = 0;
+    const bool last = j + a.k == g.n;
+    a.dst = last ? dst : kDstLayers;
+    if (kn.pipe == 3 && kid >= 0 && last && dst != kDstLayers &&
+        a.src == kSrcLayers) {
+      // read-heavy last group: prefetch its tiles too (if they still fit)
+      GroupArgs t = a;
+      t.pipe = 1;
+      if (group_smem_bytes(t, R1) <= budget) a.pipe = 1;
+    }
+    a.lin = layered ? live_layers(g, j) : 1;
+    a.lout = layered ? live_layers(g, j + a.k) : 1;
+    if (last && dst == kDstLayers) a.lout = R1;   // every layer, zeros too
+    a.pmode = kPredEq;
+    a.ptarget = 0;
+    GroupPlan p;
+    p.a = a;
+    p.kernel = kid;
+    p.smem = group_smem_bytes(a, R1);
+    p.threads = threads_for(a, kid, bm, q);
+    p.grid = occupancy_grid(p);
+    out.push_back(p);
+    j += a.k;
+  }
+  return out;
+}
+
+
+}  // namespace cc

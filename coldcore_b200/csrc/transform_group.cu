@@ -310,7 +310,7 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
           }
         }
       } else if (dst == kIoMap) {
-        int32_t *p = g.layers + xb;
+        int32_t *p = (g.map ? g.map : g.layers) + xb;
 #pragma unroll
         for (int e = 0; e < QB; e++) {
           if (!FULL && e >= ne) break;
@@ -506,119 +506,242 @@ group_kernel_pipe(const GroupArgs g) {
 // Any axis size (<= 16) and layer count (<= 8), one axis per round, fibres
 // processed in place in shared memory.  Used for the cells without a
 // register-blocked instantiation (mixed radix, wide Hamming / Lee alphabets,
-// small torus / grid axes).
-__global__ void __launch_bounds__(512) group_generic(const GroupArgs g) {
-  extern __shared__ int32_t sm[];
+// small torus / grid axes) and, one tile per work item, by the batched
+// engine (CG: global reads through L2 only, because other SMs of the same
+// launch wrote them).  Optional epilogue reductions of the output (red_mode
+// 1: deficit sum max(0, mu - cnt) of a written cnt; 2: maximum of a written
+// map) add into *red.
+template <bool CG>
+__device__ __forceinline__ int32_t ld_i32(const int32_t *p) {
+  return CG ? __ldcg(p) : *p;
+}
+template <bool CG>
+__device__ __forceinline__ int ld_u16(const uint16_t *p) {
+  return CG ? (int)__ldcg(p) : (int)*p;
+}
+
+template <bool CG>
+__device__ void generic_tile(const GroupArgs &g, long long tile,
+                             int32_t *sm) {
   const int R1 = g.prob == kTorus || g.prob == kGrid ? 1 : g.R + 1;
   const long long imid = g.inner * (long long)g.mid;
   const int W = g.W;
   const int tile_words = g.Bo * g.mid;
   const int SD = (skewed(tile_words, g.skew) + 1) * W;
   const int nel = tile_words * W;
-  for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-    const long long o0 = (tile / g.nchunk) * g.Bo;
-    const long long i0 = (tile % g.nchunk) * W;
-    if (g.src == kSrcCode) {
-      long long len = (g.outer - o0) * (long long)g.mid;
-      stage_code(g, sm, tile, o0 * g.mid,
-                 (int)(len < tile_words ? len : tile_words));
+  int32_t *map = g.map ? g.map : g.layers;
+  const long long o0 = (tile / g.nchunk) * g.Bo;
+  const long long i0 = (tile % g.nchunk) * W;
+  if (g.src == kSrcCode) {
+    long long len = (g.outer - o0) * (long long)g.mid;
+    stage_code(g, sm, tile, o0 * g.mid,
+               (int)(len < tile_words ? len : tile_words));
+  }
+  // -------- load the tile
+  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
+    const int w = t % W, p = t / W, ob = p / g.mid, m = p % g.mid;
+    const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
+    const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
+    const int sp = skewed(p, g.skew) * W + w;
+    for (int d = 0; d < R1; d++) {
+      int32_t val = 0;
+      if (g.src == kSrcLayers) {
+        if (valid && d < g.lin) val = ld_i32<CG>(g.layers + d * g.plane + x);
+      } else if (g.src == kSrcCnt) {
+        if (valid && d == 0)
+          val = cnt_pred(g.pmode, ld_u16<CG>(g.cnt + x), g.ptarget, g.mu);
+      } else if (d == 0) {
+        val = sm[sp];
+      }
+      sm[d * SD + sp] = val;
     }
-    // -------- load the tile
-    for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-      const int w = t % W, p = t / W, ob = p / g.mid, m = p % g.mid;
-      const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
-      const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
-      const int sp = skewed(p, g.skew) * W + w;
-      for (int d = 0; d < R1; d++) {
-        int32_t val = 0;
-        if (g.src == kSrcLayers) {
-          if (valid && d < g.lin) val = g.layers[d * g.plane + x];
-        } else if (g.src == kSrcCnt) {
-          if (valid && d == 0)
-            val = cnt_pred(g.pmode, (int)g.cnt[x], g.ptarget, g.mu);
-        } else if (d == 0) {
-          val = sm[sp];
+  }
+  __syncthreads();
+  // -------- one axis at a time
+  int S = 1;
+  for (int j = 0; j < g.k; j++) {
+    const int q = g.qax[j];
+    const int nh = g.mid / (S * q);
+    const int nfib = W * S * nh * g.Bo;
+    for (int f = threadIdx.x; f < nfib; f += blockDim.x) {
+      const int w = f % W;
+      int rest = f / W;
+      const int mlo = rest % S;
+      rest /= S;
+      const int mhi = rest % nh, ob = rest / nh;
+      const int pb = ob * g.mid + mlo + S * q * mhi;
+      int sp[16];
+      for (int a = 0; a < q; a++) sp[a] = skewed(pb + S * a, g.skew) * W + w;
+      if (g.prob == kHamming) {
+        int32_t T[kMaxLayers];
+        for (int d = 0; d + 1 < R1; d++) {
+          int32_t s = 0;
+          for (int a = 0; a < q; a++) s += sm[d * SD + sp[a]];
+          T[d] = s;
         }
-        sm[d * SD + sp] = val;
+        for (int d = R1 - 1; d >= 1; d--)
+          for (int a = 0; a < q; a++)
+            sm[d * SD + sp[a]] += T[d - 1] - sm[(d - 1) * SD + sp[a]];
+      } else if (g.prob == kLee) {
+        const int H = q / 2;
+        for (int d = R1 - 1; d >= 1; d--) {
+          const int wm = d < H ? d : H;
+          for (int a = 0; a < q; a++) {
+            int32_t s = sm[d * SD + sp[a]];
+            for (int w2 = 1; w2 <= wm; w2++) {
+              int am = a - w2; if (am < 0) am += q;
+              int ap = a + w2; if (ap >= q) ap -= q;
+              s += sm[(d - w2) * SD + sp[am]];
+              if (ap != am) s += sm[(d - w2) * SD + sp[ap]];
+            }
+            sm[d * SD + sp[a]] = s;   // reads only lower layers + itself
+          }
+        }
+      } else {
+        int32_t old[16];
+        for (int a = 0; a < q; a++) old[a] = sm[sp[a]];
+        for (int a = 0; a < q; a++) {
+          int32_t s = 0;
+          for (int b = 0; b < q; b++) {
+            int dd = a > b ? a - b : b - a;
+            if (g.prob == kTorus && q - dd < dd) dd = q - dd;
+            if (dd <= g.R) s += old[b];
+          }
+          sm[sp[a]] = s;
+        }
+      }
+    }
+    S *= q;
+    __syncthreads();
+  }
+  // -------- store the tile (+ epilogue reduction)
+  long long red = 0;
+  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
+    const int w = t % W, p = t / W, ob = p / g.mid, m = p % g.mid;
+    const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
+    if (!valid) continue;
+    const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
+    const int sp = skewed(p, g.skew) * W + w;
+    if (g.dst == kDstLayers) {
+      for (int d = 0; d < g.lout; d++)
+        g.layers[d * g.plane + x] = sm[d * SD + sp];
+    } else {
+      int32_t s = 0;
+      for (int d = 0; d < R1; d++) s += sm[d * SD + sp];
+      if (g.dst == kDstMap) {
+        map[x] = s;
+        if (g.red_mode == 2 && s > red) red = s;
+      } else {
+        const int c = s > 65535 ? 65535 : s;
+        g.cnt[x] = (uint16_t)c;
+        if (g.red_mode == 1 && c < g.mu) red += g.mu - c;
+      }
+    }
+  }
+  if (g.red_mode) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const long long other = __shfl_down_sync(0xffffffffu, red, o);
+      red = g.red_mode == 2 ? (other > red ? other : red) : red + other;
+    }
+    if ((threadIdx.x & 31) == 0 && red) {
+      if (g.red_mode == 2) atomicMax((unsigned long long *)g.red,
+                                     (unsigned long long)red);
+      else atomicAdd((unsigned long long *)g.red, (unsigned long long)red);
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(512) group_generic(const GroupArgs g) {
+  extern __shared__ int32_t sm[];
+  for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x)
+    generic_tile<false>(g, tile, sm);
+}
+
+// ------------------------------------------------------------ batched engine
+// One persistent launch over many independent cells.  Work items (pass,
+// tile) are claimed in table order from one atomic counter; the table is
+// ordered by pass level (every cell's pass 0, then every cell's pass 1, ...)
+// and a pass depends only on the previous pass of its own cell, so an item
+// only ever waits for items claimed before it — by CTAs already running —
+// and the schedule cannot deadlock.  The wait is bounded: after
+// kBatchSpinLimit polls the CTA records an error and stops, and the host
+// reports it.  Data written by other CTAs of the launch is read through L2
+// (generic_tile<true>).
+constexpr long long kBatchSpinLimit = 1LL << 22;
+
+__global__ void __launch_bounds__(256)
+batch_kernel(const GroupArgs *passes, const int *pass_dep,
+             const unsigned *pass_need, const int4 *items, long long nitems,
+             unsigned *done, unsigned long long *next, int *err) {
+  extern __shared__ int32_t sm[];
+  __shared__ long long s_it;
+  __shared__ int s_bad;
+  __shared__ GroupArgs sg;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_it = (long long)atomicAdd(next, 1ULL);
+      s_bad = 0;
+    }
+    __syncthreads();
+    const long long it = s_it;
+    if (it >= nitems) break;
+    const int4 item = items[it];           // pass, first tile, tiles
+    const int *src = reinterpret_cast<const int *>(passes + item.x);
+    int *dst = reinterpret_cast<int *>(&sg);
+    for (int i = threadIdx.x; i < (int)(sizeof(GroupArgs) / 4);
+         i += blockDim.x)
+      dst[i] = src[i];
+    if (threadIdx.x == 0) {
+      const int dep = pass_dep[item.x];
+      if (dep >= 0) {
+        const unsigned need = pass_need[dep];
+        long long spins = 0;
+        while (*(volatile unsigned *)(done + dep) < need) {
+          if (++spins > kBatchSpinLimit) {
+            atomicExch(err, 1);
+            s_bad = 1;
+            break;
+          }
+          __nanosleep(256);
+        }
+        __threadfence();
       }
     }
     __syncthreads();
-    // -------- one axis at a time
-    int S = 1;
-    for (int j = 0; j < g.k; j++) {
-      const int q = g.qax[j];
-      const int nh = g.mid / (S * q);
-      const int nfib = W * S * nh * g.Bo;
-      for (int f = threadIdx.x; f < nfib; f += blockDim.x) {
-        const int w = f % W;
-        int rest = f / W;
-        const int mlo = rest % S;
-        rest /= S;
-        const int mhi = rest % nh, ob = rest / nh;
-        const int pb = ob * g.mid + mlo + S * q * mhi;
-        int sp[16];
-        for (int a = 0; a < q; a++) sp[a] = skewed(pb + S * a, g.skew) * W + w;
-        if (g.prob == kHamming) {
-          int32_t T[kMaxLayers];
-          for (int d = 0; d + 1 < R1; d++) {
-            int32_t s = 0;
-            for (int a = 0; a < q; a++) s += sm[d * SD + sp[a]];
-            T[d] = s;
-          }
-          for (int d = R1 - 1; d >= 1; d--)
-            for (int a = 0; a < q; a++)
-              sm[d * SD + sp[a]] += T[d - 1] - sm[(d - 1) * SD + sp[a]];
-        } else if (g.prob == kLee) {
-          const int H = q / 2;
-          for (int d = R1 - 1; d >= 1; d--) {
-            const int wm = d < H ? d : H;
-            for (int a = 0; a < q; a++) {
-              int32_t s = sm[d * SD + sp[a]];
-              for (int w2 = 1; w2 <= wm; w2++) {
-                int am = a - w2; if (am < 0) am += q;
-                int ap = a + w2; if (ap >= q) ap -= q;
-                s += sm[(d - w2) * SD + sp[am]];
-                if (ap != am) s += sm[(d - w2) * SD + sp[ap]];
-              }
-              sm[d * SD + sp[a]] = s;   // reads only lower layers + itself
-            }
-          }
-        } else {
-          int32_t old[16];
-          for (int a = 0; a < q; a++) old[a] = sm[sp[a]];
-          for (int a = 0; a < q; a++) {
-            int32_t s = 0;
-            for (int b = 0; b < q; b++) {
-              int dd = a > b ? a - b : b - a;
-              if (g.prob == kTorus && q - dd < dd) dd = q - dd;
-              if (dd <= g.R) s += old[b];
-            }
-            sm[sp[a]] = s;
-          }
-        }
-      }
-      S *= q;
-      __syncthreads();
-    }
-    // -------- store the tile
-    for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-      const int w = t % W, p = t / W, ob = p / g.mid, m = p % g.mid;
-      const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
-      if (!valid) continue;
-      const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
-      const int sp = skewed(p, g.skew) * W + w;
-      if (g.dst == kDstLayers) {
-        for (int d = 0; d < g.lout; d++)
-          g.layers[d * g.plane + x] = sm[d * SD + sp];
-      } else {
-        int32_t s = 0;
-        for (int d = 0; d < R1; d++) s += sm[d * SD + sp];
-        if (g.dst == kDstMap) g.layers[x] = s;
-        else g.cnt[x] = (uint16_t)(s > 65535 ? 65535 : s);
-      }
+    if (s_bad) break;
+    for (int t = 0; t < item.z; t++)
+      generic_tile<true>(sg, (long long)item.y + t, sm);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(done + item.x, (unsigned)item.z);
     }
     __syncthreads();
   }
+}
+
+int launch_batch(const BatchLaunch &b, cudaStream_t s) {
+  batch_kernel<<<b.grid, 256, b.smem, s>>>(b.passes, b.dep, b.need, b.items,
+                                           b.nitems, b.done, b.next, b.err);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+// opts the kernel in to `smem` bytes of dynamic shared memory (outside any
+// stream capture) and returns the persistent grid: every CTA that fits
+int batch_grid(size_t smem) {
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    if (cudaFuncSetAttribute((const void *)batch_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) == cudaSuccess)
+      attr = smem;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 256,
+                                                smem);
+  if (per_sm < 1) per_sm = 1;
+  return per_sm * sm_count();
 }
 
 // ------------------------------------------------------------ dispatch table
@@ -682,21 +805,40 @@ size_t group_smem_bytes(const GroupArgs &a, int R1) {
   return 2 * tile;                          // two tiles
 }
 
-int launch_group(const GroupPlan &p, cudaStream_t s) {
-  GroupFn fn = p.kernel < 0 ? group_generic
-               : p.a.pipe ? kTable[p.kernel].fn_pipe : kTable[p.kernel].fn;
-  // opt in to the dynamic shared memory this launch needs (the per-block
-  // limit counts the kernel's static shared memory too)
+static GroupFn group_fn(const GroupPlan &p) {
+  return p.kernel < 0 ? group_generic
+         : p.a.pipe ? kTable[p.kernel].fn_pipe : kTable[p.kernel].fn;
+}
+
+// Opt the plan's kernel in to the dynamic shared memory it needs (the
+// per-block limit counts the kernel's static shared memory too).  The
+// opt-in only ever grows, so one launch never lowers another's.
+int ensure_group_smem(const GroupPlan &p) {
   static size_t attr_set[2 * 64 + 1];
   const int slot = p.kernel < 0 ? 128 : p.kernel + (p.a.pipe ? 64 : 0);
   if (p.smem > 48 * 1024 && p.smem > attr_set[slot]) {
-    CC_CK(cudaFuncSetAttribute((const void *)fn,
+    CC_CK(cudaFuncSetAttribute((const void *)group_fn(p),
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)p.smem));
     attr_set[slot] = p.smem;
   }
+  return 0;
+}
+
+// ahead of a stream capture, so that the capture only records launches
+int prepare_group(const GroupPlan &p) { return ensure_group_smem(p); }
+
+int launch_group(const GroupPlan &p, cudaStream_t s) {
+  GroupFn fn = group_fn(p);
+  const int rc = ensure_group_smem(p);
+  if (rc) return rc;
   fn<<<p.grid, p.threads, p.smem, s>>>(p.a);
-  CC_CK(cudaGetLastError());
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    fprintf(stderr, "coldcore_b200: group launch (kernel %d pipe %d grid %d "
+            "threads %d smem %zu tiles %lld) failed\n", p.kernel, p.a.pipe,
+            p.grid, p.threads, p.smem, p.a.ntiles);
+  CC_CK(e);
   return 0;
 }
 

@@ -93,3 +93,28 @@ def candidates(size, n, seed):
     """``n`` uniformly random candidate words (repeats allowed)."""
     rng = np.random.default_rng(seed)
     return rng.integers(0, size, size=n).astype(np.int64)
+
+
+def batch_cells(count=256, seed=7, lo=3.0, hi=7.0):
+    """The batched-campaign workload: ``count`` seeded cells of uneven size.
+
+    q uniform in {2..6}; n = round(log_q(10^U[lo, hi])) (so q^n is
+    log-uniform in 10^lo..10^hi); R uniform in {1..4}, clipped to n;
+    Hamming with probability 0.8, else Lee; a uniform random code covering
+    about half the space (M = floor(ln 2 |X| / |B|), at least 1).
+    Returns a list of (problem, axes, R, code)."""
+    from .patterns import ball_size
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        q = int(rng.integers(2, 7))
+        n = max(1, int(round(rng.uniform(lo, hi) * math.log(10) / math.log(q))))
+        R = min(int(rng.integers(1, 5)), n)
+        problem = "hamming" if rng.random() < 0.8 else "lee"
+        axes = (q,) * n
+        size = q ** n
+        ball = ball_size(axes, R, problem)
+        M = max(1, min(size, int(math.floor(math.log(2.0) * size / ball))))
+        code = np.sort(rng.choice(size, size=M, replace=False)).astype(np.int64)
+        out.append((problem, axes, R, code))
+    return out

@@ -154,6 +154,32 @@ CCP_API int  dct_b200_set_timing(int on);
 CCP_API int  dct_b200_last_timings(float *ms, int cap);
 /* words [off, off+len) of the map (the last transform's out_mode 1 field) */
 CCP_API int  dct_b200_read_map(long long off, long long len, int32_t *out);
+/* ---- batched campaign (no counterpart in the reference, which runs one
+ * process per cell: src/coldcore/campaign.py:186-221).  A batch holds many
+ * independent cells (any problem, axes <= 16, each code within the exact
+ * uint16 bound min(occurrences, max multiplicity x |B|) <= 65,535) and
+ * computes, for every cell, cnt from its code, the deficit
+ * sum max(0, mu - cnt), the gain map and its maximum and the loss map and
+ * its maximum in ONE persistent launch replayed from a CUDA graph.  Handles
+ * are independent of the dct_* singleton cell. ---- */
+CCP_API long long dct_batch_create(void);
+/* returns the cell index, or a negative error */
+CCP_API int  dct_batch_add(long long h, int problem, int n, const int *ax,
+                           int R, int mu, const long long *code, int M);
+/* allocates and schedules; tile_kb = shared memory per tile, 0 = autotune */
+CCP_API int  dct_batch_build(long long h, int tile_kb);
+/* mode 0: the persistent graph launch; 1: one launch per pass per cell;
+ * 2: self-test of the bounded dependency wait (returns -7, no hang) */
+CCP_API int  dct_batch_run(long long h, int mode);
+/* field 0 cnt (uint16), 1 gain map (int32), 2 loss map (int32) */
+CCP_API int  dct_batch_read(long long h, int cell, int field, long long off,
+                            long long len, void *out);
+/* per cell: deficit, gain maximum, loss maximum; returns values written */
+CCP_API int  dct_batch_scalars(long long h, long long *out, int cap);
+/* cells, passes, work items, tile KB, grid, tuned step microseconds */
+CCP_API int  dct_batch_info(long long h, long long *out, int cap);
+CCP_API int  dct_batch_free(long long h);
+
 /* No counterpart in the reference.  Gain (role 0) or loss (role 1) map of
  * a Hamming / Lee cell for callers that may not allocate device memory —
  * a framework whose own allocator must own every buffer, a service that
