@@ -1021,6 +1021,48 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
   return n;
 }
 
+int dct_b200_ball_map_hist(const long long *words, int nw, int nbins,
+                           int32_t *out) {
+  if (!S.live || nbins < 1 || nbins > 32 || !out) return -1;
+  if (nw <= 0) return 0;
+  if (!valid_words(words, nw)) return -1;
+  const WalkArgs w = walk_args();
+  const long long cap = kStageCap / nbins;   // nb * nbins fits d_out
+  for (long long off = 0; off < nw; off += cap) {
+    const int nb = (int)std::min<long long>(cap, nw - off);
+    int rc = stage_words(words + off, nb);
+    if (rc) return rc;
+    rc = launch_ball_map_hist(w, S.d_words, nb, S.layers, nbins, S.d_out,
+                              g_stream);
+    if (rc) return rc;
+    CC_CK(cudaMemcpyAsync(S.h_out, S.d_out, (size_t)nb * nbins * 4,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    memcpy(out + off * nbins, S.h_out, (size_t)nb * nbins * 4);
+  }
+  return 0;
+}
+
+int dct_b200_layers_at(const long long *idx, int k, int32_t *out) {
+  if (!S.live || !S.layered_out || (k && !out)) return -1;
+  if (k <= 0) return 0;
+  if (!valid_words(idx, k)) return -1;
+  const long long cap = kStageCap / S.R1;
+  for (long long off = 0; off < k; off += cap) {
+    const int nb = (int)std::min<long long>(cap, k - off);
+    int rc = stage_words(idx + off, nb);
+    if (rc) return rc;
+    rc = launch_layers_at(S.layers, S.plane, S.R1, S.d_words, nb, S.d_out,
+                          g_stream);
+    if (rc) return rc;
+    CC_CK(cudaMemcpyAsync(S.h_out, S.d_out, (size_t)nb * S.R1 * 4,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    memcpy(out + off * S.R1, S.h_out, (size_t)nb * S.R1 * 4);
+  }
+  return 0;
+}
+
 int dct_b200_set_timing(int on) {
   g_timing = on ? 1 : 0;
   return 0;

@@ -123,6 +123,67 @@ k_gather(const WalkArgs a, const long long *words, int split, int mode,
   }
 }
 
+// out[wi][b] = #{x in B(w_i) : bin(map[x]) == b}, log2 bins: 0 for v <= 0,
+// 1 for v == 1, 2 for 2..3, 3 for 4..7, ... clipped to nbins - 1
+template <bool GRID>
+__global__ void __launch_bounds__(256)
+k_ball_map_hist(const WalkArgs a, const long long *words, int split,
+                const int32_t *map, int nbins, int32_t *out) {
+  __shared__ WordSmem s;
+  __shared__ int32_t hist[32];
+  const int wi = blockIdx.x / split, seg = blockIdx.x % split;
+  const long long w = words[wi];
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[b] = 0;
+  word_setup(a.g, w, s);
+  const long long step = (long long)split * blockDim.x;
+  for (long long t = (long long)seg * blockDim.x + threadIdx.x; t < a.len;
+       t += step) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x < 0) continue;
+    const int32_t v = map[x];
+    const int b = v <= 0 ? 0 : min(nbins - 1, 32 - __clz(v));
+    atomicAdd(&hist[b], 1);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+    if (hist[b]) atomicAdd(&out[(long long)wi * nbins + b], hist[b]);
+}
+
+int launch_ball_map_hist(const WalkArgs &w, const long long *dwords, int nb,
+                         const int32_t *map, int nbins, int32_t *out,
+                         cudaStream_t s) {
+  if (nb <= 0) return 0;
+  const int split = pick_split(w.len, nb);
+  CC_CK(cudaMemsetAsync(out, 0, (size_t)nb * nbins * 4, s));
+  const dim3 grid((unsigned)nb * split);
+  if (w.g.prob == kGrid)
+    k_ball_map_hist<true><<<grid, 256, 0, s>>>(w, dwords, split, map, nbins,
+                                               out);
+  else
+    k_ball_map_hist<false><<<grid, 256, 0, s>>>(w, dwords, split, map, nbins,
+                                                out);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+// the R + 1 layer values at each of k words: out[i][d]
+__global__ void k_layers_at(const int32_t *layers, long long plane, int R1,
+                            const long long *idx, int k, int32_t *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k) return;
+  for (int d = 0; d < R1; d++) out[(long long)i * R1 + d] =
+      layers[d * plane + idx[i]];
+}
+
+int launch_layers_at(const int32_t *layers, long long plane, int R1,
+                     const long long *idx, int k, int32_t *out,
+                     cudaStream_t s) {
+  if (k <= 0) return 0;
+  k_layers_at<<<(k + 255) / 256, 256, 0, s>>>(layers, plane, R1, idx, k, out);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
 // blocks per word so that single-word walks still fill the GPU
 int pick_split(long long len, int nb) {
   long long cover = (len + 255) / 256;

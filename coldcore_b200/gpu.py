@@ -88,6 +88,8 @@ def _bind(path):
         "dct_b200_read_layer": (I, [I, _LL, _LL, _I32P]),
         "dct_b200_read_map": (I, [_LL, _LL, _I32P]),
         "dct_b200_set_timing": (I, [I]),
+        "dct_b200_ball_map_hist": (I, [_LLP, I, I, _I32P]),
+        "dct_b200_layers_at": (I, [_LLP, I, _I32P]),
         "dct_b200_last_timings": (I, [ctypes.POINTER(ctypes.c_float), I]),
     }
     for name, (res, args) in sig.items():
@@ -281,6 +283,24 @@ class GpuBackend:
         buf = (ctypes.c_float * 64)()
         n = self._lib.dct_b200_last_timings(buf, 64)
         return [float(buf[i]) for i in range(min(n, 64))]
+
+    def ball_map_hist(self, idx, nbins=8):
+        """Per word: log2 histogram of the current map over its ball."""
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        out = np.zeros((len(idx), nbins), dtype=np.int32)
+        if len(idx):
+            _check("ball_map_hist", self._lib.dct_b200_ball_map_hist(
+                _p(idx), len(idx), int(nbins), _p(out, ctypes.c_int32)))
+        return out
+
+    def layers_at(self, idx):
+        """(k, R+1) exact distance layers at k words, after layers_map()."""
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        out = np.zeros((len(idx), self.R + 1), dtype=np.int32)
+        if len(idx):
+            _check("layers_at", self._lib.dct_b200_layers_at(
+                _p(idx), len(idx), _p(out, ctypes.c_int32)))
+        return out
 
     def plan(self, init_mode, out_mode):
         """Launches of one transform: rows (first axis, axes, bytes, kernel)."""

@@ -180,6 +180,24 @@ CCP_API int  dct_batch_scalars(long long h, long long *out, int cap);
 CCP_API int  dct_batch_info(long long h, long long *out, int cap);
 CCP_API int  dct_batch_free(long long h);
 
+/* ---- learned ruin proposal scorer (no counterpart in the reference): a
+ * 32-128-128-1 ReLU MLP, BF16 operands with FP32 accumulation, trained
+ * with binary cross-entropy and Adam by this library's kernels.  The
+ * parameter vector is 20,865 floats: W1[32][128], b1[128], W2[128][128],
+ * b2[128], w3[128], b3. ---- */
+CCP_API long long dct_mlp_create(unsigned long long seed);
+/* copy the parameters out (get_out) and / or in (set_in); returns count */
+CCP_API int  dct_mlp_params(long long h, float *get_out, const float *set_in);
+/* gradient of the mean loss over n samples (X n x 32, T n in {0,1}) */
+CCP_API int  dct_mlp_grad(long long h, const float *X, const float *T, int n,
+                          float *grad_out);
+CCP_API int  dct_mlp_train(long long h, const float *X, const float *T, int n,
+                           int epochs, int batch, float lr,
+                           unsigned long long seed);
+/* logits of n samples */
+CCP_API int  dct_mlp_predict(long long h, const float *X, int n, float *out);
+CCP_API int  dct_mlp_free(long long h);
+
 /* No counterpart in the reference.  Gain (role 0) or loss (role 1) map of
  * a Hamming / Lee cell for callers that may not allocate device memory —
  * a framework whose own allocator must own every buffer, a service that
@@ -196,6 +214,13 @@ CCP_API int  dct_b200_field_noalloc(int problem, int n, const int *ax, int R,
                                     int mu, int role, const uint16_t *cnt,
                                     int32_t *map, long long stream);
 /* after dct_transform(init, 3): words [off, off+len) of distance layer d */
+/* (the two below have no counterpart in the reference; they feed the
+ * learned ruin proposal) per word: a log2 histogram of the map over its
+ * ball (bin 0: v <= 0, 1: v == 1, 2: 2..3, ...; nbins <= 32) */
+CCP_API int  dct_b200_ball_map_hist(const long long *words, int nw, int nbins,
+                                    int32_t *out);
+/* after dct_transform(init, 3): the R+1 layer values at each of k words */
+CCP_API int  dct_b200_layers_at(const long long *idx, int k, int32_t *out);
 CCP_API int  dct_b200_read_layer(int d, long long off, long long len, int32_t *out);
 
 #ifdef __cplusplus
