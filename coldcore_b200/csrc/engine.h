@@ -145,9 +145,9 @@ int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
                   int mode, int target, int32_t *out, bool zeroed,
                   cudaStream_t s);
 int pick_split(long long len, int nb);
-int launch_ball_map_hist(const WalkArgs &w, const long long *dwords, int nb,
-                         const int32_t *map, int nbins, int32_t *out,
-                         cudaStream_t s);
+int launch_ball_hist(const WalkArgs &w, const long long *dwords, int nb,
+                     const int32_t *map, int src, int nbins, int32_t *out,
+                     cudaStream_t s);
 int launch_layers_at(const int32_t *layers, long long plane, int R1,
                      const long long *idx, int k, int32_t *out,
                      cudaStream_t s);

@@ -1021,9 +1021,10 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
   return n;
 }
 
-int dct_b200_ball_map_hist(const long long *words, int nw, int nbins,
-                           int32_t *out) {
-  if (!S.live || nbins < 1 || nbins > 32 || !out) return -1;
+int dct_b200_ball_hist(const long long *words, int nw, int src, int nbins,
+                       int32_t *out) {
+  if (!S.live || nbins < 1 || nbins > 32 || !out || (src != 0 && src != 1))
+    return -1;
   if (nw <= 0) return 0;
   if (!valid_words(words, nw)) return -1;
   const WalkArgs w = walk_args();
@@ -1032,8 +1033,8 @@ int dct_b200_ball_map_hist(const long long *words, int nw, int nbins,
     const int nb = (int)std::min<long long>(cap, nw - off);
     int rc = stage_words(words + off, nb);
     if (rc) return rc;
-    rc = launch_ball_map_hist(w, S.d_words, nb, S.layers, nbins, S.d_out,
-                              g_stream);
+    rc = launch_ball_hist(w, S.d_words, nb, S.layers, src, nbins, S.d_out,
+                          g_stream);
     if (rc) return rc;
     CC_CK(cudaMemcpyAsync(S.h_out, S.d_out, (size_t)nb * nbins * 4,
                           cudaMemcpyDeviceToHost, g_stream));

@@ -123,12 +123,13 @@ k_gather(const WalkArgs a, const long long *words, int split, int mode,
   }
 }
 
-// out[wi][b] = #{x in B(w_i) : bin(map[x]) == b}, log2 bins: 0 for v <= 0,
-// 1 for v == 1, 2 for 2..3, 3 for 4..7, ... clipped to nbins - 1
+// out[wi][b] = #{x in B(w_i) : bin(x) == b}.  src 0 bins the map in log2
+// steps (0 for v <= 0, 1 for v == 1, 2 for 2..3, 3 for 4..7, ...), src 1
+// bins cnt linearly (cnt == b); both clip to nbins - 1.
 template <bool GRID>
 __global__ void __launch_bounds__(256)
-k_ball_map_hist(const WalkArgs a, const long long *words, int split,
-                const int32_t *map, int nbins, int32_t *out) {
+k_ball_hist(const WalkArgs a, const long long *words, int split,
+            const int32_t *map, int src, int nbins, int32_t *out) {
   __shared__ WordSmem s;
   __shared__ int32_t hist[32];
   const int wi = blockIdx.x / split, seg = blockIdx.x % split;
@@ -140,8 +141,13 @@ k_ball_map_hist(const WalkArgs a, const long long *words, int split,
        t += step) {
     const long long x = walk_word<GRID>(a, w, t, s);
     if (x < 0) continue;
-    const int32_t v = map[x];
-    const int b = v <= 0 ? 0 : min(nbins - 1, 32 - __clz(v));
+    int b;
+    if (src == 0) {
+      const int32_t v = map[x];
+      b = v <= 0 ? 0 : min(nbins - 1, 32 - __clz(v));
+    } else {
+      b = min(nbins - 1, (int)a.cnt[x]);
+    }
     atomicAdd(&hist[b], 1);
   }
   __syncthreads();
@@ -149,19 +155,19 @@ k_ball_map_hist(const WalkArgs a, const long long *words, int split,
     if (hist[b]) atomicAdd(&out[(long long)wi * nbins + b], hist[b]);
 }
 
-int launch_ball_map_hist(const WalkArgs &w, const long long *dwords, int nb,
-                         const int32_t *map, int nbins, int32_t *out,
-                         cudaStream_t s) {
+int launch_ball_hist(const WalkArgs &w, const long long *dwords, int nb,
+                     const int32_t *map, int src, int nbins, int32_t *out,
+                     cudaStream_t s) {
   if (nb <= 0) return 0;
   const int split = pick_split(w.len, nb);
   CC_CK(cudaMemsetAsync(out, 0, (size_t)nb * nbins * 4, s));
   const dim3 grid((unsigned)nb * split);
   if (w.g.prob == kGrid)
-    k_ball_map_hist<true><<<grid, 256, 0, s>>>(w, dwords, split, map, nbins,
-                                               out);
+    k_ball_hist<true><<<grid, 256, 0, s>>>(w, dwords, split, map, src, nbins,
+                                           out);
   else
-    k_ball_map_hist<false><<<grid, 256, 0, s>>>(w, dwords, split, map, nbins,
-                                                out);
+    k_ball_hist<false><<<grid, 256, 0, s>>>(w, dwords, split, map, src,
+                                            nbins, out);
   CC_CK(cudaGetLastError());
   return 0;
 }

@@ -88,7 +88,7 @@ def _bind(path):
         "dct_b200_read_layer": (I, [I, _LL, _LL, _I32P]),
         "dct_b200_read_map": (I, [_LL, _LL, _I32P]),
         "dct_b200_set_timing": (I, [I]),
-        "dct_b200_ball_map_hist": (I, [_LLP, I, I, _I32P]),
+        "dct_b200_ball_hist": (I, [_LLP, I, I, I, _I32P]),
         "dct_b200_layers_at": (I, [_LLP, I, _I32P]),
         "dct_b200_last_timings": (I, [ctypes.POINTER(ctypes.c_float), I]),
     }
@@ -284,13 +284,16 @@ class GpuBackend:
         n = self._lib.dct_b200_last_timings(buf, 64)
         return [float(buf[i]) for i in range(min(n, 64))]
 
-    def ball_map_hist(self, idx, nbins=8):
-        """Per word: log2 histogram of the current map over its ball."""
+    def ball_hist(self, idx, src=0, nbins=8):
+        """Per word, a histogram over its ball: src 0 = the current map in
+        log2 bins (0: v <= 0, 1: v == 1, 2: 2..3, ...), src 1 = cnt in
+        linear bins; the last bin takes everything above."""
         idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
         out = np.zeros((len(idx), nbins), dtype=np.int32)
         if len(idx):
-            _check("ball_map_hist", self._lib.dct_b200_ball_map_hist(
-                _p(idx), len(idx), int(nbins), _p(out, ctypes.c_int32)))
+            _check("ball_hist", self._lib.dct_b200_ball_hist(
+                _p(idx), len(idx), int(src), int(nbins),
+                _p(out, ctypes.c_int32)))
         return out
 
     def layers_at(self, idx):

@@ -215,10 +215,12 @@ CCP_API int  dct_b200_field_noalloc(int problem, int n, const int *ax, int R,
                                     int32_t *map, long long stream);
 /* after dct_transform(init, 3): words [off, off+len) of distance layer d */
 /* (the two below have no counterpart in the reference; they feed the
- * learned ruin proposal) per word: a log2 histogram of the map over its
- * ball (bin 0: v <= 0, 1: v == 1, 2: 2..3, ...; nbins <= 32) */
-CCP_API int  dct_b200_ball_map_hist(const long long *words, int nw, int nbins,
-                                    int32_t *out);
+ * learned ruin proposal) per word, a histogram over its ball: src 0 bins
+ * the current map in log2 steps (bin 0: v <= 0, 1: v == 1, 2: 2..3, ...),
+ * src 1 bins cnt linearly (bin b: cnt == b); the last of nbins (<= 32)
+ * bins takes everything above.  out is nw x nbins. */
+CCP_API int  dct_b200_ball_hist(const long long *words, int nw, int src,
+                                int nbins, int32_t *out);
 /* after dct_transform(init, 3): the R+1 layer values at each of k words */
 CCP_API int  dct_b200_layers_at(const long long *idx, int k, int32_t *out);
 CCP_API int  dct_b200_read_layer(int d, long long off, long long len, int32_t *out);

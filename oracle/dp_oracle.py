@@ -125,6 +125,15 @@ class OracleBackend:
         self._A = np.zeros((self.nlayers, size), dtype=self.dtype)
         self.bpos, self.bdel = ball_columns(self.axes, self.R, problem)
         self.ball_len = len(self.bpos)
+        # search-protocol attributes (dp.py:97-98)
+        self.indep_dist = 2 * R if problem in ("hamming", "lee") else None
+        self.supports_hist = True
+
+    def index_word(self, idx):
+        return self.space.digits(np.atleast_1d(np.asarray(idx, np.int64)))
+
+    def word_index(self, digs):
+        return self.space.index(np.asarray(digs, dtype=np.int64))
 
     # ------------------------------------------------ axis passes
     def _fibres(self, j):
