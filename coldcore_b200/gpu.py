@@ -253,6 +253,10 @@ class GpuBackend:
         idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
         _check("set_code", self._lib.dct_set_code(_p(idx), len(idx)))
 
+    def stage_code(self, idx):
+        """Upload a code for ``layers_map(0)`` without touching cnt."""
+        self._set_code(idx)
+
     def recount(self, idx):
         self._set_code(idx)
         _check("transform(code->cnt)", self._lib.dct_transform(0, 2))

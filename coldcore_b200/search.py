@@ -104,9 +104,10 @@ class Searcher:
     None`` and ``observe(searcher, mode, pre, post, new_best)``; used by
     ``select="learned"``.  ``move_log``: called once per LNS round as
     ``move_log(searcher, event, **info)`` with event ``"pre"`` (before the
-    ruin, with ``k`` and ``mode``), ``"ruin"`` (with the removed positions)
-    and ``"post"`` (after the accept/reject rule, with ``pre``, ``post``
-    and ``new_best``)."""
+    ruin, with ``k`` and ``mode``), ``"ruin"`` (with the removed positions),
+    ``"repair"`` (after the greedy repair, with the repaired ``code``) and
+    ``"post"`` (after the accept/reject rule, with ``pre``, ``post`` (the
+    repaired count), ``after`` and ``new_best``)."""
 
     def __init__(self, backend, seed=1, deadline=None, on_log=None,
                  on_solved=None, proposer=None, move_log=None):
@@ -397,6 +398,8 @@ class Searcher:
                     self.move_log(self, "ruin", pick=np.asarray(pick))
             self.ruin(k, mode, pick=pick)
             self.greedy_fill(M)
+            if self.move_log is not None:
+                self.move_log(self, "repair", code=self.code)
             self.stats["rounds"] += 1
             r += 1
             post = self.uncov
