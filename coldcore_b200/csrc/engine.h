@@ -145,6 +145,27 @@ int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
                   int mode, int target, int32_t *out, bool zeroed,
                   cudaStream_t s);
 int pick_split(long long len, int nb);
+// set side (setside.cu): list {x : pred(cnt[x])} as packed digit words, then
+// count, per candidate, the listed words within distance R
+int launch_list_pred(const Geometry &g, const uint16_t *cnt, int mode,
+                     int target, unsigned long long *out, long long cap,
+                     unsigned long long *found, cudaStream_t s);
+int launch_gather_set(const Geometry &g, const long long *dcand, int nc,
+                      const unsigned long long *Z, long long zn, int32_t *out,
+                      bool zeroed, cudaStream_t s);
+// swap evaluation fast path: per drop its loss and the list of its ball
+// words at exactly mu (two walks and a segment scan), then per candidate
+// the listed words of its drop within distance R
+int launch_seg_scan(const int32_t *cnt, int n, long long cap, int32_t *offs,
+                    int32_t *cursor, cudaStream_t s);
+int launch_drop_walks(const WalkArgs &w, const long long *ddrops, int k,
+                      int32_t *loss, int32_t *nmu, int32_t *offs,
+                      int32_t *cursor, long long cap, long long *list,
+                      cudaStream_t s);
+int launch_swap_corr(const Geometry &g, int k, const long long *dcand,
+                     const int32_t *dcoff, const int32_t *offs,
+                     const long long *list, long long cap, int32_t *gain,
+                     cudaStream_t s);
 int launch_ball_hist(const WalkArgs &w, const long long *dwords, int nb,
                      const int32_t *map, int src, int nbins, int32_t *out,
                      cudaStream_t s);

@@ -87,6 +87,22 @@ struct State {
   long long bytes_dev = 0, bytes_host = 0;
   unsigned long long dd_last = 0;
   bool layered_out = false;        // last transform left N_0..N_R
+  // set side (setside.cu): the listed predicate set Z, cached per cnt state
+  bool set_ok = false;             // support table proven == metric ball
+  int set_policy = 1;              // DCT_SET_GATHER: 0 off, 1 auto, 2 force
+  long long set_min = -1;          // DCT_SET_MIN: walk size that tries it
+  long long set_ratio = 2;         // DCT_SET_RATIO: set side while |Z| <= r|B|
+  unsigned long long *zbuf = nullptr, *d_found = nullptr;
+  long long zcap = 0, zcap_max = 0;
+  unsigned long long cnt_ver = 1;  // bumped by every cnt mutation
+  int z_mode = -1, z_target = 0, z_mu = 0;
+  unsigned long long z_ver = 0;
+  bool z_valid = false;
+  long long z_n = 0;
+  // swap_eval fast path: packed host/device staging and the drop lists
+  char *h_swap = nullptr, *d_swap = nullptr;
+  long long *d_list = nullptr;
+  long long lcap = 0;
   Plan plans[3][4];                // [init_mode][out_mode]
   bool plan_ok[3][4] = {{false}};
   bool tuned[3][4] = {{false}};
@@ -242,7 +258,8 @@ void free_all() {
   F(S.layers); F(S.cnt); F(S.owner); F(S.tbl); F(S.tbl2); F(S.d_code);
   F(S.d_bounds);
   F(S.d_words); F(S.d_out); F(S.d_scalar); F(S.d_hist); F(S.d_ext32);
-  F(S.d_ext64); F(S.d_extv);
+  F(S.d_ext64); F(S.d_extv); F(S.zbuf); F(S.d_found);
+  F(S.d_swap); F(S.d_list); FH(S.h_swap);
   FH(S.h_words); FH(S.h_out); FH(S.h_scalar);
   S.~State();
   new (&S) State();
@@ -567,19 +584,158 @@ int finish_init(long long *bytes) {
   return 0;
 }
 
+// Is the support table exactly the metric ball?  Every pattern must move
+// distinct axes by admissible deltas within radius R, the patterns must be
+// distinct, and their number must equal the ball's cardinality (coldcore
+// dct_hc.cu:158-204 states the same test).  Only then may a gather count
+// listed words by distance instead of walking the table.
+bool table_is_ball(const std::vector<int32_t> &soa, int slots, long long len) {
+  const int n = S.g.n, R = S.g.R, prob = S.g.prob;
+  if (n > 16) return false;
+  for (int i = 0; i < n; i++)
+    if (S.g.ax[i] > 16) return false;
+  auto weight = [&](int pos, int d) -> int {      // -1: inadmissible
+    const int a = S.g.ax[pos];
+    if (d < 1 || d >= a) return -1;
+    const int c = std::min(d, a - d);
+    if (prob == kHamming) return 1;
+    if (prob == kLee) return c <= R ? c : -1;
+    return c <= R ? 0 : -1;                        // L-infinity
+  };
+  std::vector<unsigned long long> keys;
+  keys.reserve((size_t)len);
+  for (long long t = 0; t < len; t++) {
+    unsigned seen = 0;
+    unsigned long long key = 0;
+    int w = 0;
+    for (int k = 0; k < slots; k++) {
+      const int32_t c = soa[(size_t)k * len + t];
+      if (!c) continue;
+      const int pos = c >> 24, d = c & 0xFFFFFF;
+      if (pos >= n || ((seen >> pos) & 1u)) return false;
+      seen |= 1u << pos;
+      const int e = weight(pos, d);
+      if (e < 0) return false;
+      w += e;
+      key |= (unsigned long long)d << (4 * pos);
+    }
+    if (w > R) return false;
+    keys.push_back(key);
+  }
+  std::sort(keys.begin(), keys.end());
+  if (std::adjacent_find(keys.begin(), keys.end()) != keys.end()) return false;
+  // cardinality: coefficients 0..W of prod_i (1 + sum_d t^weight(i, d))
+  const int W = (prob == kHamming || prob == kLee) ? R : 0;
+  std::vector<long double> poly(W + 1, 0.0L);
+  poly[0] = 1.0L;
+  for (int i = 0; i < n; i++) {
+    std::vector<long double> nx(W + 1, 0.0L);
+    for (int w = 0; w <= W; w++) {
+      if (poly[w] == 0) continue;
+      nx[w] += poly[w];
+      for (int d = 1; d < S.g.ax[i]; d++) {
+        const int e = weight(i, d);
+        if (e >= 0 && w + e <= W) nx[w + e] += poly[w];
+      }
+    }
+    poly.swap(nx);
+  }
+  long double tot = 0;
+  for (int w = 0; w <= W; w++) tot += poly[w];
+  return tot == (long double)len;
+}
+
+void set_side_init(const std::vector<int32_t> &soa, int slots) {
+  const char *sp = getenv("DCT_SET_GATHER");
+  const char *sm = getenv("DCT_SET_MIN");
+  const char *sr = getenv("DCT_SET_RATIO");
+  S.set_policy = sp ? atoi(sp) : 1;
+  S.set_min = sm ? atoll(sm) : -1;
+  S.set_ratio = sr ? std::max(1LL, atoll(sr)) : 2;
+  S.set_ok = S.set_policy != 0 && table_is_ball(soa, slots, S.len);
+  S.zcap_max = std::min<long long>(S.g.space, 1LL << 27);
+  S.z_mode = -1;
+}
+
+// the walk of nb candidates reads nb*|B| counters: worth trying the list?
+bool want_set(int mode, int target, int nb) {
+  if (!S.set_ok || !(mode == kPredDef || (mode == kPredEq && target == 0)))
+    return false;
+  if (S.set_policy == 2) return true;
+  const long long walk = (long long)nb * S.len;
+  const long long lim = S.set_min >= 0 ? S.set_min
+                        : std::max<long long>(S.g.space / 8, 1LL << 21);
+  return walk >= lim;
+}
+
+// List Z = {x : pred(cnt[x])} for the current cnt, unless it is listed
+// already.  Returns 1 when the list is usable (|Z| <= ratio*|B|), 0 when
+// the caller must walk, negative on error.
+int ensure_zlist(int mode, int target) {
+  if (S.z_mode == mode && S.z_target == target && S.z_mu == g_mu &&
+      S.z_ver == S.cnt_ver)
+    return S.z_valid ? 1 : 0;
+  const long long lim = std::min(S.len * S.set_ratio, S.zcap_max);
+  if (!S.d_found) CC_CK(cudaMalloc(&S.d_found, 8));
+  long long want = std::min<long long>(std::max<long long>(S.len / 4, 4096),
+                                       1LL << 22);
+  want = std::min(want, lim);
+  for (;;) {
+    if (S.zcap < want) {
+      if (S.zbuf) CC_CK(cudaFree(S.zbuf));
+      S.zbuf = nullptr;
+      S.zcap = 0;
+      CC_CK(cudaMalloc(&S.zbuf, (size_t)want * 8));
+      S.zcap = want;
+    }
+    Geometry g = S.g;
+    g.mu = g_mu;
+    int rc = launch_list_pred(g, S.cnt, mode, target, S.zbuf, S.zcap,
+                              S.d_found, g_stream);
+    if (rc) return rc;
+    CC_CK(cudaMemcpyAsync(S.h_scalar + 8, S.d_found, 8,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    const long long found = S.h_scalar[8];
+    S.stats[2]++;
+    if (found > S.zcap && found <= lim) { want = found; continue; }
+    S.z_mode = mode; S.z_target = target; S.z_mu = g_mu;
+    S.z_ver = S.cnt_ver;
+    S.z_n = found;
+    S.z_valid = found <= lim;
+    if (!S.z_valid) S.stats[3]++;
+    return S.z_valid ? 1 : 0;
+  }
+}
+
+// launch the gather of nb staged words into dout (set side or walk)
+int gather_launch(int mode, int target, int nb, const long long *dw,
+                  int32_t *dout, bool zeroed) {
+  const int zs = want_set(mode, target, nb) ? ensure_zlist(mode, target) : 0;
+  if (zs < 0) return zs;
+  if (zs == 1) {
+    S.stats[0]++;
+    if (S.z_n > 32768) S.stats[7]++;
+    Geometry g = S.g;
+    g.mu = g_mu;
+    return launch_gather_set(g, dw, nb, S.zbuf, S.z_n, dout, zeroed,
+                             g_stream);
+  }
+  S.stats[1]++;
+  return launch_gather(walk_args(), dw, nb, mode, target, dout, zeroed,
+                       g_stream);
+}
+
 int gather_impl(const long long *words, int nwords, int mode, int target,
                 int32_t *out) {
   if (nwords <= 0) return 0;
   if (!out || !valid_words(words, nwords)) return -1;
-  const WalkArgs w = walk_args();
   for (long long off = 0; off < nwords; off += kStageCap) {
     const int nb = (int)std::min<long long>(kStageCap, nwords - off);
     int rc = stage_words(words + off, nb);
     if (rc) return rc;
-    rc = launch_gather(w, S.d_words, nb, mode, target, S.d_out, false,
-                       g_stream);
+    rc = gather_launch(mode, target, nb, S.d_words, S.d_out, false);
     if (rc) return rc;
-    S.stats[1]++;
     CC_CK(cudaMemcpyAsync(S.h_out, S.d_out, (size_t)nb * 4,
                           cudaMemcpyDeviceToHost, g_stream));
     CC_CK(cudaStreamSynchronize(g_stream));
@@ -592,6 +748,7 @@ int gather_impl(const long long *words, int nwords, int mode, int target,
 int update_impl(const long long *words, int nwords, int delta,
                 unsigned long long *trans) {
   const WalkArgs w = walk_args();
+  S.cnt_ver++;
   for (long long off = 0; off < nwords; off += kStageCap) {
     const int nb = (int)std::min<long long>(kStageCap, nwords - off);
     int rc;
@@ -651,6 +808,7 @@ int dct_init3(int problem, int n, const int *ax, int R,
   if (unpack_v1(ballpat, balllen, soa, &slots)) { free_all(); return -1; }
   rc = upload_table(soa, slots, &S.tbl, &S.slots);
   if (rc) return rc;
+  set_side_init(soa, slots);
   return finish_init(bytes);
 }
 
@@ -673,6 +831,7 @@ int dct_init3w(int problem, int n, const int *ax, int R, const int32_t *tbl,
     }
   rc = upload_table(soa, slots, &S.tbl, &S.slots);
   if (rc) return rc;
+  set_side_init(soa, slots);
   return finish_init(bytes);
 }
 
@@ -765,7 +924,10 @@ int dct_transform(int init_mode, int out_mode) {
   if (rc) return rc;
   CC_CK(cudaStreamSynchronize(g_stream));
   S.layered_out = out_mode == 3;
-  if (out_mode == 2) set_active(S.uploaded, S.codeM);
+  if (out_mode == 2) {
+    set_active(S.uploaded, S.codeM);
+    S.cnt_ver++;
+  }
   return 0;
 }
 
@@ -815,6 +977,76 @@ int dct_ball_gather_mu(const long long *words, int nwords, int role,
   return gather_impl(words, nwords, role == 0 ? kPredDef : kPredCrit, 0, out);
 }
 
+// Read-only swap evaluation with one synchronisation (coldcore
+// dct_hc.cu:882-963): loss[i] and the list of drop i's ball words at exactly
+// mu come from two walks of its ball; gain[j] is the role-0 gather of cand j
+// on the current cnt (set side or walk) plus the listed words of its drop
+// within distance R, the words that removing the drop makes deficient.
+// Returns 1 when the list overflowed (the caller falls back), else 0 or an
+// error code.
+int swap_eval_fast(const long long *drops, int k, const long long *cand,
+                   const long long *off, int32_t *gain, int32_t *loss) {
+  constexpr long long kMaxN = 65536;
+  // staging: [cand kMaxN x 8][drops kMaxN x 8][coff (kMaxN + 1) x 4]
+  // results: [gain kMaxN x 4][loss kMaxN x 4][nmu x 4][offs (+1) x 4]
+  //          [cursor x 4]
+  const size_t in_drop = kMaxN * 8, in_coff = 2 * kMaxN * 8;
+  const size_t in_bytes = in_coff + (kMaxN + 1) * 4;
+  const size_t r0 = in_bytes + 64;           // results start, 16-aligned
+  const size_t r_loss = r0 + kMaxN * 4, r_nmu = r_loss + kMaxN * 4;
+  const size_t r_offs = r_nmu + kMaxN * 4, r_cur = r_offs + (kMaxN + 1) * 4;
+  const size_t total_bytes = r_cur + kMaxN * 4 + 64;
+  if (!S.d_swap) {
+    CC_CK(cudaMalloc(&S.d_swap, total_bytes));
+    CC_CK(cudaHostAlloc((void **)&S.h_swap, total_bytes,
+                        cudaHostAllocDefault));
+    S.lcap = std::min<long long>(std::max<long long>(4 * S.len, 1 << 16),
+                                 1LL << 22);
+    CC_CK(cudaMalloc(&S.d_list, (size_t)S.lcap * 8));
+  }
+  const long long nc = off[k];
+  char *h = S.h_swap, *d = S.d_swap;
+  if (nc) memcpy(h, cand, (size_t)nc * 8);
+  memcpy(h + in_drop, drops, (size_t)k * 8);
+  int32_t *hc = reinterpret_cast<int32_t *>(h + in_coff);
+  for (int i = 0; i <= k; i++) hc[i] = (int32_t)off[i];
+  const long long *d_cand = reinterpret_cast<const long long *>(d);
+  const long long *d_drop = reinterpret_cast<const long long *>(d + in_drop);
+  const int32_t *d_coff = reinterpret_cast<const int32_t *>(d + in_coff);
+  int32_t *d_gain = reinterpret_cast<int32_t *>(d + r0);
+  int32_t *d_loss = reinterpret_cast<int32_t *>(d + r_loss);
+  int32_t *d_nmu = reinterpret_cast<int32_t *>(d + r_nmu);
+  int32_t *d_offs = reinterpret_cast<int32_t *>(d + r_offs);
+  int32_t *d_cur = reinterpret_cast<int32_t *>(d + r_cur);
+  CC_CK(cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, g_stream));
+  CC_CK(cudaMemsetAsync(d + r0, 0, r_offs - r0, g_stream));
+  WalkArgs w = walk_args();
+  int rc = launch_drop_walks(w, d_drop, k, d_loss, d_nmu, d_offs, d_cur,
+                             S.lcap, S.d_list, g_stream);
+  if (rc) return rc;
+  if (nc) {
+    int gm, gt;
+    mode_role(0, &gm, &gt);
+    rc = gather_launch(gm, gt, (int)nc, d_cand, d_gain, true);
+    if (rc) return rc;
+    Geometry g = S.g;
+    g.mu = g_mu;
+    rc = launch_swap_corr(g, k, d_cand, d_coff, d_offs, S.d_list, S.lcap,
+                          d_gain, g_stream);
+    if (rc) return rc;
+  }
+  // gain, loss and the list total (offs[k]) in one copy
+  CC_CK(cudaMemcpyAsync(h + r0, d + r0, r_offs - r0 + (size_t)(k + 1) * 4,
+                        cudaMemcpyDeviceToHost, g_stream));
+  CC_CK(cudaStreamSynchronize(g_stream));
+  const int32_t listed = reinterpret_cast<int32_t *>(h + r_offs)[k];
+  if (listed > S.lcap) return 1;
+  memcpy(loss, h + r_loss, (size_t)k * 4);
+  if (nc) memcpy(gain, h + r0, (size_t)nc * 4);
+  S.stats[4]++;
+  return 0;
+}
+
 int dct_swap_eval(const long long *drops, int k, const long long *cand,
                   const long long *off, int32_t *gain, int32_t *loss) {
   if (!S.live) return -1;
@@ -827,6 +1059,10 @@ int dct_swap_eval(const long long *drops, int k, const long long *cand,
   if (!valid_words(drops, k) || !valid_words(cand, nc)) return -1;
   for (int i = 0; i < k; i++)
     if (S.active.find(drops[i]) == S.active.end()) return -1;
+  if (S.set_ok) {
+    const int rc = swap_eval_fast(drops, k, cand, off, gain, loss);
+    if (rc <= 0) return rc;                  // done (0) or an error
+  }
   // drop / gather / undo per drop word; cnt ends where it started
   S.stats[5]++;
   int lm, lt, gm, gt;
@@ -872,6 +1108,13 @@ int dct_stats(long long *out, int n) {
 
 long long dct_count_eq(int target) {
   if (!S.live) return -1;
+  // the zero-word list of a set-side gather already counted them
+  if (target == 0 && S.z_valid && S.z_ver == S.cnt_ver &&
+      (S.z_mode == kPredEq ? S.z_target == 0
+                           : (S.z_mode == kPredDef && S.z_mu == 1))) {
+    S.stats[6]++;
+    return S.z_n;
+  }
   CC_CK(cudaMemsetAsync(S.d_scalar, 0, 8, g_stream));
   int rc = launch_cnt_reduce(S.cnt, S.g.space, kPredEq, target, g_mu,
                              S.d_scalar, g_stream);

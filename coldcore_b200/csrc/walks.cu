@@ -190,6 +190,76 @@ int launch_layers_at(const int32_t *layers, long long plane, int R1,
   return 0;
 }
 
+// swap evaluation, first walk: per drop word, its loss (critical ball words)
+// and nmu = its ball words at exactly mu, the words that become deficient
+// when one copy of the drop is removed
+template <bool GRID>
+__global__ void __launch_bounds__(256)
+k_drop_count(const WalkArgs a, const long long *drops, int split,
+             int32_t *loss, int32_t *nmu) {
+  __shared__ WordSmem s;
+  const int wi = blockIdx.x / split, seg = blockIdx.x % split;
+  const long long w = drops[wi];
+  word_setup(a.g, w, s);
+  long long lo = 0, at = 0;
+  const long long step = (long long)split * blockDim.x;
+  for (long long t = (long long)seg * blockDim.x + threadIdx.x; t < a.len;
+       t += step) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x < 0) continue;
+    const int c = (int)a.cnt[x];
+    lo += c >= 1 && c <= a.g.mu;
+    at += c == a.g.mu;
+  }
+  lo = block_sum(lo);
+  if (threadIdx.x == 0 && lo) atomicAdd(&loss[wi], (int32_t)lo);
+  at = block_sum(at);
+  if (threadIdx.x == 0 && at) atomicAdd(&nmu[wi], (int32_t)at);
+}
+
+// second walk: the words at exactly mu, into the drop's segment of `list`
+// (cursor[i] starts at the segment's offset); slots past cap are dropped and
+// the caller, seeing the total above cap, falls back
+template <bool GRID>
+__global__ void __launch_bounds__(256)
+k_drop_list(const WalkArgs a, const long long *drops, int split,
+            int32_t *cursor, long long cap, long long *list) {
+  __shared__ WordSmem s;
+  const int wi = blockIdx.x / split, seg = blockIdx.x % split;
+  const long long w = drops[wi];
+  word_setup(a.g, w, s);
+  const long long step = (long long)split * blockDim.x;
+  for (long long t = (long long)seg * blockDim.x + threadIdx.x; t < a.len;
+       t += step) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x < 0 || (int)a.cnt[x] != a.g.mu) continue;
+    const int slot = atomicAdd(&cursor[wi], 1);
+    if (slot < cap) list[slot] = x;
+  }
+}
+
+int launch_drop_walks(const WalkArgs &w, const long long *ddrops, int k,
+                      int32_t *loss, int32_t *nmu, int32_t *offs,
+                      int32_t *cursor, long long cap, long long *list,
+                      cudaStream_t s) {
+  if (k <= 0) return 0;
+  const int split = pick_split(w.len, k);
+  const dim3 grid((unsigned)k * split);
+  const bool gp = w.g.prob == kGrid;
+  if (gp) k_drop_count<true><<<grid, 256, 0, s>>>(w, ddrops, split, loss, nmu);
+  else k_drop_count<false><<<grid, 256, 0, s>>>(w, ddrops, split, loss, nmu);
+  CC_CK(cudaGetLastError());
+  int rc = launch_seg_scan(nmu, k, cap, offs, cursor, s);
+  if (rc) return rc;
+  if (gp)
+    k_drop_list<true><<<grid, 256, 0, s>>>(w, ddrops, split, cursor, cap, list);
+  else
+    k_drop_list<false><<<grid, 256, 0, s>>>(w, ddrops, split, cursor, cap,
+                                            list);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
 // blocks per word so that single-word walks still fill the GPU
 int pick_split(long long len, int nb) {
   long long cover = (len + 255) / 256;

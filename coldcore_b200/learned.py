@@ -14,11 +14,13 @@ Pieces:
     the uncovered words of its own ball, so this histogram sees the
     uncovered words of B_2R(c);
   - a histogram of the coverage counts cnt over B_R(c);
-  - the per-distance layer counts N_d(c) of the uncovered words and of
-    the code (d = 0..R, from ``layers_map`` + ``layers_at``), each scaled
-    by the sphere size;
-  - two ranks among the incumbents: uncovered words within R, and ball
-    words of positive gain.
+  - the per-distance layer counts N_d(c) of the critical words (covered
+    exactly mu times: the words c alone covers, by their distance from c)
+    and of the code (d = 0..R, from ``layers_map`` + ``layers_at``), each
+    scaled by the sphere size;
+  - two ranks among the incumbents: the log-gain mass of the ball (how
+    much uncovered territory lies within 2R), and the ball words of
+    positive gain.
   Every feature describes c relative to the current state; none is
   constant across a round, so the model ranks incumbents rather than
   rounds.
@@ -27,14 +29,16 @@ Pieces:
   repair covered more than the code before the ruin and did not put that
   incumbent back, 0 otherwise.
 * :func:`train_scorer`: z-scores the features and fits the GPU MLP
-  (:class:`coldcore_b200.mlp.GpuMlp`).  It reports the held-out AUC, both
-  pooled and within rounds (the ranking a proposal uses).
+  (:class:`coldcore_b200.mlp.GpuMlp`).  It reports the AUC on held-out
+  rounds, pooled (the gate reads this) and within rounds.
 * :class:`LearnedRuin`: the proposer that ``select="learned"`` calls.  It
-  scores every incumbent and draws an anchor from the scores.  It then
-  removes the k incumbents nearest the anchor, breaking ties towards higher
-  scores.  A confidence gate hands the round back to the bandit in two
-  cases: the model's held-out AUC was below ``auc_min``, or the learned
-  rounds' recent rewards fall below half of the fallback rounds'.
+  scores every incumbent and draws k of them without replacement with
+  probabilities softmax(score / temperature) (the Gumbel top-k draw), or,
+  with ``pick="anchor"``, draws one anchor that way and removes the k
+  incumbents nearest it.  A confidence gate hands the round back to the
+  bandit in two cases: the model's held-out AUC was below ``auc_min``, or
+  the learned rounds' recent rewards fall below half of the fallback
+  rounds'.
 """
 import time
 
@@ -93,18 +97,18 @@ class RuinFeatures:
         f[:, 0] = loss / B
         f[:, 1] = _rank(loss)
         b.gain_map()
-        f[:, 2:10] = b.ball_hist(code, 0, _HIST_BINS) / B
+        gh = b.ball_hist(code, 0, _HIST_BINS)
+        f[:, 2:10] = gh / B
         f[:, 10:18] = b.ball_hist(code, 1, _HIST_BINS) / B
         if self.layered:
             nd = min(R + 1, _MAX_D)
             sph = self.sphere[:nd][None, :]
-            b.layers_map(1)                    # uncovered words by distance
-            near = b.layers_at(code)[:, :nd]
-            f[:, 18:18 + nd] = near / sph
+            b.layers_map(2)                    # critical words by distance
+            f[:, 18:18 + nd] = b.layers_at(code)[:, :nd] / sph
             b.stage_code(code)
             b.layers_map(0)                    # the code by distance
             f[:, 24:24 + nd] = b.layers_at(code)[:, :nd] / sph
-            f[:, 30] = _rank(near.sum(axis=1))
+        f[:, 30] = _rank(gh @ np.arange(_HIST_BINS, dtype=np.float64))
         f[:, 31] = _rank(1.0 - f[:, 2].astype(np.float64))
         self.seconds += time.perf_counter() - t0
         self.calls += 1
@@ -200,7 +204,7 @@ class Scorer:
     def __init__(self, mlp, mean, std, heldout_auc=None):
         self.mlp, self.mean, self.std = mlp, mean, std
         self.heldout_auc = heldout_auc
-        self.pooled_auc = self.train_auc = None
+        self.within_auc = self.train_auc = None
 
     def __call__(self, X):
         return self.mlp.predict((np.asarray(X, np.float32) - self.mean) /
@@ -211,8 +215,8 @@ def train_scorer(X, y, groups=None, epochs=30, batch=512, lr=2e-3, seed=0,
                  holdout=0.1):
     """Fit the MLP on logged moves.  The held-out slice is split by round
     (``groups``), so the moves of one round never straddle the split.
-    Returns a :class:`Scorer` whose ``heldout_auc`` is the within-round
-    AUC of the held-out rounds."""
+    Returns a :class:`Scorer` whose ``heldout_auc`` is the pooled AUC of
+    the held-out rounds (``within_auc``: the AUC within those rounds)."""
     X = np.asarray(X, dtype=np.float32)
     y = np.asarray(y, dtype=np.float32)
     rng = np.random.default_rng(seed)
@@ -229,8 +233,8 @@ def train_scorer(X, y, groups=None, epochs=30, batch=512, lr=2e-3, seed=0,
     sc = Scorer(mlp, mean.astype(np.float32), std.astype(np.float32))
     if test.any():
         st = sc(X[test])
-        sc.pooled_auc = auc(st, y[test])
-        sc.heldout_auc = grouped_auc(st, y[test], groups[test])
+        sc.heldout_auc = auc(st, y[test])
+        sc.within_auc = grouped_auc(st, y[test], groups[test])
     sc.train_auc = auc(sc(X[~test][:20000]), y[~test][:20000])
     return sc
 
@@ -238,8 +242,11 @@ def train_scorer(X, y, groups=None, epochs=30, batch=512, lr=2e-3, seed=0,
 class LearnedRuin:
     """The ``select="learned"`` proposer, with its confidence gate."""
 
-    def __init__(self, scorer, features, auc_min=0.55, temperature=0.5,
-                 score_weight=1.0, decay=0.9, seed=0):
+    def __init__(self, scorer, features, auc_min=0.6, temperature=0.5,
+                 score_weight=1.0, decay=0.9, seed=0, pick="topk"):
+        if pick not in ("topk", "anchor"):
+            raise ValueError(f"unknown pick rule {pick!r}")
+        self.pick = pick
         self.scorer, self.features = scorer, features
         self.auc_min = float(auc_min)
         self.temperature = float(temperature)
@@ -270,6 +277,11 @@ class LearnedRuin:
         if z.std() < 1e-4:
             self.stats["gated_flat"] += 1
             return None
+        self.stats["proposed"] += 1
+        if self.pick == "topk":
+            # Gumbel top-k: k draws without replacement, P ~ exp(z / T)
+            gumbel = -np.log(-np.log(self.rng.random(len(z)) + 1e-300))
+            return np.argsort(-(z / self.temperature + gumbel))[:k]
         p = np.exp((z - z.max()) / self.temperature)
         p /= p.sum()
         anchor = int(self.rng.choice(len(z), p=p))
@@ -278,7 +290,6 @@ class LearnedRuin:
         zr = (z - z.mean()) / (z.std() + 1e-9)
         key = (d - self.score_weight * 0.25 * np.tanh(zr) +
                0.5 * self.rng.random(len(z)))
-        self.stats["proposed"] += 1
         return np.argsort(key)[:k]
 
     def observe(self, s, mode, pre, post, new_best):

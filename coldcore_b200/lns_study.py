@@ -11,7 +11,7 @@ Steps, all on the GPU engine:
    :class:`~coldcore_b200.learned.MoveLog` attached, until ``--moves``
    removals are logged.
 3. **Train.** :func:`~coldcore_b200.learned.train_scorer` on the log.  The
-   held-out within-round AUC is reported.
+   AUC on held-out rounds is reported, pooled and within rounds.
 4. **Evaluate.** From each seed's greedy start, a ``budget``-second notch
    descent with ``select="fixed"``, ``"adaptive"`` and ``"learned"``.
    Each run records the wall time at which each verified size was reached.
@@ -151,6 +151,8 @@ def main(argv=None):
     ap.add_argument("--log-budget", type=float, default=600.0)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--selects", default="fixed,adaptive,learned")
+    ap.add_argument("--temperature", type=float, default=0.5)
+    ap.add_argument("--pick", default="topk", choices=("topk", "anchor"))
     ap.add_argument("--out", default=None)
     ap.add_argument("--save-log", default=None)
     ap.add_argument("--load-log", default=None)
@@ -162,7 +164,8 @@ def main(argv=None):
     b = GpuBackend([a.q] * a.n, a.R, "hamming")
     feats = RuinFeatures(b)
     report = {"cell": f"K_{a.q}({a.n},{a.R})", "budget_s": a.budget,
-              "notch_s": a.notch, "kmin": a.kmin, "kmax": a.kmax}
+              "notch_s": a.notch, "kmin": a.kmin, "kmax": a.kmax,
+              "temperature": a.temperature, "pick": a.pick}
     t0 = time.time()
     if a.load_log:
         z = np.load(a.load_log)
@@ -179,14 +182,14 @@ def main(argv=None):
     say("log", report["log"])
     t1 = time.time()
     scorer = train_scorer(X, y, g, epochs=a.epochs)
-    report["train"] = {"heldout_within_round_auc": scorer.heldout_auc,
-                       "heldout_pooled_auc": scorer.pooled_auc,
+    report["train"] = {"heldout_auc": scorer.heldout_auc,
+                       "heldout_within_round_auc": scorer.within_auc,
                        "train_auc": scorer.train_auc,
                        "seconds": round(time.time() - t1, 2)}
     say("train", report["train"])
     runs = evaluate(b, feats, scorer, range(1, a.seeds + 1), a.budget,
                     a.notch, a.selects.split(","), kmin=a.kmin, kmax=a.kmax,
-                    say=say)
+                    say=say, temperature=a.temperature, pick=a.pick)
     report["runs"] = runs
     report["summary"] = summarize(runs)
     say("summary", report["summary"])

@@ -21,9 +21,10 @@ def features(ob, code, n_features=32, bins=8, max_d=6):
     """Features of every incumbent over an ``OracleBackend`` ``ob``.
 
     The slots are: loss/|B|; loss rank/(m-1); log2 gain histogram/|B| (8);
-    cnt histogram/|B| (8); uncovered words at distance d / |S_d| (6);
-    codewords at distance d / |S_d| (6); the rank of the uncovered words
-    within R; the rank of the ball words of positive gain."""
+    cnt histogram/|B| (8); critical words at distance d / |S_d| (6);
+    codewords at distance d / |S_d| (6); the rank of the ball's log-gain
+    mass (sum of bin index x count); the rank of the ball words of positive
+    gain."""
     code = np.asarray(code, dtype=np.int64)
     m, B = len(code), float(ob.ball_len)
     R, axes, prob = ob.R, ob.axes, ob.problem
@@ -43,9 +44,9 @@ def features(ob, code, n_features=32, bins=8, max_d=6):
     for x in range(ob.space.size):
         gain[x] = deficient[ob.ball_indices(x)].sum()
     f = np.zeros((m, n_features), dtype=np.float64)
-    unc_words = words[deficient]
+    crit_words = words[critical]
     code_words = words[code]
-    near = np.zeros(m)
+    mass = np.zeros(m)
     for i, c in enumerate(code):
         ball = ob.ball_indices(c)
         loss[i] = critical[ball].sum()
@@ -53,16 +54,16 @@ def features(ob, code, n_features=32, bins=8, max_d=6):
         gb = np.where(g <= 0, 0, np.minimum(
             bins - 1, np.floor(np.log2(np.maximum(g, 1))) + 1))
         f[i, 2:2 + bins] = np.bincount(gb.astype(int), minlength=bins)[:bins]
+        mass[i] = f[i, 2:2 + bins] @ np.arange(bins)
         cb = np.minimum(cnt[ball], bins - 1)
         f[i, 10:10 + bins] = np.bincount(cb.astype(int), minlength=bins)[:bins]
         if prob in ("hamming", "lee"):
             nd = min(R + 1, max_d)
-            du = _distance(prob, axes, words[c], unc_words)
+            dk = _distance(prob, axes, words[c], crit_words)
             dc = _distance(prob, axes, words[c], code_words)
             for d in range(nd):
-                f[i, 18 + d] = (du == d).sum() / sphere[d]
+                f[i, 18 + d] = (dk == d).sum() / sphere[d]
                 f[i, 24 + d] = (dc == d).sum() / sphere[d]
-            near[i] = (du < nd).sum()
     f[:, 2:18] /= B
     f[:, 0] = loss / B
 
@@ -70,7 +71,6 @@ def features(ob, code, n_features=32, bins=8, max_d=6):
         return np.argsort(np.argsort(v, kind="stable")) / max(1, m - 1)
 
     f[:, 1] = rank(loss)
-    if prob in ("hamming", "lee"):
-        f[:, 30] = rank(near)
+    f[:, 30] = rank(mass)
     f[:, 31] = rank(1.0 - f[:, 2].astype(np.float32).astype(np.float64))
     return f.astype(np.float32), uncov
