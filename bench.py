@@ -20,6 +20,9 @@ roofline : the dominant launch: its algorithmic bytes (cnt / layers read,
 cpu_baseline : the C restatement of the reference's CPU axis DP on every
         host thread (oracle/cport), a bounded sample of the same cell.
 
+lns   : (1 GPU) LNS time-to-verified-size on K_3(14,3), learned ruin
+        proposal against plain LNS from the same greedy start, one seed.
+
 --impl reference runs that CPU restatement alone (rank 0), on the same
 cell, metric and unit: each step one transform of the cell, rotating
 recount / gain / loss.
@@ -380,6 +383,37 @@ def measure_batch(args, dist):
     return out
 
 
+def measure_lns(args):
+    """LNS time-to-verified-size on K_3(14,3) (4.78M words, R = 3), one
+    seed: plain LNS moves are logged on other seeds and the MLP is trained
+    on them; then, from one greedy start, a plain descent (record mix) and
+    a learned-ruin descent run for the same wall-time budget.  The ratio is
+    the learned run's time to the plain run's best size over the plain
+    run's time to it (coldcore_b200.lns_study runs the multi-seed form)."""
+    from coldcore_b200.gpu import GpuBackend
+    from coldcore_b200.learned import RuinFeatures, train_scorer
+    from coldcore_b200.lns_study import evaluate, log_moves
+    t0 = time.perf_counter()
+    with GpuBackend([3] * 14, 3) as b:
+        feats = RuinFeatures(b)
+        mlog = log_moves(b, feats, args.lns_moves, 60.0, 15.0,
+                         say=lambda *a: None)
+        X, y, g = mlog.arrays()
+        sc = train_scorer(X, y, g, epochs=15)
+        run = evaluate(b, feats, sc, [1], args.lns_budget, 15.0,
+                       ["fixed", "learned"], say=lambda *a: None)[0]
+    return {"cell": "K_3(14,3)", "seed": 1, "start_M": run["start_M"],
+            "budget_s": args.lns_budget, "notch_s": 15.0,
+            "best_plain": run["fixed"]["best"],
+            "best_learned": run["learned"]["best"],
+            "target_M": run["target_M"], "t_plain_s": run["t_plain"],
+            "t_learned_s": run["t_learned"], "ratio": run["ratio"],
+            "rounds_plain": run["fixed"]["rounds"],
+            "rounds_learned": run["learned"]["rounds"],
+            "moves_logged": int(len(y)), "heldout_auc": sc.heldout_auc,
+            "wall_s": round(time.perf_counter() - t0, 1)}
+
+
 def run_b200(args, dist):
     cell = CELLS[args.cell]
     res = measure_cell(cell, args, dist)
@@ -444,6 +478,8 @@ def run_b200(args, dist):
         line["also"] = also
     if not args.no_batch:
         line["batched"] = measure_batch(args, dist)
+    if not args.no_lns and dist.world == 1:
+        line["lns"] = measure_lns(args)
     print(json.dumps(line), flush=True)
 
 
@@ -457,6 +493,9 @@ def main():
     ap.add_argument("--no-also", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-lns", action="store_true")
+    ap.add_argument("--lns-budget", type=float, default=30.0)
+    ap.add_argument("--lns-moves", type=int, default=30000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -90,17 +90,35 @@ def log_moves(b, feats, moves, budget, notch_s, kmin=8, kmax=None,
     return mlog
 
 
+class LossScorer:
+    """Ablation scorer: the negative z-scored exact loss.  The proposer
+    then draws like a ``low`` ruin through the same Gumbel top-k rule, so
+    the gap to the MLP scorer is what the model adds over the pick rule."""
+
+    heldout_auc = None
+
+    def __call__(self, X):
+        lo = np.asarray(X, dtype=np.float64)[:, 0]
+        return -(lo - lo.mean()) / (lo.std() + 1e-12)
+
+
 def evaluate(b, feats, scorer, seeds, budget, notch_s, selects, kmin=8,
              kmax=None, say=print, **learned_kw):
+    """``selects``: any of "fixed", "adaptive", "learned" and "loss-topk"
+    (the ablation: the learned proposer driven by :class:`LossScorer`)."""
     runs = []
     for seed in seeds:
         start = greedy_start(b, seed)
         row = {"seed": seed, "start_M": int(len(start))}
         for sel in selects:
-            prop = (LearnedRuin(scorer, feats, seed=seed, **learned_kw)
-                    if sel == "learned" else None)
+            prop = None
+            if sel in ("learned", "loss-topk"):
+                prop = LearnedRuin(scorer if sel == "learned" else
+                                   LossScorer(), feats, seed=seed,
+                                   **learned_kw)
             fsec0 = feats.seconds
-            trace, stats, ok = descent(b, start, seed, budget, sel,
+            trace, stats, ok = descent(b, start, seed, budget,
+                                       "learned" if prop else sel,
                                        proposer=prop, notch_s=notch_s,
                                        kmin=kmin, kmax=kmax)
             row[sel] = {"trace": trace, "ok": ok,

@@ -147,3 +147,34 @@ def test_gate_closes_on_low_auc(gpu):
         assert prop.stats["gated_flat"] == 1
     finally:
         b.close()
+
+
+def test_learned_proposal_beats_plain_lns_on_k3_14_3(gpu):
+    """The gain, measured: on K_3(14,3) (4.78M words, R = 3) from the same
+    greedy start, a descent whose ruins the trained model picks reaches a
+    smaller verified size within the same wall time than the plain descent
+    with the record mix.  Both are judged by the exact repair and full
+    recounts.  The model is trained here on moves logged from plain runs
+    on other seeds."""
+    from coldcore_b200.learned import LearnedRuin, RuinFeatures, train_scorer
+    from coldcore_b200.lns_study import descent, greedy_start, log_moves
+    b = gpu.GpuBackend([3] * 14, 3)
+    try:
+        feats = RuinFeatures(b)
+        mlog = log_moves(b, feats, 30000, 60.0, 15.0, say=lambda *a: None)
+        X, y, g = mlog.arrays()
+        assert len(y) >= 10000 and 0 < y.mean() < 0.5
+        sc = train_scorer(X, y, g, epochs=15)
+        assert sc.heldout_auc > 0.6
+        start = greedy_start(b, 7)
+        plain, _, ok_p = descent(b, start, 7, 25.0, "fixed", notch_s=15.0)
+        prop = LearnedRuin(sc, feats, seed=7)
+        learned, st, ok_l = descent(b, start, 7, 25.0, "learned",
+                                    proposer=prop, notch_s=15.0)
+        assert ok_p and ok_l
+        assert st["learned_rounds"] > 0
+        best_plain = min(m for _, m in plain)
+        best_learned = min(m for _, m in learned)
+        assert best_learned < best_plain, (plain, learned)
+    finally:
+        b.close()
