@@ -25,7 +25,10 @@ lns   : (1 GPU) LNS time-to-verified-size on K_3(14,3), learned ruin
 
 --impl reference runs that CPU restatement alone (rank 0), on the same
 cell, metric and unit: each step one transform of the cell, rotating
-recount / gain / loss.
+recount / gain / loss.  When the reference's own plugin has been built for
+sm_100a (oracle/build_ref.py) and a GPU is present, that arm also times it
+on the cells it accepts (H3_16_4, K_3(14,3), K_3(8,2)) under "gpu_plugin";
+the B200 arm reports the engine on the same cells under "same_cells".
 
 Multi-GPU (torchrun): every rank runs its own replica of the cell (the
 transform does not shard into independent pieces without an exchange
@@ -185,6 +188,53 @@ def cpu_sample(cell, modes, code):
     return by / t / 1e9, t
 
 
+def ref_plugin_gpu(args):
+    """The reference's own ABI-v1 plugin, compiled from its source for
+    sm_100a (oracle/build_ref.py), timed on this B200 over the cells it
+    accepts (axes <= 16, n <= 16, <= 65,535 occurrences): one step =
+    recount + gain map + loss map, CUDA events on the default stream the
+    plugin uses.  None when the library or the GPU is absent."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_covering.so")
+    if not os.path.exists(path):
+        return None
+    import torch
+    if not torch.cuda.is_available():
+        return None
+    from coldcore_b200.gpu import GpuBackend
+    out = {"library": "oracle/_ref/libref_covering.so (reference "
+                      "src/plugins/covering/dct_hc.cu, nvcc -O3 sm_100a)"}
+    for name in ("H3_16_4", "H3_14_3", "K3_8_2"):
+        cell = CELLS[name]
+        code = code_for(cell)
+        with GpuBackend(list(cell.axes), cell.R, problem=cell.problem,
+                        plugin_path=path) as b:
+            lib = b._lib
+            b._set_code(code)
+
+            def step():                   # the B200 arm's step, same calls
+                if lib.dct_transform(0, 2) or lib.dct_transform(1, 1) or \
+                        lib.dct_transform(2, 1):
+                    raise RuntimeError("reference transform failed")
+            for _ in range(args.warmup):
+                step()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            reps = max(3, args.steps // 2)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                step()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+        by = sum(model_bytes(list(cell.axes), cell.R, cell.problem, m)
+                 for m in ("recount", "gain", "loss"))
+        out[name] = {"ms_per_step": round(ms, 4),
+                     "value": round(by / (ms * 1e-3) / 1e9, 1),
+                     "unit": "GB/s"}
+    return out
+
+
 def run_reference(args, dist):
     if dist.rank != 0:
         return
@@ -225,6 +275,10 @@ def run_reference(args, dist):
         "e2e": {"value": round(val, 3), "unit": "GB/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        gp = ref_plugin_gpu(args)
+        if gp:
+            line["gpu_plugin"] = gp
     print(json.dumps(line), flush=True)
 
 
@@ -418,11 +472,17 @@ def run_b200(args, dist):
     cell = CELLS[args.cell]
     res = measure_cell(cell, args, dist)
     also = None
+    same = {}
     if not args.no_also and args.cell == HEADLINE:
         r2 = measure_cell(CELLS[ALSO], args, dist, timed=False)
         also = {"workload": ALSO, "value": round(r2["value"], 1),
                 "ms_per_step": round(r2["ms"], 4),
                 "e2e": r2["e2e"]["value"]}
+        # the smaller cells the reference's own plugin also accepts
+        for name in ("H3_14_3", "K3_8_2"):
+            r3 = measure_cell(CELLS[name], args, dist, timed=False)
+            same[name] = {"ms_per_step": round(r3["ms"], 4),
+                          "value": round(r3["value"], 1)}
     if dist.rank != 0:
         return
     peak, peak_kind = peaks()
@@ -476,6 +536,8 @@ def run_b200(args, dist):
     }
     if also:
         line["also"] = also
+    if same:
+        line["same_cells"] = same
     if not args.no_batch:
         line["batched"] = measure_batch(args, dist)
     if not args.no_lns and dist.world == 1:
@@ -494,6 +556,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-lns", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--lns-budget", type=float, default=30.0)
     ap.add_argument("--lns-moves", type=int, default=30000)
     args = ap.parse_args()

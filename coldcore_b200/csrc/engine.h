@@ -153,6 +153,15 @@ int launch_list_pred(const Geometry &g, const uint16_t *cnt, int mode,
 int launch_gather_set(const Geometry &g, const long long *dcand, int nc,
                       const unsigned long long *Z, long long zn, int32_t *out,
                       bool zeroed, cudaStream_t s);
+// device-side exact greedy (walks.cu): state in device memory, one step =
+// argmax of the gain map, placement of that word, incremental gain update
+struct GreedyState;
+constexpr int kGreedyStateBytes = 32;
+int launch_greedy_exclude(int32_t *map, const long long *dwords, int n,
+                          int32_t exclude, cudaStream_t s);
+int launch_greedy_step(const WalkArgs &w, int32_t *map, long long N,
+                       GreedyState *st, long long *placed, int max_add,
+                       long long *fresh, int32_t exclude, cudaStream_t s);
 // swap evaluation fast path: per drop its loss and the list of its ball
 // words at exactly mu (two walks and a segment scan), then per candidate
 // the listed words of its drop within distance R

@@ -103,6 +103,10 @@ struct State {
   char *h_swap = nullptr, *d_swap = nullptr;
   long long *d_list = nullptr;
   long long lcap = 0;
+  // device greedy: state, placed words, words satisfied per placement
+  char *d_greedy = nullptr;
+  long long *d_placed = nullptr, *h_placed = nullptr, *d_fresh = nullptr;
+  long long placed_cap = 0;
   Plan plans[3][4];                // [init_mode][out_mode]
   bool plan_ok[3][4] = {{false}};
   bool tuned[3][4] = {{false}};
@@ -260,6 +264,7 @@ void free_all() {
   F(S.d_words); F(S.d_out); F(S.d_scalar); F(S.d_hist); F(S.d_ext32);
   F(S.d_ext64); F(S.d_extv); F(S.zbuf); F(S.d_found);
   F(S.d_swap); F(S.d_list); FH(S.h_swap);
+  F(S.d_greedy); F(S.d_placed); F(S.d_fresh); FH(S.h_placed);
   FH(S.h_words); FH(S.h_out); FH(S.h_scalar);
   S.~State();
   new (&S) State();
@@ -1045,6 +1050,111 @@ int swap_eval_fast(const long long *drops, int k, const long long *cand,
   if (nc) memcpy(gain, h + r0, (size_t)nc * 4);
   S.stats[4]++;
   return 0;
+}
+
+// Exact greedy repair on the device (no counterpart in the reference; its
+// greedy_fill is the Python lazy greedy of search.py:260-360).  From the
+// gain map of the current cnt, with the active words excluded, each
+// step places the word of largest exact gain (ties: smallest index),
+// updates cnt over its ball and lowers the gain of every candidate whose
+// ball holds a word the placement satisfied, all without leaving the GPU;
+// it stops at zero deficit, at no positive gain, or after max_add words.
+// The placed words are added to the active multiset.  placed (capacity
+// max_add) receives them in placement order; *deficit the deficit left.
+// Returns the number placed, or a negative error.  The map is clobbered.
+int greedy_fill_impl(int max_add, long long *placed, long long *deficit) {
+  if (!S.live || max_add < 0 || (max_add && !placed) || !deficit) return -1;
+  if (S.g.space >= (1LL << 32)) return -1;    // 32-bit index in the key
+  // placed words are new (multiplicity 1): the counters stay within uint16
+  if (!within_counter(S.active_size + max_add, std::max(S.act_max, 1)))
+    return -1;
+  std::vector<long long> code;
+  code.reserve(S.active.size());
+  for (const auto &e : S.active) code.push_back(e.first);
+  const long long M = (long long)code.size();
+  if (!S.d_greedy) {
+    CC_CK(cudaMalloc(&S.d_greedy, kGreedyStateBytes));
+    CC_CK(cudaMalloc(&S.d_fresh, (size_t)S.len * 8));
+  }
+  if (max_add > S.placed_cap) {
+    if (S.d_placed) CC_CK(cudaFree(S.d_placed));
+    if (S.h_placed) CC_CK(cudaFreeHost(S.h_placed));
+    S.d_placed = S.h_placed = nullptr;
+    S.placed_cap = 0;
+    const long long cap = std::max<long long>(max_add, 1024);
+    CC_CK(cudaMalloc(&S.d_placed, (size_t)cap * 8));
+    CC_CK(cudaHostAlloc((void **)&S.h_placed, (size_t)cap * 8,
+                        cudaHostAllocDefault));
+    S.placed_cap = cap;
+  }
+  // the deficit to start from, and the gain map of the current cnt
+  CC_CK(cudaMemsetAsync(S.d_scalar, 0, 8, g_stream));
+  int rc = launch_cnt_reduce(S.cnt, S.g.space, kPredDef, 0, g_mu,
+                             S.d_scalar, g_stream);
+  if (rc) return rc;
+  long long d0;
+  rc = fetch_scalar(&d0);
+  if (rc) return rc;
+  *deficit = d0;
+  if (max_add == 0 || d0 == 0) return 0;
+  rc = autotune(1, 1);
+  if (rc) return rc;
+  rc = run_transform(1, 1);
+  if (rc) return rc;
+  S.layered_out = false;
+  constexpr int32_t kExcluded = INT_MIN / 2;
+  for (long long off = 0; off < M; off += kStageCap) {
+    const int nb = (int)std::min<long long>(kStageCap, M - off);
+    rc = stage_words(code.data() + off, nb);
+    if (rc) return rc;
+    rc = launch_greedy_exclude(S.layers, S.d_words, nb, kExcluded, g_stream);
+    if (rc) return rc;
+    CC_CK(cudaStreamSynchronize(g_stream));     // staging buffer reused
+  }
+  struct { unsigned long long best; long long deficit; int done, placed,
+           nnew, pad; } st0 = {0, d0, 0, 0, 0, 0};
+  static_assert(sizeof(st0) == kGreedyStateBytes, "state layout");
+  CC_CK(cudaMemcpyAsync(S.d_greedy, &st0, sizeof(st0),
+                        cudaMemcpyHostToDevice, g_stream));
+  const WalkArgs w = walk_args();
+  GreedyState *st = reinterpret_cast<GreedyState *>(S.d_greedy);
+  // every placement serves at least one deficient word: at most d0 steps.
+  // Steps go out in chunks (32, 64, ... 512) with one look at the state
+  // between chunks; steps after the stop are no-ops on the device.
+  const long long steps = std::min<long long>(max_add, d0);
+  long long issued = 0, chunk = 32;
+  while (issued < steps) {
+    const long long n = std::min(chunk, steps - issued);
+    for (long long i = 0; i < n; i++) {
+      rc = launch_greedy_step(w, S.layers, S.g.space, st, S.d_placed,
+                              max_add, S.d_fresh, kExcluded, g_stream);
+      if (rc) return rc;
+    }
+    issued += n;
+    CC_CK(cudaMemcpyAsync(S.h_scalar + 16, S.d_greedy, sizeof(st0),
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    memcpy(&st0, S.h_scalar + 16, sizeof(st0));
+    if (st0.done) break;
+    chunk = std::min<long long>(chunk * 2, 512);
+  }
+  const int n = st0.placed;
+  if (n) {
+    CC_CK(cudaMemcpyAsync(S.h_placed, S.d_placed, (size_t)n * 8,
+                          cudaMemcpyDeviceToHost, g_stream));
+    CC_CK(cudaStreamSynchronize(g_stream));
+    memcpy(placed, S.h_placed, (size_t)n * 8);
+    std::unordered_map<long long, int> batch;
+    for (int i = 0; i < n; i++) ++batch[placed[i]];
+    apply_active(batch, +1, n);
+  }
+  S.cnt_ver++;
+  *deficit = st0.deficit;
+  return n;
+}
+
+int dct_b200_greedy_fill(int max_add, long long *placed, long long *deficit) {
+  return greedy_fill_impl(max_add, placed, deficit);
 }
 
 int dct_swap_eval(const long long *drops, int k, const long long *cand,

@@ -260,6 +260,162 @@ int launch_drop_walks(const WalkArgs &w, const long long *ddrops, int k,
   return 0;
 }
 
+// ------------------------------------------------------------ device greedy
+// State of one device-side greedy fill (all fields in device memory).
+// best: the packed argmax key of the current step, (gain ^ sign) << 32 |
+// ~index, so the largest gain wins and ties go to the smallest index.
+struct GreedyState {
+  unsigned long long best;
+  long long deficit;          // sum max(0, mu - cnt), maintained exactly
+  int done;                   // 1: no positive gain or nothing uncovered
+  int placed;                 // words placed so far
+  int nnew;                   // words satisfied by the last placement
+  int pad;
+};
+static_assert(sizeof(GreedyState) == kGreedyStateBytes, "state layout");
+
+__device__ __forceinline__ unsigned long long greedy_key(int32_t v,
+                                                         long long x) {
+  return ((unsigned long long)((uint32_t)v ^ 0x80000000u) << 32) |
+         (uint32_t)~(uint32_t)x;
+}
+
+// map[x] = exclude for every listed word (incumbents never re-enter)
+__global__ void k_greedy_exclude(int32_t *map, const long long *words, int n,
+                                 int32_t exclude) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) map[words[i]] = exclude;
+}
+
+// step 1: best = argmax map (largest value, then smallest index)
+__global__ void __launch_bounds__(256)
+k_greedy_argmax(const int32_t *map, long long N, GreedyState *st) {
+  if (st->done) return;
+  unsigned long long k = 0;
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  const long long nv = N >> 2;
+  const int4 *v4 = reinterpret_cast<const int4 *>(map);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       i < nv; i += gs) {
+    const int4 q = __ldcg(v4 + i);
+    k = max(k, greedy_key(q.x, 4 * i));
+    k = max(k, greedy_key(q.y, 4 * i + 1));
+    k = max(k, greedy_key(q.z, 4 * i + 2));
+    k = max(k, greedy_key(q.w, 4 * i + 3));
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (N & 3))
+    k = max(k, greedy_key(map[nv * 4 + threadIdx.x], nv * 4 + threadIdx.x));
+  for (int o = 16; o > 0; o >>= 1)
+    k = max(k, __shfl_down_sync(0xffffffffu, k, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&st->best, k);
+}
+
+// step 2: place the argmax word (one block): cnt += 1 over its ball, the
+// words it satisfies (old count mu - 1) go to `fresh`, the deficit drops by
+// the words it serves (old count < mu)
+template <bool GRID>
+__global__ void __launch_bounds__(256)
+k_greedy_place(const WalkArgs a, int32_t *map, GreedyState *st,
+               long long *placed, int max_add, long long *fresh,
+               int32_t exclude) {
+  __shared__ WordSmem s;
+  __shared__ long long w_s;
+  __shared__ int stop;
+  __shared__ int nfresh;
+  __shared__ long long served;
+  if (threadIdx.x == 0) {
+    stop = st->done;
+    if (!stop) {
+      const unsigned long long k = st->best;
+      const int32_t v = (int32_t)((uint32_t)(k >> 32) ^ 0x80000000u);
+      const long long x = (long long)(uint32_t)~(uint32_t)k;
+      if (v <= 0 || st->deficit <= 0 || st->placed >= max_add) {
+        st->done = 1;
+        stop = 1;
+      } else {
+        w_s = x;
+        placed[st->placed] = x;
+        st->placed += 1;
+        map[x] = exclude;
+      }
+    }
+    st->best = 0;                     // fresh for the next step's argmax
+    st->nnew = 0;
+    nfresh = 0;
+    served = 0;
+  }
+  __syncthreads();
+  if (stop) return;
+  const long long w = w_s;
+  word_setup(a.g, w, s);
+  long long mine = 0;
+  for (long long t = threadIdx.x; t < a.len; t += blockDim.x) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x < 0) continue;
+    uint32_t *cell = reinterpret_cast<uint32_t *>(a.cnt + (x & ~1LL));
+    const int sh = (x & 1) ? 16 : 0;
+    const uint32_t old = atomicAdd(cell, 1u << sh);
+    const int c = (int)((old >> sh) & 0xFFFFu);
+    if (c < a.g.mu) mine++;
+    if (c == a.g.mu - 1) fresh[atomicAdd(&nfresh, 1)] = x;
+  }
+  mine = block_sum(mine);
+  if (threadIdx.x == 0) {
+    st->deficit -= mine;
+    st->nnew = nfresh;
+  }
+}
+
+// step 3: every word satisfied by the placement stops counting towards the
+// gain of the candidates whose balls hold it: map[y] -= 1 for y in B(u)
+template <bool GRID>
+__global__ void __launch_bounds__(256)
+k_greedy_refresh(const WalkArgs a, int32_t *map, const GreedyState *st,
+                 const long long *fresh) {
+  __shared__ WordSmem s;
+  if (st->done) return;
+  const int n = st->nnew;
+  for (int u = blockIdx.x; u < n; u += gridDim.x) {
+    const long long x0 = fresh[u];
+    __syncthreads();                      // s is reused across words
+    word_setup(a.g, x0, s);
+    for (long long t = threadIdx.x; t < a.len; t += blockDim.x) {
+      const long long y = walk_word<GRID>(a, x0, t, s);
+      if (y >= 0) atomicSub(&map[y], 1);
+    }
+  }
+}
+
+int launch_greedy_exclude(int32_t *map, const long long *dwords, int n,
+                          int32_t exclude, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_greedy_exclude<<<(n + 255) / 256, 256, 0, s>>>(map, dwords, n, exclude);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_greedy_step(const WalkArgs &w, int32_t *map, long long N,
+                       GreedyState *st, long long *placed, int max_add,
+                       long long *fresh, int32_t exclude, cudaStream_t s) {
+  long long blocks = ((N >> 2) + 255) / 256;
+  const long long cap = (long long)sm_count() * 4;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  k_greedy_argmax<<<(unsigned)blocks, 256, 0, s>>>(map, N, st);
+  const bool gp = w.g.prob == kGrid;
+  if (gp)
+    k_greedy_place<true><<<1, 256, 0, s>>>(w, map, st, placed, max_add, fresh,
+                                           exclude);
+  else
+    k_greedy_place<false><<<1, 256, 0, s>>>(w, map, st, placed, max_add,
+                                            fresh, exclude);
+  const unsigned rb = (unsigned)(sm_count() * 4);
+  if (gp) k_greedy_refresh<true><<<rb, 256, 0, s>>>(w, map, st, fresh);
+  else k_greedy_refresh<false><<<rb, 256, 0, s>>>(w, map, st, fresh);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
 // blocks per word so that single-word walks still fill the GPU
 int pick_split(long long len, int nb) {
   long long cover = (len + 255) / 256;

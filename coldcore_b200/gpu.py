@@ -90,6 +90,7 @@ def _bind(path):
         "dct_b200_set_timing": (I, [I]),
         "dct_b200_ball_hist": (I, [_LLP, I, I, I, _I32P]),
         "dct_b200_layers_at": (I, [_LLP, I, _I32P]),
+        "dct_b200_greedy_fill": (I, [I, _LLP, _LLP]),
         "dct_b200_last_timings": (I, [ctypes.POINTER(ctypes.c_float), I]),
     }
     for name, (res, args) in sig.items():
@@ -308,6 +309,18 @@ class GpuBackend:
             _check("layers_at", self._lib.dct_b200_layers_at(
                 _p(idx), len(idx), _p(out, ctypes.c_int32)))
         return out
+
+    def greedy_fill_device(self, max_add):
+        """Exact greedy repair on the GPU: places up to ``max_add`` words of
+        largest exact gain (ties: smallest index), non-active words only;
+        returns (placed words in order, deficit left)."""
+        placed = np.zeros(max(1, int(max_add)), dtype=np.int64)
+        deficit = _LL(0)
+        n = self._lib.dct_b200_greedy_fill(int(max_add), _p(placed),
+                                           ctypes.byref(deficit))
+        if n < 0:
+            _check("greedy_fill", n)
+        return placed[:n].copy(), int(deficit.value)
 
     def plan(self, init_mode, out_mode):
         """Launches of one transform: rows (first axis, axes, bytes, kernel)."""

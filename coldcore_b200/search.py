@@ -15,6 +15,11 @@ The random draws happen in the reference's order, so with a backend whose
 ``map_extract`` returns ascending indices (the CPU backends) a seeded run
 makes the same moves as the reference's.
 
+One repair rule is added: ``repair="device"`` runs the exact greedy on
+the GPU (``GpuBackend.greedy_fill_device``): the word of largest exact
+gain, ties to the smallest index, placed one after another without a host
+round trip.  The default stays the Python lazy greedy.
+
 One selection rule is added: ``select="learned"`` asks a *proposer* (see
 :mod:`coldcore_b200.learned`) for the k incumbents to remove.  When its
 confidence gate is closed the round falls back to the bandit.  Every round
@@ -110,7 +115,13 @@ class Searcher:
     repaired count), ``after`` and ``new_best``)."""
 
     def __init__(self, backend, seed=1, deadline=None, on_log=None,
-                 on_solved=None, proposer=None, move_log=None):
+                 on_solved=None, proposer=None, move_log=None,
+                 repair="exact"):
+        if repair not in ("exact", "device"):
+            raise ValueError(f"unknown repair mode: {repair!r}")
+        if repair == "device" and not hasattr(backend, "greedy_fill_device"):
+            raise ValueError("repair='device' needs a GPU backend")
+        self.repair = repair
         self.b = backend
         self.rng = _rng_for(seed)
         self.deadline = deadline
@@ -207,6 +218,8 @@ class Searcher:
         and the best is placed when it is at least the next stale bound and
         the extraction threshold (search.py:260-360)."""
         b = self.b
+        if self.repair == "device":
+            return self._device_fill(target_m)
         cap = min(b.extract_cap, 1 << 18)
         codeset = set(self.code.tolist())
         heap, thr, since = [], 1, refresh_every
@@ -254,6 +267,18 @@ class Searcher:
             if not placed and bg < thr:
                 since = refresh_every
         self.code = np.array(sorted(codeset), dtype=np.int64)
+        return self.uncov
+
+    def _device_fill(self, target_m):
+        """The exact greedy on the GPU, up to ``target_m`` points."""
+        need = int(target_m) - len(self.code)
+        if need > 0 and self.uncov > 0:
+            placed, deficit = self.b.greedy_fill_device(need)
+            if len(placed):
+                self.code = np.sort(np.concatenate([self.code, placed]))
+                self.stats["placements"] += len(placed)
+            self.stats["transforms"] += 1
+            self.uncov = deficit
         return self.uncov
 
     # ------------------------------------------------ ruin

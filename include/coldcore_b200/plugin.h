@@ -223,6 +223,16 @@ CCP_API int  dct_b200_ball_hist(const long long *words, int nw, int src,
                                 int nbins, int32_t *out);
 /* after dct_transform(init, 3): the R+1 layer values at each of k words */
 CCP_API int  dct_b200_layers_at(const long long *idx, int k, int32_t *out);
+/* Exact greedy repair on the device (no counterpart in the reference, whose
+ * repair is the Python lazy greedy of src/coldcore/search.py:260-360): from
+ * the current cnt, repeatedly place the non-active word of largest exact
+ * gain (ties: the smallest index) until nothing is deficient, no word has a
+ * positive gain, or max_add words are placed.  placed (capacity max_add)
+ * receives the words in placement order and joins the active multiset;
+ * *deficit receives the total deficit left.  Returns the number placed or a
+ * negative code.  The map (plane 0) is overwritten.  |X| < 2^32. */
+CCP_API int  dct_b200_greedy_fill(int max_add, long long *placed,
+                                  long long *deficit);
 CCP_API int  dct_b200_read_layer(int d, long long off, long long len, int32_t *out);
 
 #ifdef __cplusplus

@@ -1,0 +1,50 @@
+#!/usr/bin/env python3
+"""Build the reference's own covering plugin for sm_100a (test and
+comparison infrastructure only).
+
+The reference's ABI-v1 plugin is one CUDA translation unit,
+``src/plugins/covering/dct_hc.cu`` (with the ``dctcore_*.cuh`` headers
+beside it).  This recipe compiles it where it lies, with nvcc directly (not
+the reference's CMake build), into ``oracle/_ref/libref_covering.so``:
+
+    python oracle/build_ref.py            # ~3 minutes
+
+The library exports the same ``dct_*`` symbols as this engine, so the GPU
+tests can pin the engine's fields against the reference's own kernels on
+the same B200, and ``bench.py`` can time the reference's kernels on the
+cells they accept (axes <= 16, n <= 16, <= 65,535 occurrences).  Nothing
+here is linked into the engine; the reference source stays outside the
+repository, and the built library is git-ignored.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT_DIR = os.path.join(HERE, "_ref")
+OUT = os.path.join(OUT_DIR, "libref_covering.so")
+REF_SRC = os.environ.get("COLDCORE_REF_SRC", "/root/reference/src")
+
+
+def build(force=False):
+    src = os.path.join(REF_SRC, "plugins", "covering", "dct_hc.cu")
+    if not os.path.exists(src):
+        if os.path.exists(OUT):
+            return OUT                    # prebuilt (the GPU box has no source)
+        raise FileNotFoundError(src)
+    if os.path.exists(OUT) and not force and \
+            os.path.getmtime(OUT) >= os.path.getmtime(src):
+        return OUT
+    os.makedirs(OUT_DIR, exist_ok=True)
+    cmd = ["nvcc", "-O3", "-std=c++17",
+           "-gencode", "arch=compute_100a,code=sm_100a",
+           "-shared", "-Xcompiler", "-fPIC",
+           "-I", os.path.join(REF_SRC, "include"),
+           src, "-o", OUT + ".tmp"]
+    subprocess.run(cmd, check=True)
+    os.replace(OUT + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv))

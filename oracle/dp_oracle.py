@@ -344,6 +344,29 @@ class OracleBackend:
         return loss, gains
 
 
+def exact_greedy(oracle, code, max_add):
+    """The exact greedy the device repair runs, by brute force: from the
+    counts of ``code`` (already loaded into ``oracle``), repeatedly place
+    the word outside ``code`` and outside the words placed so far with the
+    largest gain (deficient words in its ball), ties to the smallest index;
+    stop at zero deficit, no positive gain, or ``max_add`` words.  Returns
+    (placed words in order, deficit left)."""
+    taken = set(np.asarray(code, dtype=np.int64).tolist())
+    placed = []
+    while len(placed) < max_add and oracle.uncovered() > 0:
+        oracle.gain_map()
+        g = oracle.map.astype(np.int64).copy()
+        if taken:
+            g[np.fromiter(taken, dtype=np.int64)] = np.iinfo(np.int64).min
+        w = int(np.argmax(g))
+        if g[w] <= 0:
+            break
+        oracle.ball_update(np.array([w]), +1)
+        placed.append(w)
+        taken.add(w)
+    return np.array(placed, dtype=np.int64), oracle.uncovered()
+
+
 def owner_losses(oracle, code):
     """Exact per-codeword deficit increase of removing that one copy — what
     the reference's owner-trick loss pass returns
