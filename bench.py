@@ -462,6 +462,7 @@ def measure_lns(args):
             "best_learned": run["learned"]["best"],
             "target_M": run["target_M"], "t_plain_s": run["t_plain"],
             "t_learned_s": run["t_learned"], "ratio": run["ratio"],
+            "ratio_bound": run["ratio_bound"],
             "rounds_plain": run["fixed"]["rounds"],
             "rounds_learned": run["learned"]["rounds"],
             "moves_logged": int(len(y)), "heldout_auc": sc.heldout_auc,
@@ -557,7 +558,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-lns", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--lns-budget", type=float, default=30.0)
+    ap.add_argument("--lns-budget", type=float, default=60.0)
     ap.add_argument("--lns-moves", type=int, default=30000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

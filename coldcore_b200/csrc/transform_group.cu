@@ -222,13 +222,17 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
   const int phi = g.pmode == kPredDef ? g.mu - 1 : g.pmode == kPredCrit
                   ? g.mu : g.ptarget;
   const unsigned pspan = (unsigned)(phi - plo);
+  // blk = ((ob * nh + mhi) * S + mlo) * W + w, kept as mixed-radix digits
+  // that advance by blockDim.x per trip (one compare per digit, no
+  // division in the loop); every digit sum stays below twice its radix
+  int w, mlo, mhi, ob, dw, dmlo, dmhi, dob;
+  {
+    int r = threadIdx.x;
+    w = r % W; r /= W; mlo = r % S; r /= S; mhi = r % nh; ob = r / nh;
+    r = blockDim.x;
+    dw = r % W; r /= W; dmlo = r % S; r /= S; dmhi = r % nh; dob = r / nh;
+  }
   for (int blk = threadIdx.x; blk < nblk; blk += blockDim.x) {
-    const int w = blk % W;
-    int rest = blk / W;
-    const int mlo = rest % S;
-    rest /= S;
-    const int mhi = rest % nh;
-    const int ob = rest / nh;
     const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
     const int pb = ob * g.mid + mlo + S * ne * mhi;      // tile word, e = 0
     const int sp0 = skewed(pb, g.skew) * W + w;
@@ -333,6 +337,17 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
         }
       }
     }
+    // advance the digits by blockDim.x
+    w += dw;
+    int c = w >= W;
+    if (c) w -= W;
+    mlo += dmlo + c;
+    c = mlo >= S;
+    if (c) mlo -= S;
+    mhi += dmhi + c;
+    c = mhi >= nh;
+    if (c) mhi -= nh;
+    ob += dob + c;
   }
 }
 

@@ -211,6 +211,22 @@ class Scorer:
                                 self.std)
 
 
+def heldout_rounds(y, groups, holdout, rng):
+    """Mask of the held-out moves: the same share of the rounds with a
+    positive move and of those without, whole rounds only, so a rare label
+    cannot leave the held-out slice one-sided."""
+    ug, inv = np.unique(groups, return_inverse=True)
+    pos_g = np.zeros(len(ug), dtype=bool)
+    np.logical_or.at(pos_g, inv, np.asarray(y) > 0.5)
+    picked = []
+    for part in (ug[pos_g], ug[~pos_g]):
+        if len(part) >= 2:
+            picked.append(rng.choice(part, size=max(1, int(len(part) *
+                                                           holdout)),
+                                     replace=False))
+    return np.isin(groups, np.concatenate(picked) if picked else [])
+
+
 def train_scorer(X, y, groups=None, epochs=30, batch=512, lr=2e-3, seed=0,
                  holdout=0.1):
     """Fit the MLP on logged moves.  The held-out slice is split by round
@@ -219,19 +235,17 @@ def train_scorer(X, y, groups=None, epochs=30, batch=512, lr=2e-3, seed=0,
     the held-out rounds (``within_auc``: the AUC within those rounds)."""
     X = np.asarray(X, dtype=np.float32)
     y = np.asarray(y, dtype=np.float32)
-    rng = np.random.default_rng(seed)
     groups = np.arange(len(y)) if groups is None else np.asarray(groups)
-    ug = np.unique(groups)
-    test_g = rng.choice(ug, size=max(1, int(len(ug) * holdout)),
-                        replace=False)
-    test = np.isin(groups, test_g)
+    test = heldout_rounds(y, groups, holdout, np.random.default_rng(seed))
     mean = X[~test].mean(axis=0)
     std = X[~test].std(axis=0) + 1e-3
     mlp = GpuMlp(seed=seed)
     mlp.train((X[~test] - mean) / std, y[~test], epochs=epochs, batch=batch,
               lr=lr, seed=seed)
     sc = Scorer(mlp, mean.astype(np.float32), std.astype(np.float32))
-    if test.any():
+    if not (y > 0.5).any():
+        sc.heldout_auc = 0.0           # nothing to learn from: gate closed
+    elif test.any():
         st = sc(X[test])
         sc.heldout_auc = auc(st, y[test])
         sc.within_auc = grouped_auc(st, y[test], groups[test])

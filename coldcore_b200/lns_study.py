@@ -42,13 +42,13 @@ def greedy_start(b, seed):
 
 
 def descent(b, start, seed, budget, select, proposer=None, move_log=None,
-            notch_s=10.0, kmin=8, kmax=None, step0=4):
+            notch_s=10.0, kmin=8, kmax=None, step0=4, repair="exact"):
     """One timed notch descent; returns ([(seconds, M), ...], stats, ok)
     with the verified sizes in the order they were reached."""
     t0 = time.time()
     trace = []
     s = Searcher(b, seed=seed, deadline=t0 + budget, proposer=proposer,
-                 move_log=move_log,
+                 move_log=move_log, repair=repair,
                  on_solved=lambda m, c: trace.append(
                      (round(time.time() - t0, 3), int(m))))
     s.build_reserve_s = s.loop_reserve_s = 0.0
@@ -69,7 +69,7 @@ def time_to(trace, size):
 
 
 def log_moves(b, feats, moves, budget, notch_s, kmin=8, kmax=None,
-              seed0=1000, say=print):
+              seed0=1000, say=print, repair="exact"):
     """Plain (fixed-mix) descents on seeds seed0, seed0 + 1, ... with the
     move log attached, until ``moves`` removals or ``budget`` seconds."""
     t0 = time.time()
@@ -79,7 +79,7 @@ def log_moves(b, feats, moves, budget, notch_s, kmin=8, kmax=None,
         start = greedy_start(b, seed)
         left = budget - (time.time() - t0)
         s = Searcher(b, seed=seed, deadline=time.time() + min(left, 120.0),
-                     move_log=mlog)
+                     move_log=mlog, repair=repair)
         s.build_reserve_s = s.loop_reserve_s = 0.0
         s.load(start)
         s.descend(notch_budget_s=notch_s, step0=4, reserve_s=0.0,
@@ -103,7 +103,7 @@ class LossScorer:
 
 
 def evaluate(b, feats, scorer, seeds, budget, notch_s, selects, kmin=8,
-             kmax=None, say=print, **learned_kw):
+             kmax=None, say=print, repair="exact", **learned_kw):
     """``selects``: any of "fixed", "adaptive", "learned" and "loss-topk"
     (the ablation: the learned proposer driven by :class:`LossScorer`)."""
     runs = []
@@ -120,7 +120,7 @@ def evaluate(b, feats, scorer, seeds, budget, notch_s, selects, kmin=8,
             trace, stats, ok = descent(b, start, seed, budget,
                                        "learned" if prop else sel,
                                        proposer=prop, notch_s=notch_s,
-                                       kmin=kmin, kmax=kmax)
+                                       kmin=kmin, kmax=kmax, repair=repair)
             row[sel] = {"trace": trace, "ok": ok,
                         "best": trace[-1][1] if trace else None,
                         "rounds": stats["rounds"],
@@ -133,25 +133,52 @@ def evaluate(b, feats, scorer, seeds, budget, notch_s, selects, kmin=8,
                 f"rounds {stats['rounds']} ok {ok}")
         plain = [s for s in ("fixed", "adaptive") if s in row]
         if plain and "learned" in row:
-            target = min(row[s]["best"] for s in plain)
-            tp = min(t for t in (time_to(row[s]["trace"], target)
-                                 for s in plain) if t is not None)
-            tl = time_to(row["learned"]["trace"], target)
-            row.update(target_M=target, t_plain=tp, t_learned=tl,
-                       ratio=(tl / tp) if (tl is not None and tp > 0)
-                       else None)
-            say(f"seed {seed}: target {target} plain {tp}s learned {tl}s")
+            row.update(time_to_size(row, plain, budget))
+            say(f"seed {seed}: target {row['target_M']} plain "
+                f"{row['t_plain']}s learned {row['t_learned']}s")
         runs.append(row)
     return runs
 
 
+def time_to_size(row, plain, budget):
+    """The target is the best size the plain arms reached, and at least one
+    word below the start.  ratio = learned time to it / plain time to it.
+    When no plain arm reached it within the budget, the plain time is
+    above the budget and ratio_bound = learned time / budget bounds the
+    ratio from above."""
+    target = min([row[s]["best"] for s in plain] + [row["start_M"] - 1])
+    tps = [t for t in (time_to(row[s]["trace"], target) for s in plain)
+           if t is not None]
+    tp = min(tps) if tps else None
+    tl = time_to(row["learned"]["trace"], target)
+    out = {"target_M": target, "t_plain": tp, "t_learned": tl,
+           "ratio": (tl / tp) if (tl is not None and tp) else None,
+           "ratio_bound": None}
+    if tp is None and tl is not None:
+        out["ratio_bound"] = tl / budget
+    return out
+
+
 def summarize(runs):
-    ratios = [r.get("ratio") for r in runs if "target_M" in r]
-    reached = [x for x in ratios if x is not None]
-    return {"reached": f"{len(reached)}/{len(ratios)}",
-            "median_ratio": float(np.median(reached)) if reached else None,
-            "geo_mean_ratio": (float(np.exp(np.mean(np.log(reached))))
-                               if reached else None)}
+    """Per-seed ratios; a seed where only the learned arm reached the
+    target counts with its upper bound, one where neither did is left out.
+    Also the best sizes of each arm."""
+    rows = [r for r in runs if "target_M" in r]
+    vals = []
+    for r in rows:
+        v = r["ratio"] if r["ratio"] is not None else r["ratio_bound"]
+        if v is not None:
+            vals.append(v)
+    out = {"seeds": len(rows), "learned_reached": f"{len(vals)}/{len(rows)}",
+           "median_ratio": float(np.median(vals)) if vals else None,
+           "geo_mean_ratio": (float(np.exp(np.mean(np.log(vals))))
+                              if vals else None),
+           "ratios": [round(v, 3) for v in vals]}
+    for arm in ("fixed", "adaptive", "learned", "loss-topk"):
+        bests = [r[arm]["best"] for r in runs if arm in r]
+        if bests:
+            out[f"best_{arm}"] = bests
+    return out
 
 
 def main(argv=None):
@@ -171,6 +198,9 @@ def main(argv=None):
     ap.add_argument("--selects", default="fixed,adaptive,learned")
     ap.add_argument("--temperature", type=float, default=0.5)
     ap.add_argument("--pick", default="topk", choices=("topk", "anchor"))
+    ap.add_argument("--repair", default="exact", choices=("exact", "device"),
+                    help="LNS repair of every arm: the Python lazy greedy "
+                         "(the reference's) or the device exact greedy")
     ap.add_argument("--out", default=None)
     ap.add_argument("--save-log", default=None)
     ap.add_argument("--load-log", default=None)
@@ -183,14 +213,15 @@ def main(argv=None):
     feats = RuinFeatures(b)
     report = {"cell": f"K_{a.q}({a.n},{a.R})", "budget_s": a.budget,
               "notch_s": a.notch, "kmin": a.kmin, "kmax": a.kmax,
-              "temperature": a.temperature, "pick": a.pick}
+              "temperature": a.temperature, "pick": a.pick,
+              "repair": a.repair}
     t0 = time.time()
     if a.load_log:
         z = np.load(a.load_log)
         X, y, g = z["X"], z["y"], z["g"]
     else:
         mlog = log_moves(b, feats, a.moves, a.log_budget, a.notch,
-                         kmin=a.kmin, kmax=a.kmax, say=say)
+                         kmin=a.kmin, kmax=a.kmax, say=say, repair=a.repair)
         X, y, g = mlog.arrays()
         if a.save_log:
             np.savez_compressed(a.save_log, X=X, y=y, g=g)
@@ -207,7 +238,8 @@ def main(argv=None):
     say("train", report["train"])
     runs = evaluate(b, feats, scorer, range(1, a.seeds + 1), a.budget,
                     a.notch, a.selects.split(","), kmin=a.kmin, kmax=a.kmax,
-                    say=say, temperature=a.temperature, pick=a.pick)
+                    say=say, repair=a.repair, temperature=a.temperature,
+                    pick=a.pick)
     report["runs"] = runs
     report["summary"] = summarize(runs)
     say("summary", report["summary"])

@@ -138,3 +138,35 @@ def test_move_log_labels_elements():
     assert y.tolist() == [1.0, 0.0, 1.0, 0.0, 0.0]
     assert g.tolist() == [0, 0, 0, 1, 1]
     assert mlog.mode == ["low"] * 3 + ["hole"] * 2
+
+
+def test_heldout_rounds_keep_both_labels():
+    from coldcore_b200.learned import heldout_rounds
+    g = np.repeat(np.arange(200), 5)
+    y = np.zeros(len(g), dtype=np.float32)
+    y[g == 17] = 1.0                          # two rare positive rounds
+    y[(g == 123) & (np.arange(len(g)) % 5 == 0)] = 1.0
+    for seed in range(20):
+        t = heldout_rounds(y, g, 0.1, np.random.default_rng(seed))
+        assert (y[t] > 0.5).any() and (y[t] < 0.5).any()
+        for r in np.unique(g[t]):             # whole rounds only
+            assert t[g == r].all()
+
+
+def test_time_to_size_target_and_bound():
+    from coldcore_b200.lns_study import summarize, time_to_size
+    row = {"start_M": 100,
+           "fixed": {"trace": [(0.0, 100)], "best": 100},
+           "adaptive": {"trace": [(0.0, 100), (40.0, 99)], "best": 99},
+           "learned": {"trace": [(0.0, 100), (5.0, 99), (9.0, 97)],
+                       "best": 97}}
+    r = time_to_size(row, ["fixed", "adaptive"], 60.0)
+    assert r["target_M"] == 99 and r["t_plain"] == 40.0
+    assert r["t_learned"] == 5.0 and abs(r["ratio"] - 0.125) < 1e-12
+    row["adaptive"] = {"trace": [(0.0, 100)], "best": 100}
+    r = time_to_size(row, ["fixed", "adaptive"], 60.0)
+    assert r["target_M"] == 99 and r["t_plain"] is None
+    assert r["ratio"] is None and abs(r["ratio_bound"] - 5.0 / 60) < 1e-12
+    row.update(r)
+    s = summarize([row])
+    assert s["learned_reached"] == "1/1" and s["best_learned"] == [97]
