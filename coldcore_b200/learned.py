@@ -257,10 +257,13 @@ class LearnedRuin:
     """The ``select="learned"`` proposer, with its confidence gate."""
 
     def __init__(self, scorer, features, auc_min=0.6, temperature=0.5,
-                 score_weight=1.0, decay=0.9, seed=0, pick="topk"):
+                 score_weight=1.0, decay=0.9, seed=0, pick="topk",
+                 scale="raw"):
         if pick not in ("topk", "anchor"):
             raise ValueError(f"unknown pick rule {pick!r}")
-        self.pick = pick
+        if scale not in ("raw", "std"):
+            raise ValueError(f"unknown score scale {scale!r}")
+        self.pick, self.scale = pick, scale
         self.scorer, self.features = scorer, features
         self.auc_min = float(auc_min)
         self.temperature = float(temperature)
@@ -293,9 +296,11 @@ class LearnedRuin:
             return None
         self.stats["proposed"] += 1
         if self.pick == "topk":
-            # Gumbel top-k: k draws without replacement, P ~ exp(z / T)
+            # Gumbel top-k: k draws without replacement, P ~ exp(z / T);
+            # scale="std" measures T in units of this round's score spread
+            zt = z if self.scale == "raw" else (z - z.mean()) / z.std()
             gumbel = -np.log(-np.log(self.rng.random(len(z)) + 1e-300))
-            return np.argsort(-(z / self.temperature + gumbel))[:k]
+            return np.argsort(-(zt / self.temperature + gumbel))[:k]
         p = np.exp((z - z.max()) / self.temperature)
         p /= p.sum()
         anchor = int(self.rng.choice(len(z), p=p))

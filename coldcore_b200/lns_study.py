@@ -198,6 +198,7 @@ def main(argv=None):
     ap.add_argument("--selects", default="fixed,adaptive,learned")
     ap.add_argument("--temperature", type=float, default=0.5)
     ap.add_argument("--pick", default="topk", choices=("topk", "anchor"))
+    ap.add_argument("--scale", default="raw", choices=("raw", "std"))
     ap.add_argument("--repair", default="exact", choices=("exact", "device"),
                     help="LNS repair of every arm: the Python lazy greedy "
                          "(the reference's) or the device exact greedy")
@@ -214,6 +215,7 @@ def main(argv=None):
     report = {"cell": f"K_{a.q}({a.n},{a.R})", "budget_s": a.budget,
               "notch_s": a.notch, "kmin": a.kmin, "kmax": a.kmax,
               "temperature": a.temperature, "pick": a.pick,
+              "scale": a.scale,
               "repair": a.repair}
     t0 = time.time()
     if a.load_log:
@@ -239,7 +241,7 @@ def main(argv=None):
     runs = evaluate(b, feats, scorer, range(1, a.seeds + 1), a.budget,
                     a.notch, a.selects.split(","), kmin=a.kmin, kmax=a.kmax,
                     say=say, repair=a.repair, temperature=a.temperature,
-                    pick=a.pick)
+                    pick=a.pick, scale=a.scale)
     report["runs"] = runs
     report["summary"] = summarize(runs)
     say("summary", report["summary"])
