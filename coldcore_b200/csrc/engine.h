@@ -95,6 +95,12 @@ int launch_group(const GroupPlan &p, cudaStream_t s);
 int prepare_group(const GroupPlan &p);
 size_t group_smem_bytes(const GroupArgs &a, int R1);
 int pick_group_kernel(int prob, int q, int R1, int *bm);
+int group_kernel_variants(int prob, int q, int R1, int *kids, int *bms,
+                          int cap);
+// the same group with every other register-blocked kernel and CTA width
+// (rounds, skew and grid recomputed; tiles unchanged), the plan itself first
+std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
+                                      size_t smem_cap);
 int launch_code_bounds(const long long *code, long long ncode,
                        long long tile_words, long long ntiles,
                        long long *bounds, cudaStream_t s);

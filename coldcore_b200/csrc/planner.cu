@@ -185,5 +185,37 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
   return out;
 }
 
+std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
+                                      size_t smem_cap) {
+  std::vector<GroupPlan> out{p};
+  if (p.kernel < 0 || p.a.nrounds <= 0) return out;
+  const int q = p.a.rq[0];
+  int kids[8], bms[8];
+  const int nk = group_kernel_variants(p.a.prob, q, R1, kids, bms, 8);
+  for (int i = 0; i < nk; i++) {
+    GroupPlan t = p;
+    t.kernel = kids[i];
+    if (t.a.W == 1 && (q & (q - 1)) == 0) {
+      int lg = 0;
+      while ((1 << lg) < ipow(q, bms[i])) lg++;
+      t.a.skew = lg;
+    }
+    set_rounds(t.a, q, bms[i]);
+    t.smem = group_smem_bytes(t.a, R1);
+    if (t.smem > smem_cap) continue;
+    const int full = threads_for(t.a, t.kernel, bms[i], q);
+    std::vector<int> widths{full};
+    if (full > 256) widths.push_back(256);
+    if (full > 128) widths.push_back(128);
+    for (int th : widths) {
+      GroupPlan v = t;
+      v.threads = th;
+      v.grid = occupancy_grid(v);
+      if (v.kernel == p.kernel && v.threads == p.threads) continue;
+      out.push_back(v);
+    }
+  }
+  return out;
+}
 
 }  // namespace cc

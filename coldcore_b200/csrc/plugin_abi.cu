@@ -467,9 +467,48 @@ int autotune(int init_mode, int out_mode) {
     CC_CK(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) { best = ms; keep = S.plans[init_mode][out_mode]; }
   }
+  // second stage, with the grouping fixed: per launch, every register
+  // block size and CTA width, each timed alone (three launches after a
+  // warm one).  A launch run again works in place on its own planes, which
+  // only scrambles values; the real transform runs from scratch after this.
+  S.plans[init_mode][out_mode] = keep;
+  // one transform with the kept plan: its code bounds (a recount's first
+  // group) and planes are then the ones every variant below reads; the
+  // variants keep the tiles, so the bounds stay valid for all of them
+  int rc0 = run_transform(init_mode, out_mode);
+  if (rc0) return rc0;
+  int pm, pt;
+  set_predicate(init_mode, &pm, &pt);
+  for (size_t gi = 0; gi < keep.groups.size() && !keep.window; gi++) {
+    std::vector<GroupPlan> vars = group_variants(keep.groups[gi], S.R1,
+                                                 220 << 10);
+    if (vars.size() < 2) continue;
+    float bv = 1e30f;
+    size_t bi = 0;
+    for (size_t vi = 0; vi < vars.size(); vi++) {
+      GroupPlan p = vars[vi];
+      p.a.pmode = pm;
+      p.a.ptarget = pt;
+      p.a.mu = g_mu;
+      p.a.code = S.d_code;
+      p.a.ncode = S.codeM;
+      p.a.code_bounds = S.d_bounds;
+      int rc = prepare_group(p);
+      if (rc) return rc;
+      if ((rc = launch_group(p, g_stream))) return rc;
+      CC_CK(cudaEventRecord(e0, g_stream));
+      for (int r = 0; r < 3; r++)
+        if ((rc = launch_group(p, g_stream))) return rc;
+      CC_CK(cudaEventRecord(e1, g_stream));
+      CC_CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CC_CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < bv) { bv = ms; bi = vi; }
+    }
+    S.plans[init_mode][out_mode].groups[gi] = vars[bi];
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  S.plans[init_mode][out_mode] = keep;
   S.tune_ms[init_mode][out_mode] = best / 2;
   return 0;
 }

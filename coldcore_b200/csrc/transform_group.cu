@@ -793,6 +793,21 @@ static int op_of(int prob) {
          : prob == kTorus ? kOpTorus : kOpGrid;
 }
 
+// Every register-blocked kernel for (problem, q, R1): ids and block axes,
+// in table order; returns how many (at most cap).
+int group_kernel_variants(int prob, int q, int R1, int *kids, int *bms,
+                          int cap) {
+  const int op = op_of(prob);
+  int n = 0;
+  for (int i = 0; i < kTableLen && n < cap; i++)
+    if (kTable[i].op == op && kTable[i].q == q && kTable[i].r1 == R1) {
+      kids[n] = i;
+      bms[n] = kTable[i].bm;
+      n++;
+    }
+  return n;
+}
+
 // Kernel id for a group whose axes all have size q; -1 = generic kernel.
 int pick_group_kernel(int prob, int q, int R1, int *bm) {
   const int op = op_of(prob);
