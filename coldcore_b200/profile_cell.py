@@ -28,10 +28,10 @@ def main():
         b.set_timing(args.timing)
         for m in modes:
             i, o = MODES[m]
-            plan = b.plan(i, o)
             for _ in range(args.reps):
                 if b._lib.dct_transform(i, o):
                     raise RuntimeError("transform failed")
+            plan = b.plan(i, o)              # after the autotuner ran
             print(f"{cell.name} {m}: plan (axis0, axes, bytes, kernel) = "
                   f"{plan.tolist()}")
             if args.timing:
