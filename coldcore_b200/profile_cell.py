@@ -20,6 +20,11 @@ def main():
     ap.add_argument("--mode", default="gain", choices=sorted(MODES) + ["all"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--timing", action="store_true")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="after the timed reps (and the autotuner), run one "
+                         "more transform per mode inside an NVTX range "
+                         "named 'capture' (ncu --nvtx --nvtx-include "
+                         "capture/ then sees the tuned launches only)")
     args = ap.parse_args()
     cell = CELLS[args.cell]
     modes = list(MODES) if args.mode == "all" else [args.mode]
@@ -34,6 +39,13 @@ def main():
             plan = b.plan(i, o)              # after the autotuner ran
             print(f"{cell.name} {m}: plan (axis0, axes, bytes, kernel) = "
                   f"{plan.tolist()}")
+            if args.nvtx:
+                import torch
+                torch.cuda.nvtx.range_push("capture")
+                if b._lib.dct_transform(i, o):
+                    raise RuntimeError("transform failed")
+                torch.cuda.synchronize()
+                torch.cuda.nvtx.range_pop()
             if args.timing:
                 for k, t in enumerate(b.last_timings()):
                     by = int(plan[k][2])
