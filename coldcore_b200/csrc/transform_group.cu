@@ -351,6 +351,29 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
   }
 }
 
+// A round of rb axes runs with a register block of exactly Q^rb words: the
+// kernel's own block size BM for full rounds, a compile-time smaller block
+// for the group's last, partial round (no runtime bounds in the loops).
+template <int OP, int Q, int R1, int B>
+struct RoundSel {
+  static __device__ __forceinline__ void run(
+      const GroupArgs &g, int32_t *sm, int SD, long long o0, long long i0,
+      int rb, int S, int src, int dst, int nl, const uint16_t *cs) {
+    if (rb == B)
+      run_round<OP, Q, R1, B, true>(g, sm, SD, o0, i0, B, S, src, dst, nl,
+                                    cs);
+    else
+      RoundSel<OP, Q, R1, B - 1>::run(g, sm, SD, o0, i0, rb, S, src, dst, nl,
+                                      cs);
+  }
+};
+template <int OP, int Q, int R1>
+struct RoundSel<OP, Q, R1, 0> {
+  static __device__ __forceinline__ void run(
+      const GroupArgs &, int32_t *, int, long long, long long, int, int, int,
+      int, int, const uint16_t *) {}
+};
+
 template <int OP, int Q, int R1, int BM>
 __global__ void __launch_bounds__(kGroupThreads)
 group_kernel(const GroupArgs g) {
@@ -374,12 +397,8 @@ group_kernel(const GroupArgs g) {
     for (int r = 0; r < g.nrounds; r++) {
       const int src = r == 0 ? first_src : kIoSmem;
       const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
-      if (g.rb[r] == BM)
-        run_round<OP, Q, R1, BM, true>(g, sm, SD, o0, i0, BM, g.rs[r], src,
-                                       dst);
-      else
-        run_round<OP, Q, R1, BM, false>(g, sm, SD, o0, i0, g.rb[r], g.rs[r],
-                                        src, dst);
+      RoundSel<OP, Q, R1, BM>::run(g, sm, SD, o0, i0, g.rb[r], g.rs[r], src,
+                                   dst, R1, nullptr);
       __syncthreads();
     }
   }
@@ -505,12 +524,8 @@ group_kernel_pipe(const GroupArgs g) {
       const int src = r > 0 ? kIoSmem : from_cnt ? kIoCntSmem : kIoSmem;
       const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
       const int nl = r > 0 ? R1 : g.lin;
-      if (g.rb[r] == BM)
-        run_round<OP, Q, R1, BM, true>(g, buf, SD, o0, i0, BM, g.rs[r], src,
-                                       dst, nl, cs);
-      else
-        run_round<OP, Q, R1, BM, false>(g, buf, SD, o0, i0, g.rb[r],
-                                        g.rs[r], src, dst, nl, cs);
+      RoundSel<OP, Q, R1, BM>::run(g, buf, SD, o0, i0, g.rb[r], g.rs[r], src,
+                                   dst, nl, cs);
       __syncthreads();
     }
   }
