@@ -192,9 +192,13 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   const int q = p.a.rq[0];
   int kids[8], bms[8];
   const int nk = group_kernel_variants(p.a.prob, q, R1, kids, bms, 8);
-  for (int i = 0; i < nk; i++) {
+  // the cp.async-prefetching form too, where its second buffer fits
+  const bool can_pipe = p.a.src != kSrcCode;
+  for (int i = 0; i < nk; i++)
+  for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {
     GroupPlan t = p;
     t.kernel = kids[i];
+    t.a.pipe = pipe;
     if (t.a.W == 1 && (q & (q - 1)) == 0) {
       int lg = 0;
       while ((1 << lg) < ipow(q, bms[i])) lg++;
@@ -211,7 +215,9 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
       GroupPlan v = t;
       v.threads = th;
       v.grid = occupancy_grid(v);
-      if (v.kernel == p.kernel && v.threads == p.threads) continue;
+      if (v.kernel == p.kernel && v.threads == p.threads &&
+          v.a.pipe == p.a.pipe)
+        continue;
       out.push_back(v);
     }
   }

@@ -445,7 +445,8 @@ int autotune(int init_mode, int out_mode) {
   static const Knobs cands[] = {{100 << 10, 1}, {160 << 10, 1},
                                 {64 << 10, 1}, {200 << 10, 1},
                                 {100 << 10, 2}, {100 << 10, 3},
-                                {200 << 10, 3}};
+                                {200 << 10, 3}, {160 << 10, 2},
+                                {200 << 10, 2}};
   cudaEvent_t e0, e1;
   CC_CK(cudaEventCreate(&e0));
   CC_CK(cudaEventCreate(&e1));
