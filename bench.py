@@ -48,6 +48,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from coldcore_b200.metrics import model_bytes          # noqa: E402
+from coldcore_b200.replicas import ReplicaGroup         # noqa: E402
 from coldcore_b200.workloads import CELLS, code_for     # noqa: E402
 
 METRIC = ("transform GB/s vs HBM peak; LNS time-to-verified-size learned "
@@ -81,37 +82,8 @@ def ncu_traffic(kernel_key):
 
 
 # ---------------------------------------------------------------- dist
-class Dist:
-    def __init__(self):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        if self.world > 1:
-            import datetime
-
-            import torch
-            import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(
-                seconds=120))
-            self.pg = dist
-
-    def barrier(self):
-        if self.pg:
-            self.pg.barrier()
-
-    def max(self, v):
-        if not self.pg:
-            return v
-        import torch
-        t = torch.tensor([float(v)], device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
+class Dist(ReplicaGroup):
+    """The bench's replica group (``coldcore_b200.replicas``)."""
 
 
 # ---------------------------------------------------------------- clocks
