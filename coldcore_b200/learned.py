@@ -92,8 +92,14 @@ class RuinFeatures:
         f = np.zeros((m, N_FEATURES), dtype=np.float32)
         if m == 0:
             return f
-        b.loss_map()
-        loss = np.asarray(b.map_read_at(code), dtype=np.float64)
+        if self.layered:
+            # the critical words by distance; their sum is the loss map
+            b.layers_map(2)
+            crit = b.layers_at(code)
+            loss = crit.sum(axis=1).astype(np.float64)
+        else:
+            b.loss_map()
+            loss = np.asarray(b.map_read_at(code), dtype=np.float64)
         f[:, 0] = loss / B
         f[:, 1] = _rank(loss)
         b.gain_map()
@@ -103,8 +109,7 @@ class RuinFeatures:
         if self.layered:
             nd = min(R + 1, _MAX_D)
             sph = self.sphere[:nd][None, :]
-            b.layers_map(2)                    # critical words by distance
-            f[:, 18:18 + nd] = b.layers_at(code)[:, :nd] / sph
+            f[:, 18:18 + nd] = crit[:, :nd] / sph
             b.stage_code(code)
             b.layers_map(0)                    # the code by distance
             f[:, 24:24 + nd] = b.layers_at(code)[:, :nd] / sph
