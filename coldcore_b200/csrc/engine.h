@@ -68,6 +68,10 @@ struct GroupArgs {
   int prob;
   int pipe;               // prefetch the next tile while computing (cp.async)
   int32_t *map;           // kDstMap target (nullptr: plane 0 of layers)
+  // 16-bit intermediate planes: plane d at layers16 + d*plane (u16 words),
+  // read when in16, written when out16 (values provably <= 65535)
+  uint16_t *layers16;
+  int in16, out16;
   long long *red;         // epilogue reduction target (generic tiles)
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
 };
@@ -81,10 +85,12 @@ struct GroupPlan {
 };
 
 // planner.cu: schedule knobs and the group plan of one transform
-struct Knobs { size_t budget; int pipe; };   // pipe: see plan_groups
+// pipe: see plan_groups; half: 16-bit planes between the launches
+struct Knobs { size_t budget; int pipe; int half = 0; };
 struct PlanPtrs {
   int32_t *layers; long long plane; uint16_t *cnt;
   const long long *code; long long ncode; int32_t *map;
+  uint16_t *layers16 = nullptr;   // u16 plane region (Knobs::half)
 };
 std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
                                    const PlanPtrs &ptr, int src, int dst,

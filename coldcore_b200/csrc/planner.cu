@@ -101,6 +101,8 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     base.code = ptr.code;
     base.ncode = ptr.ncode;
     base.map = ptr.map;
+    base.layers16 = ptr.layers16;
+    base.in16 = kn.half && j > 0;          // every later group reads u16
     base.inner = g.pw[j];
     base.prob = g.prob;
     base.R = g.R;
@@ -109,7 +111,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     // pipe 1 and 3 prefetch the cnt-reading first group; 3 also the last
     // group when it writes the 4-byte map (reads every layer, writes one
     // plane), decided below; 2 prefetches every group
-    base.pipe = kid >= 0 && base.src != kSrcCode &&
+    base.pipe = kid >= 0 && base.src != kSrcCode && !base.in16 &&
                 (kn.pipe == 2 || ((kn.pipe == 1 || kn.pipe == 3) &&
                                   base.src == kSrcCnt));
     // the most axes that fit one tile of W inner words
@@ -161,8 +163,9 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     else a.nrounds = 0;
     const bool last = j + a.k == g.n;
     a.dst = last ? dst : kDstLayers;
+    a.out16 = kn.half && !last;
     if (kn.pipe == 3 && kid >= 0 && last && dst != kDstLayers &&
-        a.src == kSrcLayers) {
+        a.src == kSrcLayers && !a.in16) {
       // read-heavy last group: prefetch its tiles too (if they still fit)
       GroupArgs t = a;
       t.pipe = 1;
@@ -193,7 +196,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   int kids[8], bms[8];
   const int nk = group_kernel_variants(p.a.prob, q, R1, kids, bms, 8);
   // the cp.async-prefetching form too, where its second buffer fits
-  const bool can_pipe = p.a.src != kSrcCode;
+  const bool can_pipe = p.a.src != kSrcCode && !p.a.in16;
   for (int i = 0; i < nk; i++)
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {
     GroupPlan t = p;

@@ -288,9 +288,25 @@ Knobs default_knobs() {
   return {smem_budget(), pe ? atoi(pe) : 1};
 }
 
+// 16-bit planes between the launches of one transform are exact when no
+// intermediate layer value can pass 65535: a layer counts words within a
+// distance, so it is at most the occurrences (<= 65535 by the rule that
+// set_code enforces) for a code, and at most |B| for a predicate.  They sit
+// from int32 plane 1 on, clear of the int32 map in plane 0; a transform
+// that outputs every layer keeps int32 planes throughout.  CC_HALF=0 turns
+// them off.
+bool half_planes_ok(int src, int dst) {
+  const char *e = getenv("CC_HALF");
+  if (e && atoi(e) == 0) return false;
+  if (S.R1 < 2 || dst == kDstLayers) return false;
+  return src == kSrcCode || S.len <= 65535;
+}
+
 Plan build_group_plan(int src, int dst, Knobs kn) {
   Plan P;
   PlanPtrs ptr{S.layers, S.plane, S.cnt, S.d_code, S.codeM, nullptr};
+  kn.half = half_planes_ok(src, dst) ? 1 : 0;
+  ptr.layers16 = reinterpret_cast<uint16_t *>(S.layers + S.plane);
   Geometry g = S.g;
   g.mu = g_mu;
   P.groups = plan_groups(g, S.R1, ptr, src, dst, kn);
@@ -1398,8 +1414,8 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
   for (const auto &p : P.groups) {
     long long rd = 0, wr = 0;
     if (p.a.src == kSrcCnt) rd = 2;
-    else if (p.a.src == kSrcLayers) rd = 4LL * p.a.lin;
-    if (p.a.dst == kDstLayers) wr = 4LL * p.a.lout;
+    else if (p.a.src == kSrcLayers) rd = (p.a.in16 ? 2LL : 4LL) * p.a.lin;
+    if (p.a.dst == kDstLayers) wr = (p.a.out16 ? 2LL : 4LL) * p.a.lout;
     else if (p.a.dst == kDstMap) wr = 4;
     else wr = 2;
     long long by = X * (rd + wr);

@@ -264,7 +264,19 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
         }
       }
     } else if (valid) {
-      if (src == kIoLayers) {
+      if (src == kIoLayers && g.in16) {
+#pragma unroll
+        for (int d = 0; d < R1; d++) {
+          if (d >= g.lin) break;
+          const uint16_t *p = g.layers16 + d * g.plane + xb;
+#pragma unroll
+          for (int e = 0; e < QB; e++) {
+            if (!FULL && e >= ne) break;
+            v[d][e] = __ldcs(p);
+            p += gstep;
+          }
+        }
+      } else if (src == kIoLayers) {
 #pragma unroll
         for (int d = 0; d < R1; d++) {
           if (d >= g.lin) break;
@@ -301,7 +313,19 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
         }
       }
     } else if (valid) {
-      if (dst == kIoLayers) {
+      if (dst == kIoLayers && g.out16) {
+#pragma unroll
+        for (int d = 0; d < R1; d++) {
+          if (d >= g.lout) break;
+          uint16_t *p = g.layers16 + d * g.plane + xb;
+#pragma unroll
+          for (int e = 0; e < QB; e++) {
+            if (!FULL && e >= ne) break;
+            __stcs(p, (uint16_t)v[d][e]);
+            p += gstep;
+          }
+        }
+      } else if (dst == kIoLayers) {
 #pragma unroll
         for (int d = 0; d < R1; d++) {
           if (d >= g.lout) break;
@@ -576,7 +600,9 @@ __device__ void generic_tile(const GroupArgs &g, long long tile,
     for (int d = 0; d < R1; d++) {
       int32_t val = 0;
       if (g.src == kSrcLayers) {
-        if (valid && d < g.lin) val = ld_i32<CG>(g.layers + d * g.plane + x);
+        if (valid && d < g.lin)
+          val = g.in16 ? ld_u16<CG>(g.layers16 + d * g.plane + x)
+                       : ld_i32<CG>(g.layers + d * g.plane + x);
       } else if (g.src == kSrcCnt) {
         if (valid && d == 0)
           val = cnt_pred(g.pmode, ld_u16<CG>(g.cnt + x), g.ptarget, g.mu);
@@ -653,8 +679,10 @@ __device__ void generic_tile(const GroupArgs &g, long long tile,
     const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
     const int sp = skewed(p, g.skew) * W + w;
     if (g.dst == kDstLayers) {
-      for (int d = 0; d < g.lout; d++)
-        g.layers[d * g.plane + x] = sm[d * SD + sp];
+      for (int d = 0; d < g.lout; d++) {
+        if (g.out16) g.layers16[d * g.plane + x] = (uint16_t)sm[d * SD + sp];
+        else g.layers[d * g.plane + x] = sm[d * SD + sp];
+      }
     } else {
       int32_t s = 0;
       for (int d = 0; d < R1; d++) s += sm[d * SD + sp];
