@@ -78,7 +78,12 @@ struct State {
   int32_t *d_extv = nullptr;
   long long extract_cap = 0;
   // multisets (coldcore dct_hc.cu:46-56) + max multiplicity of `active`
-  std::unordered_map<long long, int> uploaded, active;
+  // uploaded: the staged code, sorted; active: the represented multiset.
+  // A recount makes active = uploaded; the hash map is then built lazily,
+  // on the first call that needs per-word counts (ensure_active).
+  std::vector<long long> up_sorted;
+  std::unordered_map<long long, int> active;
+  bool active_pending = false;
   long long active_size = 0;
   int up_max = 0;
   std::vector<int> mult_hist;      // distinct active words per multiplicity
@@ -183,6 +188,7 @@ void hist_move(int from, int to) {
 }
 
 void set_active(const std::unordered_map<long long, int> &m, long long sz) {
+  S.active_pending = false;
   S.active = m;
   S.active_size = sz;
   std::fill(S.mult_hist.begin(), S.mult_hist.end(), 0);
@@ -193,8 +199,30 @@ void set_active(const std::unordered_map<long long, int> &m, long long sz) {
   }
 }
 
+// the multiset of the last recount, as a hash map with its histogram
+void ensure_active() {
+  if (!S.active_pending) return;
+  S.active_pending = false;
+  S.active.clear();
+  S.active.reserve(S.up_sorted.size() * 2 + 1);
+  std::fill(S.mult_hist.begin(), S.mult_hist.end(), 0);
+  S.act_max = 0;
+  const auto &v = S.up_sorted;
+  for (size_t i = 0; i < v.size();) {
+    size_t j = i + 1;
+    while (j < v.size() && v[j] == v[i]) j++;
+    const int c = (int)(j - i);
+    S.active.emplace(v[i], c);
+    S.mult_hist[c]++;
+    if (c > S.act_max) S.act_max = c;
+    i = j;
+  }
+  S.active_size = (long long)v.size();
+}
+
 void apply_active(const std::unordered_map<long long, int> &batch,
                   int delta, long long nw) {
+  ensure_active();
   for (const auto &e : batch) {
     int &c = S.active[e.first];
     const int before = c;
@@ -208,6 +236,7 @@ void apply_active(const std::unordered_map<long long, int> &batch,
 // validate an update batch against `active`; fills `batch`
 int check_update(const long long *words, int nw, int delta,
                  std::unordered_map<long long, int> &batch) {
+  ensure_active();
   if (!valid_words(words, nw) || (delta != 1 && delta != -1)) return -1;
   batch.reserve((size_t)nw * 2 + 1);
   for (int i = 0; i < nw; i++) ++batch[words[i]];
@@ -948,13 +977,17 @@ int dct_use_fmt(int fmt) {
 
 int dct_set_code(const long long *idx, int M) {
   if (!S.live || !valid_words(idx, M)) return -1;
-  std::unordered_map<long long, int> up;
-  up.reserve((size_t)M * 2 + 1);
-  int mx = 0;
-  for (int i = 0; i < M; i++) mx = std::max(mx, ++up[idx[i]]);
-  if (!within_counter(M, mx)) return -1;
   std::vector<long long> sorted(idx, idx + M);
-  std::sort(sorted.begin(), sorted.end());
+  if (!std::is_sorted(sorted.begin(), sorted.end()))
+    std::sort(sorted.begin(), sorted.end());
+  int mx = 0;                                  // largest multiplicity
+  for (int i = 0; i < M;) {
+    int j = i + 1;
+    while (j < M && sorted[j] == sorted[i]) j++;
+    mx = std::max(mx, j - i);
+    i = j;
+  }
+  if (!within_counter(M, mx)) return -1;
   if (M > S.code_cap) {
     if (S.d_code) cudaFree(S.d_code);
     S.d_code = nullptr;
@@ -968,7 +1001,7 @@ int dct_set_code(const long long *idx, int M) {
     CC_CK(cudaStreamSynchronize(g_stream));
   }
   S.codeM = M;
-  S.uploaded.swap(up);
+  S.up_sorted.swap(sorted);
   S.up_max = mx;
   return 0;
 }
@@ -986,7 +1019,11 @@ int dct_transform(int init_mode, int out_mode) {
   CC_CK(cudaStreamSynchronize(g_stream));
   S.layered_out = out_mode == 3;
   if (out_mode == 2) {
-    set_active(S.uploaded, S.codeM);
+    // active = uploaded; its size and largest multiplicity now, the
+    // per-word counts when a call needs them
+    S.active_pending = true;
+    S.active_size = S.codeM;
+    S.act_max = S.up_max;
     S.cnt_ver++;
   }
   return 0;
@@ -1121,6 +1158,7 @@ int swap_eval_fast(const long long *drops, int k, const long long *cand,
 int greedy_fill_impl(int max_add, long long *placed, long long *deficit) {
   if (!S.live || max_add < 0 || (max_add && !placed) || !deficit) return -1;
   if (S.g.space >= (1LL << 32)) return -1;    // 32-bit index in the key
+  ensure_active();
   // placed words are new (multiplicity 1): the counters stay within uint16
   if (!within_counter(S.active_size + max_add, std::max(S.act_max, 1)))
     return -1;
@@ -1223,6 +1261,7 @@ int dct_swap_eval(const long long *drops, int k, const long long *cand,
   const long long nc = off[k];
   if (nc > 65535 || (nc && (!cand || !gain))) return -1;
   if (!valid_words(drops, k) || !valid_words(cand, nc)) return -1;
+  ensure_active();
   for (int i = 0; i < k; i++)
     if (S.active.find(drops[i]) == S.active.end()) return -1;
   if (S.set_ok) {
