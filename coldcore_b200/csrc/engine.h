@@ -72,6 +72,7 @@ struct GroupArgs {
   // read when in16, written when out16 (values provably <= 65535)
   uint16_t *layers16;
   int in16, out16;
+  int pack;               // two inner words per 32-bit lane (group_kernel)
   long long *red;         // epilogue reduction target (generic tiles)
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
 };

@@ -200,7 +200,14 @@ enum RoundIo { kIoSmem = 0, kIoLayers = 1, kIoCnt = 2, kIoCode = 3,
 // the skew (one pad word per 2^skew) keeps that linear, because a round's
 // stride S is 1 or a multiple of 2^skew and S == 1 blocks start on a
 // multiple of 2^skew.
-template <int OP, int Q, int R1, int BM, bool FULL>
+//
+// PACK: every register, shared-memory word and lane carries TWO inner words
+// (w, w+1) as 16-bit halves of one 32-bit value, so each add and each
+// shared-memory access serves both.  Exact while every value stays below
+// 2^16 (the planner's 16-bit bound) and the inner stride is even, so a pair
+// never straddles a row; the group's HBM sides are u16 planes (one 32-bit
+// access per pair), the int32 map and the u16 cnt (unpacked at the store).
+template <int OP, int Q, int R1, int BM, bool FULL, bool PACK = false>
 __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
                                           int SD, long long o0, long long i0,
                                           int rb, int S, int src, int dst,
@@ -209,7 +216,7 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
   constexpr int QB = IPow<Q, BM>::v;
   int ne = QB;
   if (!FULL) { ne = 1; for (int t = 0; t < rb; t++) ne *= Q; }
-  const int W = g.W;
+  const int W = PACK ? g.W >> 1 : g.W;         // lanes (pairs) per row
   const int nh = g.mid / (S * ne);
   const int nblk = W * S * nh * g.Bo;
   const long long imid = g.inner * (long long)g.mid;
@@ -233,11 +240,12 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
     dw = r % W; r /= W; dmlo = r % S; r /= S; dmhi = r % nh; dob = r / nh;
   }
   for (int blk = threadIdx.x; blk < nblk; blk += blockDim.x) {
-    const bool valid = (o0 + ob < g.outer) && (i0 + w < g.inner);
+    const int wi = PACK ? 2 * w : w;                     // inner word
+    const bool valid = (o0 + ob < g.outer) && (i0 + wi < g.inner);
     const int pb = ob * g.mid + mlo + S * ne * mhi;      // tile word, e = 0
     const int sp0 = skewed(pb, g.skew) * W + w;
     const long long xb = (o0 + ob) * imid + (long long)(mlo + S * ne * mhi)
-                         * g.inner + i0 + w;
+                         * g.inner + i0 + wi;
     int32_t v[R1][QB];
 #pragma unroll
     for (int d = 0; d < R1; d++)
@@ -264,7 +272,19 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
         }
       }
     } else if (valid) {
-      if (src == kIoLayers && g.in16) {
+      if (PACK && src == kIoLayers) {            // one u32 per word pair
+#pragma unroll
+        for (int d = 0; d < R1; d++) {
+          if (d >= g.lin) break;
+          const uint16_t *p = g.layers16 + d * g.plane + xb;
+#pragma unroll
+          for (int e = 0; e < QB; e++) {
+            if (!FULL && e >= ne) break;
+            v[d][e] = (int32_t)__ldcs(reinterpret_cast<const uint32_t *>(p));
+            p += gstep;
+          }
+        }
+      } else if (src == kIoLayers && g.in16) {
 #pragma unroll
         for (int d = 0; d < R1; d++) {
           if (d >= g.lin) break;
@@ -313,7 +333,42 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
         }
       }
     } else if (valid) {
-      if (dst == kIoLayers && g.out16) {
+      if (PACK && dst == kIoLayers) {            // one u32 per word pair
+#pragma unroll
+        for (int d = 0; d < R1; d++) {
+          if (d >= g.lout) break;
+          uint16_t *p = g.layers16 + d * g.plane + xb;
+#pragma unroll
+          for (int e = 0; e < QB; e++) {
+            if (!FULL && e >= ne) break;
+            __stcs(reinterpret_cast<uint32_t *>(p), (uint32_t)v[d][e]);
+            p += gstep;
+          }
+        }
+      } else if (PACK && dst == kIoMap) {        // both halves, widened
+        int32_t *p = (g.map ? g.map : g.layers) + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          uint32_t s = 0;
+#pragma unroll
+          for (int d = 0; d < R1; d++) s += (uint32_t)v[d][e];
+          __stcs(reinterpret_cast<int2 *>(p),
+                 make_int2((int)(s & 0xFFFFu), (int)(s >> 16)));
+          p += gstep;
+        }
+      } else if (PACK) {                         // cnt: both halves at once
+        uint16_t *p = g.cnt + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          uint32_t s = 0;
+#pragma unroll
+          for (int d = 0; d < R1; d++) s += (uint32_t)v[d][e];
+          *reinterpret_cast<uint32_t *>(p) = s;
+          p += gstep;
+        }
+      } else if (dst == kIoLayers && g.out16) {
 #pragma unroll
         for (int d = 0; d < R1; d++) {
           if (d >= g.lout) break;
@@ -378,21 +433,21 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
 // A round of rb axes runs with a register block of exactly Q^rb words: the
 // kernel's own block size BM for full rounds, a compile-time smaller block
 // for the group's last, partial round (no runtime bounds in the loops).
-template <int OP, int Q, int R1, int B>
+template <int OP, int Q, int R1, int B, bool PACK = false>
 struct RoundSel {
   static __device__ __forceinline__ void run(
       const GroupArgs &g, int32_t *sm, int SD, long long o0, long long i0,
       int rb, int S, int src, int dst, int nl, const uint16_t *cs) {
     if (rb == B)
-      run_round<OP, Q, R1, B, true>(g, sm, SD, o0, i0, B, S, src, dst, nl,
-                                    cs);
+      run_round<OP, Q, R1, B, true, PACK>(g, sm, SD, o0, i0, B, S, src, dst,
+                                          nl, cs);
     else
-      RoundSel<OP, Q, R1, B - 1>::run(g, sm, SD, o0, i0, rb, S, src, dst, nl,
-                                      cs);
+      RoundSel<OP, Q, R1, B - 1, PACK>::run(g, sm, SD, o0, i0, rb, S, src,
+                                            dst, nl, cs);
   }
 };
-template <int OP, int Q, int R1>
-struct RoundSel<OP, Q, R1, 0> {
+template <int OP, int Q, int R1, bool PACK>
+struct RoundSel<OP, Q, R1, 0, PACK> {
   static __device__ __forceinline__ void run(
       const GroupArgs &, int32_t *, int, long long, long long, int, int, int,
       int, int, const uint16_t *) {}
@@ -404,7 +459,8 @@ group_kernel(const GroupArgs g) {
   extern __shared__ int32_t sm[];
   const int W = g.W;
   const int tile_words = g.Bo * g.mid;
-  const int SD = (skewed(tile_words, g.skew) + 1) * W;   // layer stride
+  const int SW = g.pack ? W >> 1 : W;                    // lanes per row
+  const int SD = (skewed(tile_words, g.skew) + 1) * SW;  // layer stride
   const int first_src = g.src == kSrcLayers ? kIoLayers
                         : g.src == kSrcCnt ? kIoCnt : kIoCode;
   const int last_dst = g.dst == kDstLayers ? kIoLayers
@@ -421,8 +477,12 @@ group_kernel(const GroupArgs g) {
     for (int r = 0; r < g.nrounds; r++) {
       const int src = r == 0 ? first_src : kIoSmem;
       const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
-      RoundSel<OP, Q, R1, BM>::run(g, sm, SD, o0, i0, g.rb[r], g.rs[r], src,
-                                   dst, R1, nullptr);
+      if (g.pack)
+        RoundSel<OP, Q, R1, BM, true>::run(g, sm, SD, o0, i0, g.rb[r],
+                                           g.rs[r], src, dst, R1, nullptr);
+      else
+        RoundSel<OP, Q, R1, BM>::run(g, sm, SD, o0, i0, g.rb[r], g.rs[r],
+                                     src, dst, R1, nullptr);
       __syncthreads();
     }
   }
@@ -870,7 +930,7 @@ int pick_group_kernel(int prob, int q, int R1, int *bm) {
 size_t group_smem_bytes(const GroupArgs &a, int R1) {
   const int tile_words = a.Bo * a.mid;
   const int skw = a.skew ? tile_words + (tile_words >> a.skew) : tile_words;
-  const size_t lay = (size_t)(skw + 1) * a.W * R1;          // words
+  const size_t lay = (size_t)(skw + 1) * (a.pack ? a.W / 2 : a.W) * R1;
   const size_t tile = ((lay + 3) & ~(size_t)3) * sizeof(int32_t);
   if (!a.pipe) return tile;
   if (a.src == kSrcCnt)                     // one tile + two cnt windows
