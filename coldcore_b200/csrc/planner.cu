@@ -103,12 +103,13 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     base.map = ptr.map;
     base.layers16 = ptr.layers16;
     base.in16 = kn.half && j > 0;          // every later group reads u16
+    base.inner = g.pw[j];
     // two inner words per lane: 16-bit values, an even inner stride (so a
-    // pair never straddles a row), and recurrences made of adds only
-    // (Hamming with q <= 3, Lee), whose every partial sum is a layer value
+    // pair never straddles a row and every pair access is 4-byte aligned),
+    // and recurrences made of adds only (Hamming with q <= 3, Lee), whose
+    // every partial sum is a layer value
     base.pack = base.in16 && kid >= 0 && base.inner % 2 == 0 &&
                 ((g.prob == kHamming && q <= 3) || g.prob == kLee);
-    base.inner = g.pw[j];
     base.prob = g.prob;
     base.R = g.R;
     base.mu = g.mu;

@@ -962,6 +962,14 @@ int ensure_group_smem(const GroupPlan &p) {
 int prepare_group(const GroupPlan &p) { return ensure_group_smem(p); }
 
 int launch_group(const GroupPlan &p, cudaStream_t s) {
+  // packed pairs need 4-byte aligned pair accesses: an even inner stride
+  // and row width, 16-bit planes in, the register kernel, no prefetch
+  if (p.a.pack && (p.a.inner % 2 || p.a.W % 2 || !p.a.in16 ||
+                   p.kernel < 0 || p.a.pipe)) {
+    fprintf(stderr, "coldcore_b200: refused a packed group with inner %lld "
+            "W %d\n", p.a.inner, p.a.W);
+    return -9;
+  }
   GroupFn fn = group_fn(p);
   const int rc = ensure_group_smem(p);
   if (rc) return rc;
