@@ -73,6 +73,9 @@ struct GroupArgs {
   uint16_t *layers16;
   int in16, out16;
   int pack;               // two inner words per 32-bit lane (group_kernel)
+  // first group of a binary Hamming cell: axis 0 is the word pair itself
+  // (inner = 2), applied once as a swap-add inside each packed lane
+  int pair_axis;
   long long *red;         // epilogue reduction target (generic tiles)
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
 };

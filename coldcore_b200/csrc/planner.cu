@@ -22,7 +22,7 @@ void set_rounds(GroupArgs &a, int q, int bm) {
   }
   std::vector<int> order(nr);
   for (int r = 0; r < nr; r++) order[r] = r;
-  if (a.W == 1 && nr >= 3) {
+  if ((a.W == 1 || a.pair_axis) && nr >= 3) {
     // HBM-facing rounds get the widest strides (coalesced lanes): the
     // widest round stores every layer, the second widest loads the
     // 2-byte cnt, the rest exchange through shared memory in between
@@ -103,13 +103,20 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     base.map = ptr.map;
     base.layers16 = ptr.layers16;
     base.in16 = kn.half && j > 0;          // every later group reads u16
-    base.inner = g.pw[j];
+    // the first group of a binary Hamming cell with 16-bit values: axis 0
+    // is the word pair itself (inner = 2, applied as a swap-add inside each
+    // lane) and the group's rounds run over axes 1.. on packed pairs
+    const bool pair = j == 0 && kn.half && kid >= 0 && g.prob == kHamming &&
+                      q == 2 && g.n >= 2 && src != kSrcLayers;
+    const int j0 = j + (pair ? 1 : 0);     // first axis of the rounds
+    base.pair_axis = pair ? 1 : 0;
+    base.inner = pair ? 2 : g.pw[j];
     // two inner words per lane: 16-bit values, an even inner stride (so a
     // pair never straddles a row and every pair access is 4-byte aligned),
     // and recurrences made of adds only (Hamming with q <= 3, Lee), whose
     // every partial sum is a layer value
-    base.pack = base.in16 && kid >= 0 && base.inner % 2 == 0 &&
-                ((g.prob == kHamming && q <= 3) || g.prob == kLee);
+    base.pack = pair || (base.in16 && kid >= 0 && base.inner % 2 == 0 &&
+                         ((g.prob == kHamming && q <= 3) || g.prob == kLee));
     base.prob = g.prob;
     base.R = g.R;
     base.mu = g.mu;
@@ -117,7 +124,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     // pipe 1 and 3 prefetch the cnt-reading first group; 3 also the last
     // group when it writes the 4-byte map (reads every layer, writes one
     // plane), decided below; 2 prefetches every group
-    base.pipe = kid >= 0 && base.src != kSrcCode && !base.in16 &&
+    base.pipe = kid >= 0 && base.src != kSrcCode && !base.in16 && !pair &&
                 (kn.pipe == 2 || ((kn.pipe == 1 || kn.pipe == 3) &&
                                   base.src == kSrcCnt));
     // the most axes that fit one tile of W inner words
@@ -126,8 +133,8 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
       a.W = W;
       long long mid = 1;
       for (;;) {
-        if (j + a.k >= g.n || a.k >= kMaxRounds) break;
-        const int qn = g.ax[j + a.k];
+        if (j0 + a.k >= g.n || a.k >= kMaxRounds) break;
+        const int qn = g.ax[j0 + a.k];
         if (kid >= 0 && qn != q) break;
         if (kid < 0 && qn > 16) break;
         const long long mid2 = mid * qn;
@@ -139,7 +146,8 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
                : (int)std::max<long long>(1, std::min<long long>(
                      outer, 2048 / (W * mid2)));
         t.skew = 0;
-        if (kid >= 0 && W == 1 && (q & (q - 1)) == 0) {
+        if (kid >= 0 && (W == 1 || (pair && W == 2)) &&
+            (q & (q - 1)) == 0) {
           int lg = 0;
           while ((1 << lg) < ipow(q, bm)) lg++;
           t.skew = lg;
@@ -164,10 +172,10 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     a.outer = g.space / (a.inner * (long long)a.mid);
     a.nchunk = (a.inner + a.W - 1) / a.W;
     a.ntiles = (a.outer + a.Bo - 1) / a.Bo * a.nchunk;
-    for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j + t];
+    for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j0 + t];
     if (kid >= 0) set_rounds(a, q, bm);
     else a.nrounds = 0;
-    const bool last = j + a.k == g.n;
+    const bool last = j0 + a.k == g.n;
     a.dst = last ? dst : kDstLayers;
     a.out16 = kn.half && !last;
     if (kn.pipe == 3 && kid >= 0 && last && dst != kDstLayers &&
@@ -178,7 +186,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
       if (group_smem_bytes(t, R1) <= budget) a.pipe = 1;
     }
     a.lin = layered ? live_layers(g, j) : 1;
-    a.lout = layered ? live_layers(g, j + a.k) : 1;
+    a.lout = layered ? live_layers(g, j0 + a.k) : 1;
     if (last && dst == kDstLayers) a.lout = R1;   // every layer, zeros too
     a.pmode = kPredEq;
     a.ptarget = 0;
@@ -189,7 +197,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     p.threads = threads_for(a, kid, bm, q);
     p.grid = occupancy_grid(p);
     out.push_back(p);
-    j += a.k;
+    j = j0 + a.k;
   }
   return out;
 }
@@ -202,13 +210,13 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   int kids[8], bms[8];
   const int nk = group_kernel_variants(p.a.prob, q, R1, kids, bms, 8);
   // the cp.async-prefetching form too, where its second buffer fits
-  const bool can_pipe = p.a.src != kSrcCode && !p.a.in16;
+  const bool can_pipe = p.a.src != kSrcCode && !p.a.in16 && !p.a.pack;
   for (int i = 0; i < nk; i++)
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {
     GroupPlan t = p;
     t.kernel = kids[i];
     t.a.pipe = pipe;
-    if (t.a.W == 1 && (q & (q - 1)) == 0) {
+    if ((t.a.W == 1 || t.a.pair_axis) && (q & (q - 1)) == 0) {
       int lg = 0;
       while ((1 << lg) < ipow(q, bms[i])) lg++;
       t.a.skew = lg;

@@ -442,7 +442,8 @@ int run_transform(int init_mode, int out_mode) {
         S.bounds_cap = need;
       }
       rc = launch_code_bounds(S.d_code, S.codeM,
-                              (long long)a0.Bo * a0.mid, a0.ntiles,
+                              (long long)a0.Bo * a0.mid * a0.inner,
+                              a0.ntiles,
                               S.d_bounds, g_stream);
       if (rc) return rc;
     }
@@ -1460,10 +1461,10 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
     long long by = X * (rd + wr);
     if (p.a.src == kSrcCode) by += 8 * S.codeM;
     if (info && 4 * n + 3 < cap) {
-      info[4 * n] = j; info[4 * n + 1] = p.a.k;
+      info[4 * n] = j; info[4 * n + 1] = p.a.k + p.a.pair_axis;
       info[4 * n + 2] = by; info[4 * n + 3] = p.kernel;
     }
-    j += p.a.k;
+    j += p.a.k + p.a.pair_axis;
     n++;
   }
   return n;

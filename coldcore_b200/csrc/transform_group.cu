@@ -162,6 +162,23 @@ __device__ __forceinline__ void stage_code(const GroupArgs &g, int32_t *sm,
   __syncthreads();
 }
 
+// The same for a first group whose words sit in pairs (inner == 2): word p
+// of the range adds 1 to the half (p & 1) of packed lane p / 2.  Counts stay
+// below 2^16 (the occurrence bound), so no add carries across halves.
+__device__ __forceinline__ void stage_code_pairs(const GroupArgs &g,
+                                                 int32_t *sm, long long tile,
+                                                 long long x0, int len) {
+  for (int P = threadIdx.x; P < (len + 1) / 2; P += blockDim.x)
+    sm[skewed(P, g.skew)] = 0;
+  __syncthreads();
+  const long long lo = g.code_bounds[tile], hi = g.code_bounds[tile + 1];
+  for (long long t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+    const int p = (int)(g.code[t] - x0);
+    atomicAdd(&sm[skewed(p >> 1, g.skew)], 1 << (16 * (p & 1)));
+  }
+  __syncthreads();
+}
+
 // bounds[t] = lower_bound(code, t * tile_words) for t = 0..ntiles
 __global__ void k_code_bounds(const long long *code, long long ncode,
                               long long tile_words, long long ntiles,
@@ -308,6 +325,17 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
             p += gstep;
           }
         }
+      } else if (PACK) {                         // kIoCnt, a word pair
+        const uint16_t *p = g.cnt + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++) {
+          if (!FULL && e >= ne) break;
+          const uint32_t c = __ldcs(reinterpret_cast<const uint32_t *>(p));
+          const uint32_t lo = (unsigned)((int)(c & 0xFFFFu) - plo) <= pspan;
+          const uint32_t hi = (unsigned)((int)(c >> 16) - plo) <= pspan;
+          v[0][e] = (int32_t)(lo | (hi << 16));
+          p += gstep;
+        }
       } else {                                   // kIoCnt
         const uint16_t *p = g.cnt + xb;
 #pragma unroll
@@ -317,6 +345,18 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
           p += gstep;
         }
       }
+    }
+    // -------- axis 0 inside each pair (binary Hamming first group), once:
+    // in the round that reads the code or cnt.  newA_d[a] = A_d[a] +
+    // A_{d-1}[a ^ 1] is an add of the halves swapped, layers descending.
+    if (PACK && OP == kOpHamming && Q == 2 && g.pair_axis &&
+        (src == kIoCnt || src == kIoCode)) {
+#pragma unroll
+      for (int e = 0; e < QB; e++)
+#pragma unroll
+        for (int d = R1 - 1; d >= 1; d--)
+          v[d][e] += (int32_t)__funnelshift_l((uint32_t)v[d - 1][e],
+                                              (uint32_t)v[d - 1][e], 16);
     }
     // -------- rb axis recurrences in registers
     if (FULL) AxisLoop<OP, Q, R1, BM, 0>::run(v, BM, g.R);
@@ -468,7 +508,13 @@ group_kernel(const GroupArgs g) {
   for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
     const long long o0 = (tile / g.nchunk) * g.Bo;
     const long long i0 = (tile % g.nchunk) * W;
-    if (g.src == kSrcCode) {
+    if (g.src == kSrcCode && g.pack) {
+      // first group, axis 0 in pairs: inner == 2, the tile is contiguous
+      const long long imid = g.inner * (long long)g.mid;
+      const long long len = (g.outer - o0) * imid;
+      const long long tw = (long long)tile_words * g.inner;
+      stage_code_pairs(g, sm, tile, o0 * imid, (int)(len < tw ? len : tw));
+    } else if (g.src == kSrcCode) {
       // first group only: W == 1, inner == 1, the tile is contiguous
       long long len = (g.outer - o0) * (long long)g.mid;
       stage_code(g, sm, tile, o0 * g.mid,
@@ -964,8 +1010,9 @@ int prepare_group(const GroupPlan &p) { return ensure_group_smem(p); }
 int launch_group(const GroupPlan &p, cudaStream_t s) {
   // packed pairs need 4-byte aligned pair accesses: an even inner stride
   // and row width, 16-bit planes in, the register kernel, no prefetch
-  if (p.a.pack && (p.a.inner % 2 || p.a.W % 2 || !p.a.in16 ||
-                   p.kernel < 0 || p.a.pipe)) {
+  if (p.a.pack && (p.a.inner % 2 || p.a.W % 2 ||
+                   !(p.a.in16 || p.a.pair_axis) || p.kernel < 0 ||
+                   p.a.pipe)) {
     fprintf(stderr, "coldcore_b200: refused a packed group with inner %lld "
             "W %d\n", p.a.inner, p.a.W);
     return -9;
