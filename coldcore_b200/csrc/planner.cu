@@ -107,7 +107,8 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     // is the word pair itself (inner = 2, applied as a swap-add inside each
     // lane) and the group's rounds run over axes 1.. on packed pairs
     const bool pair = j == 0 && kn.half && kid >= 0 && g.prob == kHamming &&
-                      q == 2 && g.n >= 2 && src != kSrcLayers;
+                      q == 2 && g.n >= 2 && g.ax[1] == 2 &&
+                      src != kSrcLayers;
     const int j0 = j + (pair ? 1 : 0);     // first axis of the rounds
     base.pair_axis = pair ? 1 : 0;
     base.inner = pair ? 2 : g.pw[j];
@@ -169,6 +170,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     } else {
       a = grow((int)base.inner);
     }
+    if (a.k < 1 || a.mid < 1) return {};     // no axis fits: no plan
     a.outer = g.space / (a.inner * (long long)a.mid);
     a.nchunk = (a.inner + a.W - 1) / a.W;
     a.ntiles = (a.outer + a.Bo - 1) / a.Bo * a.nchunk;

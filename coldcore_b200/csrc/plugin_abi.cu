@@ -432,6 +432,7 @@ int run_transform(int init_mode, int out_mode) {
       if ((rc = timing_mark(++nt))) return rc;
     }
   } else {
+    if (P.groups.empty()) return -1;           // the planner found no tile
     if (init_mode == 0) {
       const GroupArgs &a0 = P.groups[0].a;
       const long long need = a0.ntiles + 1;
