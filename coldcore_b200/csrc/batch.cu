@@ -196,10 +196,17 @@ int make_schedule(Batch *b) {
     c.first_pass = (int)b->passes.size();
     c.npass = 0;
     if (c.big) {
-      const Knobs kn{100 * 1024, 1};
+      // 16-bit planes between launches (and packed pairs where the
+      // planner can) when every layer value stays below 2^16: always for
+      // the recount (the occurrence bound checked at add), for the
+      // predicate transforms when the ball has at most 65,535 words
+      const long long ball = ball_cardinality(c.g);
       for (int t = 0; t < 3; t++) {
+        Knobs kn{100 * 1024, 1};
+        kn.half = c.R1 >= 2 && (t == 0 || ball <= 65535) ? 1 : 0;
         PlanPtrs ptr{c.layers, c.plane, c.cnt, c.dcode,
                      (long long)c.code.size(), t == 1 ? c.gain : c.loss};
+        ptr.layers16 = reinterpret_cast<uint16_t *>(c.layers + c.plane);
         const int src = t == 0 ? kSrcCode : kSrcCnt;
         const int dst = t == 0 ? kDstCnt : kDstMap;
         c.fast[t] = plan_groups(c.g, c.R1, ptr, src, dst, kn);
@@ -315,8 +322,8 @@ int run_big_cell(Batch *b, size_t i, cudaStream_t s) {
   Cell &c = b->cells[i];
   const GroupArgs &a0 = c.fast[0][0].a;
   int rc = launch_code_bounds(c.dcode, (long long)c.code.size(),
-                              (long long)a0.Bo * a0.mid, a0.ntiles, c.bounds,
-                              s);
+                              (long long)a0.Bo * a0.mid * a0.inner,
+                              a0.ntiles, c.bounds, s);
   if (rc) return rc;
   for (int t = 0; t < 3; t++) {
     for (const auto &gp : c.fast[t])
