@@ -928,14 +928,30 @@ static const KernelEntry kTable[] = {
     // Hamming, quaternary
     KE(kOpHamming, 4, 2, 2), KE(kOpHamming, 4, 3, 2), KE(kOpHamming, 4, 4, 2),
     KE(kOpHamming, 4, 5, 1),
+    // Hamming, q = 5, 6: one axis per round (up to 5 layers)
+    KE(kOpHamming, 5, 2, 1), KE(kOpHamming, 5, 3, 1), KE(kOpHamming, 5, 4, 1),
+    KE(kOpHamming, 5, 5, 1),
+    KE(kOpHamming, 6, 2, 1), KE(kOpHamming, 6, 3, 1), KE(kOpHamming, 6, 4, 1),
+    KE(kOpHamming, 6, 5, 1),
     // Lee: one axis per round
     KE(kOpLee, 7, 3, 1), KE(kOpLee, 7, 4, 1), KE(kOpLee, 7, 5, 1),
     KE(kOpLee, 5, 2, 1), KE(kOpLee, 5, 3, 1), KE(kOpLee, 5, 4, 1),
+    KE(kOpLee, 5, 5, 1),
+    KE(kOpLee, 2, 2, 1), KE(kOpLee, 2, 3, 1), KE(kOpLee, 2, 4, 1),
+    KE(kOpLee, 2, 5, 1),
+    KE(kOpLee, 3, 2, 1), KE(kOpLee, 3, 3, 1), KE(kOpLee, 3, 4, 1),
+    KE(kOpLee, 3, 5, 1),
+    KE(kOpLee, 4, 2, 1), KE(kOpLee, 4, 3, 1), KE(kOpLee, 4, 4, 1),
+    KE(kOpLee, 4, 5, 1),
+    KE(kOpLee, 6, 2, 1), KE(kOpLee, 6, 3, 1), KE(kOpLee, 6, 4, 1),
+    KE(kOpLee, 6, 5, 1),
     // small-axis window sums (torus / grid)
     KE(kOpTorus, 3, 1, 3), KE(kOpTorus, 4, 1, 2), KE(kOpTorus, 5, 1, 2),
 };
 #undef KE
 static const int kTableLen = sizeof(kTable) / sizeof(kTable[0]);
+static_assert(sizeof(kTable) / sizeof(kTable[0]) <= 64,
+              "the shared-memory opt-in cache holds 64 kernels per form");
 
 static int op_of(int prob) {
   return prob == kHamming ? kOpHamming : prob == kLee ? kOpLee
