@@ -343,16 +343,25 @@ def measure_cell(cell, args, dist, timed=True):
         rows = []
         for (i, o, k), ts in per.items():
             plan = b.plan(i, o)
+            forms = b.plan_forms(i, o)
             j0, nax, by, kid = (int(v) for v in plan[k])
             mean = sum(ts) / len(ts)
             rows.append({"transform": f"({i},{o})", "launch": k,
                          "axes": f"{j0}..{j0 + nax - 1}", "kernel_id": kid,
+                         "form": form_name(forms[k] if k < len(forms) else 0),
                          "bytes": by, "ms": mean,
                          "GBps": by / (mean * 1e-3) / 1e9})
         res["launches"] = rows
         return res
     finally:
         b.close()
+
+
+def form_name(f):
+    """Schedule form flags of one launch (GpuBackend.plan_forms) as text."""
+    names = [("pipe", 1), ("pack", 2), ("in16", 4), ("out16", 8),
+             ("pair", 16)]
+    return "+".join(n for n, bit in names if int(f) & bit) or "plain"
 
 
 def measure_batch(args, dist):
@@ -463,7 +472,8 @@ def run_b200(args, dist):
     total = sum(r["ms"] for r in rows)
     dom = max(rows, key=lambda r: r["ms"])
     ach = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
-    tkey = f"{cell.name}:{dom['transform']}:{dom['launch']}"
+    # keyed by the launch's axes: the capture must be of the same group
+    tkey = f"{cell.name}:{dom['transform']}:{dom['axes']}"
     traffic = ncu_traffic(tkey)
     cpu = None
     if dist.world == 1 and not args.no_cpu:
@@ -492,6 +502,8 @@ def run_b200(args, dist):
                             round(r["GBps"], 1) for r in rows},
             "launch_ms": {f"{r['transform']}#{r['launch']}":
                           round(r["ms"], 4) for r in rows},
+            "launch_form": {f"{r['transform']}#{r['launch']}": r["form"]
+                            for r in rows},
         },
         "clocks": res["clocks"],
         "e2e": res["e2e"],

@@ -104,6 +104,8 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
 int launch_group(const GroupPlan &p, cudaStream_t s);
 int prepare_group(const GroupPlan &p);
 size_t group_smem_bytes(const GroupArgs &a, int R1);
+// the prefetching kernel has a packed form for 16-bit layer sources
+bool pipe_pairs_ok(const GroupArgs &a);
 int pick_group_kernel(int prob, int q, int R1, int *bm);
 int group_kernel_variants(int prob, int q, int R1, int *kids, int *bms,
                           int cap);

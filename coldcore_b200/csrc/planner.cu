@@ -42,7 +42,9 @@ void set_rounds(GroupArgs &a, int q, int bm) {
 int threads_for(const GroupArgs &a, int kid, int bm, int q) {
   int t;
   if (kid >= 0) {
-    const long long words = (long long)a.W * a.mid * a.Bo;
+    // register blocks per round: packed lanes carry two words each
+    const long long words = (long long)(a.pack ? a.W / 2 : a.W) * a.mid *
+                            a.Bo;
     const int ne = ipow(q, std::min(bm, a.k));
     t = (int)std::min<long long>(kGroupThreads, words / ne);
   } else {
@@ -124,8 +126,10 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     base.src = j == 0 ? src : kSrcLayers;
     // pipe 1 and 3 prefetch the cnt-reading first group; 3 also the last
     // group when it writes the 4-byte map (reads every layer, writes one
-    // plane), decided below; 2 prefetches every group
-    base.pipe = kid >= 0 && base.src != kSrcCode && !base.in16 && !pair &&
+    // plane), decided below; 2 prefetches every group (16-bit layers only
+    // in packed pairs, whose 16-byte form is checked once W is known)
+    base.pipe = kid >= 0 && base.src != kSrcCode && !pair &&
+                (!base.in16 || base.pack) &&
                 (kn.pipe == 2 || ((kn.pipe == 1 || kn.pipe == 3) &&
                                   base.src == kSrcCnt));
     // the most axes that fit one tile of W inner words
@@ -171,6 +175,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
       a = grow((int)base.inner);
     }
     if (a.k < 1 || a.mid < 1) return {};     // no axis fits: no plan
+    if (a.pipe && a.in16 && !pipe_pairs_ok(a)) a.pipe = 0;
     a.outer = g.space / (a.inner * (long long)a.mid);
     a.nchunk = (a.inner + a.W - 1) / a.W;
     a.ntiles = (a.outer + a.Bo - 1) / a.Bo * a.nchunk;
@@ -211,13 +216,26 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   const int q = p.a.rq[0];
   int kids[8], bms[8];
   const int nk = group_kernel_variants(p.a.prob, q, R1, kids, bms, 8);
-  // the cp.async-prefetching form too, where its second buffer fits
-  const bool can_pipe = p.a.src != kSrcCode && !p.a.in16 && !p.a.pack;
+  // the cp.async-prefetching form too, where its second buffer fits (over
+  // 16-bit layers only in its packed 16-byte form)
+  const bool can_pipe = p.a.src != kSrcCode &&
+                        ((!p.a.in16 && !p.a.pack) || pipe_pairs_ok(p.a));
+  // strided groups of 32-word rows also as 16-word rows: half the tile, so
+  // twice the CTAs (and warps) per SM over the same axes
+  std::vector<int> rows{p.a.W};
+  if (p.a.W == 32 && p.a.Bo == 1 && p.a.inner >= 32 && !p.a.pair_axis)
+    rows.push_back(16);
+  for (int W : rows)
   for (int i = 0; i < nk; i++)
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {
     GroupPlan t = p;
     t.kernel = kids[i];
     t.a.pipe = pipe;
+    if (W != p.a.W) {
+      t.a.W = W;
+      t.a.nchunk = (t.a.inner + W - 1) / W;
+      t.a.ntiles = t.a.outer * t.a.nchunk;        // Bo == 1
+    }
     if ((t.a.W == 1 || t.a.pair_axis) && (q & (q - 1)) == 0) {
       int lg = 0;
       while ((1 << lg) < ipow(q, bms[i])) lg++;
@@ -235,7 +253,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
       v.threads = th;
       v.grid = occupancy_grid(v);
       if (v.kernel == p.kernel && v.threads == p.threads &&
-          v.a.pipe == p.a.pipe)
+          v.a.pipe == p.a.pipe && v.a.W == p.a.W)
         continue;
       out.push_back(v);
     }

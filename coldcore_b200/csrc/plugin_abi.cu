@@ -476,11 +476,69 @@ int run_transform(int init_mode, int out_mode) {
   return 0;
 }
 
-// Autotuner: on the first transform of a kind on a large cell, time each
-// candidate schedule twice (CUDA events on the engine stream) and keep the
-// fastest plan.  Every schedule computes the same integers, so tuning runs
-// are ordinary transforms.  CC_TUNE=0 turns it off; explicit CC_PIPE /
-// CC_SMEM_BUDGET_KB settings also pin the schedule.
+// Per-launch tuning of plan P with its grouping fixed: every register block
+// size, row width, prefetching form and CTA width of each launch, each
+// timed alone (three launches after a warm one).  A launch run again works
+// in place on its own planes, which only scrambles values; the real
+// transform runs from scratch afterwards.
+int tune_launches(Plan &P, int init_mode, int out_mode, cudaEvent_t e0,
+                  cudaEvent_t e1) {
+  // one transform with P: its code bounds (a recount's first group) and
+  // planes are then the ones every variant below reads; the variants keep
+  // the first group's tiles, so the bounds stay valid for all of them
+  S.plans[init_mode][out_mode] = P;
+  S.plan_ok[init_mode][out_mode] = true;
+  int rc = run_transform(init_mode, out_mode);
+  if (rc) return rc;
+  int pm, pt;
+  set_predicate(init_mode, &pm, &pt);
+  for (size_t gi = 0; gi < P.groups.size(); gi++) {
+    std::vector<GroupPlan> vars = group_variants(P.groups[gi], S.R1,
+                                                 220 << 10);
+    if (vars.size() < 2) continue;
+    float bv = 1e30f;
+    size_t bi = 0;
+    for (size_t vi = 0; vi < vars.size(); vi++) {
+      GroupPlan p = vars[vi];
+      p.a.pmode = pm;
+      p.a.ptarget = pt;
+      p.a.mu = g_mu;
+      p.a.code = S.d_code;
+      p.a.ncode = S.codeM;
+      p.a.code_bounds = S.d_bounds;
+      if ((rc = prepare_group(p))) return rc;
+      if ((rc = launch_group(p, g_stream))) return rc;
+      CC_CK(cudaEventRecord(e0, g_stream));
+      for (int r = 0; r < 3; r++)
+        if ((rc = launch_group(p, g_stream))) return rc;
+      CC_CK(cudaEventRecord(e1, g_stream));
+      CC_CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CC_CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < bv) { bv = ms; bi = vi; }
+    }
+    P.groups[gi] = vars[bi];
+  }
+  return 0;
+}
+
+// the axes, rows and prefetching of each launch: two knob settings that
+// give the same grouping are tuned once
+std::vector<long long> grouping_key(const Plan &P) {
+  std::vector<long long> k;
+  for (const auto &g : P.groups)
+    k.push_back(((long long)g.a.k << 32) | (g.a.W << 8) | (g.a.pipe << 1) |
+                g.a.pair_axis);
+  return k;
+}
+
+// Autotuner: on the first transform of a kind on a large cell, every
+// distinct grouping the knob settings give (shared-memory budget x
+// prefetching mode) gets its per-launch tuning, and then the whole tuned
+// transform is timed (CUDA events on the engine stream, two runs after a
+// warm one); the fastest is kept.  Every schedule computes the same
+// integers, so tuning runs are ordinary transforms.  CC_TUNE=0 turns it
+// off; explicit CC_PIPE / CC_SMEM_BUDGET_KB settings also pin the schedule.
 int autotune(int init_mode, int out_mode) {
   if (S.tuned[init_mode][out_mode]) return 0;
   S.tuned[init_mode][out_mode] = true;
@@ -499,65 +557,37 @@ int autotune(int init_mode, int out_mode) {
   CC_CK(cudaEventCreate(&e1));
   float best = 1e30f;
   Plan keep;
+  std::vector<std::vector<long long>> seen;
+  int rc = 0;
   for (const Knobs &kn : cands) {
-    S.plans[init_mode][out_mode] = make_plan(init_mode, out_mode, kn);
+    Plan P = make_plan(init_mode, out_mode, kn);
+    if (P.window || P.groups.empty()) continue;
+    const std::vector<long long> key = grouping_key(P);
+    bool dup = false;
+    for (const auto &k : seen) dup = dup || k == key;
+    if (dup) continue;
+    seen.push_back(key);
+    if ((rc = tune_launches(P, init_mode, out_mode, e0, e1))) break;
+    S.plans[init_mode][out_mode] = P;
     S.plan_ok[init_mode][out_mode] = true;
-    int rc = run_transform(init_mode, out_mode);      // warm
-    if (rc) return rc;
+    if ((rc = run_transform(init_mode, out_mode))) break;      // warm
     CC_CK(cudaEventRecord(e0, g_stream));
-    for (int r = 0; r < 2; r++) {
-      rc = run_transform(init_mode, out_mode);
-      if (rc) return rc;
-    }
+    for (int r = 0; r < 2 && !rc; r++) rc = run_transform(init_mode, out_mode);
+    if (rc) break;
     CC_CK(cudaEventRecord(e1, g_stream));
     CC_CK(cudaEventSynchronize(e1));
     float ms = 0;
     CC_CK(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) { best = ms; keep = S.plans[init_mode][out_mode]; }
-  }
-  // second stage, with the grouping fixed: per launch, every register
-  // block size and CTA width, each timed alone (three launches after a
-  // warm one).  A launch run again works in place on its own planes, which
-  // only scrambles values; the real transform runs from scratch after this.
-  S.plans[init_mode][out_mode] = keep;
-  // one transform with the kept plan: its code bounds (a recount's first
-  // group) and planes are then the ones every variant below reads; the
-  // variants keep the tiles, so the bounds stay valid for all of them
-  int rc0 = run_transform(init_mode, out_mode);
-  if (rc0) return rc0;
-  int pm, pt;
-  set_predicate(init_mode, &pm, &pt);
-  for (size_t gi = 0; gi < keep.groups.size() && !keep.window; gi++) {
-    std::vector<GroupPlan> vars = group_variants(keep.groups[gi], S.R1,
-                                                 220 << 10);
-    if (vars.size() < 2) continue;
-    float bv = 1e30f;
-    size_t bi = 0;
-    for (size_t vi = 0; vi < vars.size(); vi++) {
-      GroupPlan p = vars[vi];
-      p.a.pmode = pm;
-      p.a.ptarget = pt;
-      p.a.mu = g_mu;
-      p.a.code = S.d_code;
-      p.a.ncode = S.codeM;
-      p.a.code_bounds = S.d_bounds;
-      int rc = prepare_group(p);
-      if (rc) return rc;
-      if ((rc = launch_group(p, g_stream))) return rc;
-      CC_CK(cudaEventRecord(e0, g_stream));
-      for (int r = 0; r < 3; r++)
-        if ((rc = launch_group(p, g_stream))) return rc;
-      CC_CK(cudaEventRecord(e1, g_stream));
-      CC_CK(cudaEventSynchronize(e1));
-      float ms = 0;
-      CC_CK(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < bv) { bv = ms; bi = vi; }
-    }
-    S.plans[init_mode][out_mode].groups[gi] = vars[bi];
+    if (ms < best) { best = ms; keep = P; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  S.tune_ms[init_mode][out_mode] = best / 2;
+  if (rc) return rc;
+  if (!keep.groups.empty()) S.plans[init_mode][out_mode] = keep;
+  else S.plans[init_mode][out_mode] = make_plan(init_mode, out_mode,
+                                                default_knobs());
+  S.plan_ok[init_mode][out_mode] = true;
+  S.tune_ms[init_mode][out_mode] = best < 1e29f ? best / 2 : 0.f;
   return 0;
 }
 
@@ -1466,6 +1496,23 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
       info[4 * n + 2] = by; info[4 * n + 3] = p.kernel;
     }
     j += p.a.k + p.a.pair_axis;
+    n++;
+  }
+  return n;
+}
+
+int dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap) {
+  if (!S.live || init_mode < 0 || init_mode > 2 || out_mode < 1 ||
+      out_mode > 3 || cap < 0)
+    return -1;
+  Plan &P = plan_for(init_mode, out_mode);
+  if (P.window) return 0;
+  int n = 0;
+  for (const auto &p : P.groups) {
+    if (forms && n < cap)
+      forms[n] = (p.a.pipe ? 1 : 0) | (p.a.pack ? 2 : 0) |
+                 (p.a.in16 ? 4 : 0) | (p.a.out16 ? 8 : 0) |
+                 (p.a.pair_axis ? 16 : 0);
     n++;
   }
   return n;

@@ -593,6 +593,29 @@ __device__ __forceinline__ void prefetch_layers(const GroupArgs &g,
   }
 }
 
+// packed pairs from 16-bit planes: a 16-byte copy is 8 inner words, i.e.
+// 4 packed lanes, and lands as is (two words per 32-bit shared word, low
+// half first, the order run_round's packed lanes use).  The launcher admits
+// this form only with W and the inner stride multiples of 8, so every
+// source and destination is 16-byte aligned and no copy crosses a row end.
+__device__ __forceinline__ void prefetch_pairs(const GroupArgs &g,
+                                               int32_t *buf, int SD,
+                                               long long tile) {
+  const long long o0 = (tile / g.nchunk) * g.Bo;
+  const long long i0 = (tile % g.nchunk) * g.W;
+  const long long imid = g.inner * (long long)g.mid;
+  const int W8 = g.W / 8, SW = g.W / 2, n = g.Bo * g.mid * W8;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    const int w = (idx % W8) * 8, p = idx / W8;
+    const int ob = p / g.mid, m = p % g.mid;
+    if (o0 + ob >= g.outer || i0 + w >= g.inner) continue;
+    const long long x = (o0 + ob) * imid + (long long)m * g.inner + i0 + w;
+    const int sp = skewed(p, g.skew) * SW + w / 2;
+    for (int d = 0; d < g.lin; d++)
+      cp_async16(buf + d * SD + sp, g.layers16 + d * g.plane + x);
+  }
+}
+
 // first group (inner == 1): the tile is the contiguous range
 // [x0, x0 + len); copy the aligned 8-counter window around it and return
 // the offset of x0 inside the window
@@ -614,7 +637,11 @@ group_kernel_pipe(const GroupArgs g) {
   extern __shared__ __align__(16) int32_t sm[];
   const int W = g.W;
   const int tile_words = g.Bo * g.mid;
-  const int SD = (skewed(tile_words, g.skew) + 1) * W;   // layer stride
+  // packed pairs (16-bit layer source only): W / 2 lanes per row
+  constexpr bool kPackable = (OP == kOpHamming && Q <= 3) || OP == kOpLee;
+  const bool pk = kPackable && g.pack;
+  const int SW = pk ? W >> 1 : W;
+  const int SD = (skewed(tile_words, g.skew) + 1) * SW;  // layer stride
   const bool from_cnt = g.src == kSrcCnt;
   const int cbw = (tile_words + 16 + 7) & ~7;            // cnt window words
   // every buffer starts on a 16-byte boundary (cp.async 16-byte copies)
@@ -629,6 +656,7 @@ group_kernel_pipe(const GroupArgs g) {
   long long tile = blockIdx.x;
   if (tile < g.ntiles) {
     if (from_cnt) off0 = prefetch_cnt(g, cb0, tile);
+    else if (pk) prefetch_pairs(g, buf0, SD, tile);
     else prefetch_layers(g, buf0, SD, tile);
   }
   cp_commit();
@@ -639,6 +667,8 @@ group_kernel_pipe(const GroupArgs g) {
       if (from_cnt) {
         const int o = prefetch_cnt(g, odd ? cb0 : cb1, next);
         if (odd) off0 = o; else off1 = o;
+      } else if (pk) {
+        prefetch_pairs(g, odd ? buf0 : buf1, SD, next);
       } else {
         prefetch_layers(g, odd ? buf0 : buf1, SD, next);
       }
@@ -654,8 +684,12 @@ group_kernel_pipe(const GroupArgs g) {
       const int src = r > 0 ? kIoSmem : from_cnt ? kIoCntSmem : kIoSmem;
       const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
       const int nl = r > 0 ? R1 : g.lin;
-      RoundSel<OP, Q, R1, BM>::run(g, buf, SD, o0, i0, g.rb[r], g.rs[r], src,
-                                   dst, nl, cs);
+      if (pk)
+        RoundSel<OP, Q, R1, BM, kPackable>::run(g, buf, SD, o0, i0, g.rb[r],
+                                                g.rs[r], src, dst, nl, cs);
+      else
+        RoundSel<OP, Q, R1, BM>::run(g, buf, SD, o0, i0, g.rb[r], g.rs[r],
+                                     src, dst, nl, cs);
       __syncthreads();
     }
   }
@@ -1023,14 +1057,34 @@ int ensure_group_smem(const GroupPlan &p) {
 // ahead of a stream capture, so that the capture only records launches
 int prepare_group(const GroupPlan &p) { return ensure_group_smem(p); }
 
+// The packed form of the prefetching kernel: 16-byte copies of 16-bit
+// layers into packed lanes need W and the inner stride multiples of 8 words,
+// 16-byte aligned planes, and a layer source (not the pair first group).
+bool pipe_pairs_ok(const GroupArgs &a) {
+  return a.pack && a.in16 && !a.pair_axis && a.src == kSrcLayers &&
+         a.W % 8 == 0 && a.inner % 8 == 0 && a.plane % 8 == 0 &&
+         (reinterpret_cast<uintptr_t>(a.layers16) & 15) == 0;
+}
+
 int launch_group(const GroupPlan &p, cudaStream_t s) {
   // packed pairs need 4-byte aligned pair accesses: an even inner stride
-  // and row width, 16-bit planes in, the register kernel, no prefetch
+  // and row width, 16-bit planes in, a register kernel with a packed form
+  // (Hamming q <= 3, Lee), and prefetching only in its 16-byte form
+  const bool packs = p.kernel >= 0 &&
+                     ((kTable[p.kernel].op == kOpHamming &&
+                       kTable[p.kernel].q <= 3) ||
+                      kTable[p.kernel].op == kOpLee);
   if (p.a.pack && (p.a.inner % 2 || p.a.W % 2 ||
-                   !(p.a.in16 || p.a.pair_axis) || p.kernel < 0 ||
-                   p.a.pipe)) {
+                   !(p.a.in16 || p.a.pair_axis) || !packs ||
+                   (p.a.pipe && !pipe_pairs_ok(p.a)))) {
     fprintf(stderr, "coldcore_b200: refused a packed group with inner %lld "
-            "W %d\n", p.a.inner, p.a.W);
+            "W %d pipe %d\n", p.a.inner, p.a.W, p.a.pipe);
+    return -9;
+  }
+  // the unpacked prefetch copies 32-bit layers: no 16-bit source
+  if (!p.a.pack && p.a.pipe && p.a.in16) {
+    fprintf(stderr, "coldcore_b200: refused a prefetching group over "
+            "16-bit planes\n");
     return -9;
   }
   GroupFn fn = group_fn(p);

@@ -85,6 +85,7 @@ def _bind(path):
         "dct_use_fmt": (I, [I]),
         "dct_b200_stream": (_LL, []),
         "dct_b200_plan": (I, [I, I, _LLP, I]),
+        "dct_b200_plan_forms": (I, [I, I, _I32P, I]),
         "dct_b200_read_layer": (I, [I, _LL, _LL, _I32P]),
         "dct_b200_read_map": (I, [_LL, _LL, _I32P]),
         "dct_b200_set_timing": (I, [I]),
@@ -329,6 +330,19 @@ class GpuBackend:
         if n < 0:
             _check("plan", n)
         return buf[:4 * n].reshape(n, 4)
+
+    PIPE, PACK, IN16, OUT16, PAIR = 1, 2, 4, 8, 16
+
+    def plan_forms(self, init_mode, out_mode):
+        """Schedule form of each group launch of one transform, as bit flags
+        (PIPE prefetching kernel, PACK word pairs, IN16 / OUT16 16-bit
+        layers, PAIR axis 0 inside each pair)."""
+        buf = np.zeros(64, dtype=np.int32)
+        n = self._lib.dct_b200_plan_forms(init_mode, out_mode,
+                                          _p(buf, ctypes.c_int32), len(buf))
+        if n < 0:
+            _check("plan_forms", n)
+        return buf[:n].copy()
 
     # ---------------- incremental / exact
     def ball_update(self, idx, delta):

@@ -38,7 +38,8 @@ def main():
                     raise RuntimeError("transform failed")
             plan = b.plan(i, o)              # after the autotuner ran
             print(f"{cell.name} {m}: plan (axis0, axes, bytes, kernel) = "
-                  f"{plan.tolist()}")
+                  f"{plan.tolist()}, forms (1 pipe, 2 pack, 4 in16, "
+                  f"8 out16, 16 pair) = {b.plan_forms(i, o).tolist()}")
             if args.nvtx:
                 import torch
                 torch.cuda.nvtx.range_push("capture")

@@ -146,6 +146,11 @@ CCP_API long long dct_b200_stream(void);
  * algorithmic HBM bytes read + written, kernel id); returns the number of
  * launches (at most cap/4 described) or a negative error. */
 CCP_API int  dct_b200_plan(int init_mode, int out_mode, long long *info, int cap);
+/* schedule form of each group launch of one transform (no counterpart in
+ * the reference): bit 1 prefetching (cp.async) kernel, 2 packed word pairs,
+ * 4 16-bit layer source, 8 16-bit layer output, 16 axis 0 inside each pair;
+ * returns the number of launches (0 for window passes) or a negative error */
+CCP_API int  dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap);
 /* per-launch device timing of transforms (events around every launch;
  * DCT_TIMING=1 in the environment turns it on too and prints each time to
  * stderr, the reference's DCT_TIMING, dctcore_hamming.cuh:464-511) */

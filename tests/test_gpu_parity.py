@@ -67,6 +67,39 @@ def test_family_cells(problem, axes, R, mu):
                               g[key(cid, "upd_gather1")])
 
 
+PIPE_PAIR_CELLS = [("hamming", [2] * 16, 3, 1), ("hamming", [2] * 15, 2, 2),
+                   ("hamming", [2] * 17, 1, 1), ("lee", [4] * 8, 3, 1)]
+
+
+@pytest.mark.parametrize("budget", ["16", "40"])
+@pytest.mark.parametrize("problem,axes,R,mu", PIPE_PAIR_CELLS,
+                         ids=lambda v: str(v))
+def test_prefetch_in_pairs(monkeypatch, problem, axes, R, mu, budget):
+    """Every group prefetching (CC_PIPE=2): the 16-bit layers of the packed
+    launches are copied 16 bytes (4 packed lanes) at a time by cp.async.
+    cnt, gain and loss equal the oracle's, and the plans hold that form."""
+    monkeypatch.setenv("CC_PIPE", "2")
+    monkeypatch.setenv("CC_SMEM_BUDGET_KB", budget)
+    size = int(np.prod(axes))
+    rng = np.random.default_rng(size + 7 * R + mu)
+    code = np.sort(rng.choice(size, size=max(4, size // 300), replace=False))
+    o = OracleBackend(axes, R, problem, mu=mu)
+    with GpuBackend(axes, R, problem=problem, mu=mu) as b:
+        b.recount(code)
+        o.recount(code)
+        assert np.array_equal(b.read_cnt(), o.cnt)
+        b.gain_map()
+        o.gain_map()
+        assert np.array_equal(b.map_all(), o.map)
+        b.loss_map()
+        o.loss_map()
+        assert np.array_equal(b.map_all(), o.map)
+        both = GpuBackend.PIPE | GpuBackend.PACK
+        for mode in ((0, 2), (1, 1), (2, 1)):
+            forms = b.plan_forms(*mode)
+            assert any((f & both) == both for f in forms), forms.tolist()
+
+
 def test_k3_8_2_config_with_100_updates():
     """K_3(8,2), 30 codewords (seed 0): full int32 count / gain / loss
     fields, then 100 seeded add/remove updates; cnt and count_eq(0..3) after
