@@ -504,6 +504,8 @@ def run_b200(args, dist):
                           round(r["ms"], 4) for r in rows},
             "launch_form": {f"{r['transform']}#{r['launch']}": r["form"]
                             for r in rows},
+            "launch_axes": {f"{r['transform']}#{r['launch']}": r["axes"]
+                            for r in rows},
         },
         "clocks": res["clocks"],
         "e2e": res["e2e"],
