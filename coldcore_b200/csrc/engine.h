@@ -103,6 +103,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
 // launchers (transform_*.cu)
 int launch_group(const GroupPlan &p, cudaStream_t s);
 int prepare_group(const GroupPlan &p);
+int group_blocks_per_sm(const GroupPlan &p);
 size_t group_smem_bytes(const GroupArgs &a, int R1);
 // the prefetching kernel has a packed form for 16-bit layer sources
 bool pipe_pairs_ok(const GroupArgs &a);

@@ -57,13 +57,17 @@ int threads_for(const GroupArgs &a, int kid, int bm, int q) {
 }
 
 int occupancy_grid(const GroupPlan &p) {
-  // persistent: as many CTAs as fit, capped by the tile count
-  int per_sm = 1;
-  const size_t budget_sm = 228 * 1024;
-  per_sm = (int)std::max<size_t>(1, budget_sm / (p.smem + 1024));
-  const int by_threads = 2048 / p.threads;
-  if (per_sm > by_threads) per_sm = by_threads;
-  if (per_sm < 1) per_sm = 1;
+  // persistent: as many CTAs as are resident at once (registers included:
+  // a grid above that runs its last CTAs as a second, unbalanced wave),
+  // capped by the tile count
+  int per_sm = group_blocks_per_sm(p);
+  if (per_sm < 1) {                   // estimate from shared memory, threads
+    const size_t budget_sm = 228 * 1024;
+    per_sm = (int)std::max<size_t>(1, budget_sm / (p.smem + 1024));
+    const int by_threads = 2048 / p.threads;
+    if (per_sm > by_threads) per_sm = by_threads;
+    if (per_sm < 1) per_sm = 1;
+  }
   long long grid = (long long)sm_count() * per_sm;
   if (grid > p.a.ntiles) grid = p.a.ntiles;
   return (int)std::max<long long>(1, grid);

@@ -1057,6 +1057,20 @@ int ensure_group_smem(const GroupPlan &p) {
 // ahead of a stream capture, so that the capture only records launches
 int prepare_group(const GroupPlan &p) { return ensure_group_smem(p); }
 
+// CTAs of plan p's kernel that are resident on one SM at once (its
+// registers, shared memory and threads all counted), or 0 when the runtime
+// cannot say
+int group_blocks_per_sm(const GroupPlan &p) {
+  if (ensure_group_smem(p)) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, (const void *)group_fn(p), p.threads, p.smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 // The packed form of the prefetching kernel: 16-byte copies of 16-bit
 // layers into packed lanes need W and the inner stride multiples of 8 words,
 // 16-byte aligned planes, and a layer source (not the pair first group).
