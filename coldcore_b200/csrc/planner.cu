@@ -66,6 +66,7 @@ int occupancy_grid(const GroupPlan &p) {
     per_sm = (int)std::max<size_t>(1, budget_sm / (p.smem + 1024));
     const int by_threads = 2048 / p.threads;
     if (per_sm > by_threads) per_sm = by_threads;
+    if (per_sm > 32) per_sm = 32;     // resident CTAs per SM, at most
     if (per_sm < 1) per_sm = 1;
   }
   long long grid = (long long)sm_count() * per_sm;

@@ -1501,6 +1501,63 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
   return n;
 }
 
+int dct_b200_plan_probe(int problem, int n, const int *ax, int R,
+                        int init_mode, int out_mode, int budget_kb, int pipe,
+                        int half, long long *rows, int cap) {
+  if (n < 1 || n > kMaxAxes || R < 1 || !ax || problem < 0 || problem > 3 ||
+      init_mode < 0 || init_mode > 2 || out_mode < 1 || out_mode > 3 ||
+      (out_mode == 2 && init_mode != 0) || budget_kb < 16 ||
+      budget_kb > 220 || pipe < 0 || pipe > 3 || cap < 0)
+    return -1;
+  const bool layered = problem == kHamming || problem == kLee;
+  if (layered && R + 1 > kMaxLayers) return -1;
+  if (!layered && out_mode == 3) return -1;
+  Geometry g{};
+  g.prob = problem; g.n = n; g.R = R; g.mu = 1;
+  g.pw[0] = 1;
+  for (int i = 0; i < n; i++) {
+    if (ax[i] < 2 || ax[i] >= (1 << 24)) return -1;
+    if (layered && ax[i] > 16) return -1;
+    if (problem == kTorus && (ax[i] < 3 || 2 * R + 1 > ax[i])) return -1;
+    if (g.pw[i] > (1LL << 40) / ax[i]) return -2;
+    g.ax[i] = ax[i];
+    g.pw[i + 1] = g.pw[i] * ax[i];
+  }
+  g.space = g.pw[n];
+  bool wide = false;
+  for (int i = 0; i < n; i++) wide = wide || ax[i] > 16;
+  if (!layered && wide) return 0;             // window passes, not groups
+  const int R1 = layered ? R + 1 : 1;
+  const int src = init_mode == 0 ? kSrcCode : kSrcCnt;
+  const int dst = out_mode == 1 ? kDstMap
+                  : out_mode == 2 ? kDstCnt : kDstLayers;
+  // never dereferenced: aligned stand-ins for the planes
+  int32_t *const fake = reinterpret_cast<int32_t *>(uintptr_t(1) << 12);
+  const long long plane = round_up(g.space, kPlaneAlign);
+  PlanPtrs ptr{fake, plane, reinterpret_cast<uint16_t *>(fake),
+               reinterpret_cast<long long *>(fake), 0, nullptr};
+  ptr.layers16 = reinterpret_cast<uint16_t *>(fake + plane);
+  Knobs kn{(size_t)budget_kb << 10, pipe};
+  kn.half = half && R1 >= 2 && dst != kDstLayers;
+  const std::vector<GroupPlan> P = plan_groups(g, R1, ptr, src, dst, kn);
+  int m = 0, j = 0;
+  for (const auto &p : P) {
+    const GroupArgs &a = p.a;
+    int rbsum = 0;
+    for (int r = 0; r < a.nrounds; r++) rbsum += a.rb[r];
+    const long long row[24] = {
+        j, a.k + a.pair_axis, a.pair_axis, a.W, a.mid, a.Bo, a.inner,
+        a.outer, a.ntiles, p.kernel, a.pipe, a.pack, a.in16, a.out16,
+        (long long)p.smem, p.threads, a.lin, a.lout, a.skew, p.grid, a.src,
+        a.dst, a.nrounds, rbsum};
+    if (rows && 24 * (m + 1) <= cap)
+      for (int t = 0; t < 24; t++) rows[24 * m + t] = row[t];
+    j += a.k + a.pair_axis;
+    m++;
+  }
+  return m;
+}
+
 int dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap) {
   if (!S.live || init_mode < 0 || init_mode > 2 || out_mode < 1 ||
       out_mode > 3 || cap < 0)

@@ -1061,6 +1061,13 @@ int prepare_group(const GroupPlan &p) { return ensure_group_smem(p); }
 // registers, shared memory and threads all counted), or 0 when the runtime
 // cannot say
 int group_blocks_per_sm(const GroupPlan &p) {
+  static int have_device = -1;                // plans are also built on hosts
+  if (have_device < 0) {                      // without a GPU (plan probes)
+    int n = 0;
+    have_device = cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+    cudaGetLastError();
+  }
+  if (!have_device) return 0;
   if (ensure_group_smem(p)) return 0;
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(

@@ -86,6 +86,8 @@ def _bind(path):
         "dct_b200_stream": (_LL, []),
         "dct_b200_plan": (I, [I, I, _LLP, I]),
         "dct_b200_plan_forms": (I, [I, I, _I32P, I]),
+        "dct_b200_plan_probe": (I, [I, I, ctypes.POINTER(ctypes.c_int), I, I,
+                                    I, I, I, I, _LLP, I]),
         "dct_b200_read_layer": (I, [I, _LL, _LL, _I32P]),
         "dct_b200_read_map": (I, [_LL, _LL, _I32P]),
         "dct_b200_set_timing": (I, [I]),
@@ -121,6 +123,29 @@ def load_plugin(path=None):
                 "(run `python -m coldcore_b200.build`)")
         _libs[path] = _bind(path)
     return _libs[path]
+
+
+PLAN_FIELDS = ("axis0", "axes", "pair", "W", "mid", "Bo", "inner", "outer",
+               "tiles", "kernel", "pipe", "pack", "in16", "out16", "smem",
+               "threads", "lin", "lout", "skew", "grid", "src", "dst",
+               "rounds", "round_axes")
+
+
+def plan_probe(problem, axes, R, init_mode, out_mode, budget_kb=100, pipe=1,
+               half=True, plugin_path=None):
+    """The launches the planner gives a geometry, without a cell or a GPU:
+    one dict per launch (``PLAN_FIELDS``), [] for window passes."""
+    lib = load_plugin(plugin_path)
+    ax = (ctypes.c_int * len(axes))(*[int(a) for a in axes])
+    rows = np.zeros(24 * 64, dtype=np.int64)
+    n = lib.dct_b200_plan_probe(PROBLEM_IDS[problem], len(axes), ax, int(R),
+                                int(init_mode), int(out_mode), int(budget_kb),
+                                int(pipe), 1 if half else 0, _p(rows),
+                                len(rows))
+    if n < 0:
+        _check("plan_probe", n)
+    return [dict(zip(PLAN_FIELDS, (int(v) for v in rows[24 * i:24 * i + 24])))
+            for i in range(n)]
 
 
 def locality_order(pats, axes):

@@ -151,6 +151,17 @@ CCP_API int  dct_b200_plan(int init_mode, int out_mode, long long *info, int cap
  * 4 16-bit layer source, 8 16-bit layer output, 16 axis 0 inside each pair;
  * returns the number of launches (0 for window passes) or a negative error */
 CCP_API int  dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap);
+/* the group schedule the planner gives a geometry, without a cell or a GPU
+ * (no counterpart in the reference): for problem / axes / R, transform
+ * (init_mode, out_mode), tile budget (KB), prefetch mode 0-3 and 16-bit
+ * planes on/off, 24 values per launch: first axis, axes, pair axis, W,
+ * mid, Bo, inner, outer, tiles, kernel id, prefetching, packed, 16-bit
+ * source, 16-bit output, shared bytes, threads, live layers in, out,
+ * skew, grid, source, destination, rounds, axes over all rounds.  Returns
+ * the number of launches (0 for window passes) or a negative error. */
+CCP_API int  dct_b200_plan_probe(int problem, int n, const int *ax, int R,
+                                 int init_mode, int out_mode, int budget_kb,
+                                 int pipe, int half, long long *rows, int cap);
 /* per-launch device timing of transforms (events around every launch;
  * DCT_TIMING=1 in the environment turns it on too and prints each time to
  * stderr, the reference's DCT_TIMING, dctcore_hamming.cuh:464-511) */

@@ -100,6 +100,31 @@ def test_prefetch_in_pairs(monkeypatch, problem, axes, R, mu, budget):
             assert any((f & both) == both for f in forms), forms.tolist()
 
 
+@pytest.mark.parametrize("problem,axes,R", [("hamming", [2] * 16, 3),
+                                            ("lee", [4] * 8, 3),
+                                            ("hamming", [3] * 9, 2),
+                                            ("hamming", [2, 3, 4, 5], 2)])
+def test_plan_probe_matches_the_live_plan(monkeypatch, problem, axes, R):
+    """The host-only plan probe gives the launches a live cell runs (cells
+    below the autotuner's size, default knobs)."""
+    from coldcore_b200.gpu import plan_probe
+    monkeypatch.delenv("CC_PIPE", raising=False)
+    monkeypatch.delenv("CC_SMEM_BUDGET_KB", raising=False)
+    size = int(np.prod(axes))
+    code = np.sort(np.random.default_rng(size).choice(size, size // 50,
+                                                      replace=False))
+    with GpuBackend(axes, R, problem=problem) as b:
+        b.recount(code)
+        for mode in ((0, 2), (1, 1), (2, 1)):
+            live, forms = b.plan(*mode), b.plan_forms(*mode)
+            probe = plan_probe(problem, axes, R, *mode)
+            assert [(int(r[0]), int(r[1]), int(r[3])) for r in live] == \
+                [(L["axis0"], L["axes"], L["kernel"]) for L in probe]
+            assert forms.tolist() == [
+                L["pipe"] | 2 * L["pack"] | 4 * L["in16"] | 8 * L["out16"] |
+                16 * L["pair"] for L in probe]
+
+
 def test_k3_8_2_config_with_100_updates():
     """K_3(8,2), 30 codewords (seed 0): full int32 count / gain / loss
     fields, then 100 seeded add/remove updates; cnt and count_eq(0..3) after
