@@ -547,9 +547,9 @@ int dct_batch_build(long long h, int tile_kb) {
   if (tile_kb > 0) return schedule();
   // autotune the tile budget: time one graph launch per candidate
   static const int cand_kb[] = {24, 48, 96};
-  cudaEvent_t e0, e1;
-  CC_CK(cudaEventCreate(&e0));
-  CC_CK(cudaEventCreate(&e1));
+  EventPair ev;
+  if ((rc = ev.create())) return rc;
+  cudaEvent_t e0 = ev.e0, e1 = ev.e1;
   float best = 1e30f;
   int best_kb = 48;
   for (int kb : cand_kb) {
@@ -564,8 +564,6 @@ int dct_batch_build(long long h, int tile_kb) {
     CC_CK(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) { best = ms; best_kb = kb; }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   b->tile_budget = (size_t)best_kb * 1024;
   b->tuned_ms = best;
   return schedule();

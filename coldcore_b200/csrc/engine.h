@@ -228,3 +228,20 @@ int sm_count();
       return -(100 + (int)e_);                                              \
     }                                                                       \
   } while (0)
+
+namespace cc {
+// Two timing events, destroyed on every way out of the scope that made
+// them (error returns included).
+struct EventPair {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int create() {
+    CC_CK(cudaEventCreate(&e0));
+    CC_CK(cudaEventCreate(&e1));
+    return 0;
+  }
+  ~EventPair() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+}  // namespace cc

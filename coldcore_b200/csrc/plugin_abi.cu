@@ -552,13 +552,13 @@ int autotune(int init_mode, int out_mode) {
                                 {100 << 10, 2}, {100 << 10, 3},
                                 {200 << 10, 3}, {160 << 10, 2},
                                 {200 << 10, 2}};
-  cudaEvent_t e0, e1;
-  CC_CK(cudaEventCreate(&e0));
-  CC_CK(cudaEventCreate(&e1));
+  EventPair ev;
+  int rc = ev.create();
+  if (rc) return rc;
+  cudaEvent_t e0 = ev.e0, e1 = ev.e1;
   float best = 1e30f;
   Plan keep;
   std::vector<std::vector<long long>> seen;
-  int rc = 0;
   for (const Knobs &kn : cands) {
     Plan P = make_plan(init_mode, out_mode, kn);
     if (P.window || P.groups.empty()) continue;
@@ -580,8 +580,6 @@ int autotune(int init_mode, int out_mode) {
     CC_CK(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) { best = ms; keep = P; }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   if (rc) return rc;
   if (!keep.groups.empty()) S.plans[init_mode][out_mode] = keep;
   else S.plans[init_mode][out_mode] = make_plan(init_mode, out_mode,
