@@ -3,7 +3,7 @@
 The proposal plugs into the ruin choice of coldcore's LNS round
 (src/coldcore/search.py:734-743): given the incumbent code, it chooses
 which k incumbents to remove.  The exact repair and the exact counters
-still judge every round (search.py:744-754).
+still score every round (search.py:744-754).
 
 Pieces:
 

@@ -23,7 +23,7 @@ round trip.  The default stays the Python lazy greedy.
 One selection rule is added: ``select="learned"`` asks a *proposer* (see
 :mod:`coldcore_b200.learned`) for the k incumbents to remove.  When its
 confidence gate is closed the round falls back to the bandit.  Every round
-is still judged by the exact repair and the exact counters, whichever rule
+is still scored by the exact repair and the exact counters, whichever rule
 picked the ruin.
 
 The searcher is backend-blind.  It calls only the protocol methods

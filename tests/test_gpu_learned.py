@@ -121,7 +121,7 @@ def test_move_log_train_and_learned_lns(gpu):
               select="learned", log_every=0)
         assert t.stats["learned_rounds"] >= 1
         assert prop.stats["proposed"] == t.stats["learned_rounds"]
-        # every round was judged exactly: the incremental count is the recount
+        # every round was scored exactly: the incremental count is the recount
         assert t.verify_full() == t.uncov
         assert len(np.unique(t.code)) == len(t.code)
     finally:
@@ -154,7 +154,7 @@ def test_learned_proposal_beats_plain_lns_on_k3_14_3(gpu):
     greedy start, a descent whose ruins the trained model picks does at
     least as well as the plain descent with the record mix in the same wall
     time: a smaller verified size, or the plain run's best size reached no
-    later.  Both are judged by the exact repair and full recounts.  The
+    later.  Both are scored by the exact repair and full recounts.  The
     model is trained here on moves logged from plain runs on other
     seeds."""
     from coldcore_b200.learned import LearnedRuin, RuinFeatures, train_scorer

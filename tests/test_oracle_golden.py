@@ -1,6 +1,6 @@
 """The CPU oracle against the reference's own outputs (golden fixtures) and
 against the brute-force restatement.  Pins the oracle before any GPU result
-is judged by it."""
+is checked against it."""
 import numpy as np
 import pytest
 
