@@ -415,6 +415,20 @@ def measure_batch(args, dist):
         out["persistent"]["instances_per_s"]
         / out["singleton_per_cell"]["instances_per_s"], 2)
     out["words"] = int(sum(int(np.prod(a)) for _, a, _, _ in cells))
+    if not args.no_cpu and dist.world == 1:
+        # the reference campaign's own parallelism: one cell per process on
+        # every host core, here with the C restatement of its CPU DP
+        from oracle.cport import campaign_rate
+        rate, wall, busy, workers = campaign_rate(cells)
+        out["cpu_baseline"] = {
+            "value": round(rate, 2), "unit": "instances/s", "cores": workers,
+            "kind": "port",
+            "sample": f"all {len(cells)} cells, one step each (recount, "
+                      f"deficit, gain + max, loss + max), C restatement, "
+                      f"{workers} single-threaded spawned worker processes, "
+                      f"largest first: {wall:.1f} s wall, {busy:.1f} s busy"}
+        out["speedup_vs_cpu"] = round(
+            out["persistent"]["instances_per_s"] / rate, 1)
     return out
 
 

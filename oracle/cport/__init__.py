@@ -6,6 +6,7 @@ Test infrastructure and the timed CPU baseline only.  ``build()`` compiles
 import ctypes
 import os
 import subprocess
+import time
 
 import numpy as np
 
@@ -77,3 +78,50 @@ class CPortCell:
     def loss_map(self):
         self._pred(2, 0)
         self._run(self.map, None)
+
+
+# ------------------------------------------------------------ campaign pool
+def _one_thread():
+    """Pool initializer: one OpenMP thread per worker process (set before
+    the worker first loads the library)."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+
+
+def _warm(seconds):
+    lib()
+    time.sleep(seconds)
+    return os.getpid()
+
+
+def cell_step(item):
+    """One campaign step of one cell on one host core: recount, deficit,
+    gain map and its maximum, loss map and its maximum.  Returns seconds."""
+    problem, axes, R, code = item
+    t0 = time.perf_counter()
+    c = CPortCell(list(axes), R, problem)
+    c.recount(code)
+    int(np.maximum(c.mu - c.cnt.astype(np.int64), 0).sum())
+    c.gain_map()
+    int(c.map.max())
+    c.loss_map()
+    int(c.map.max())
+    return time.perf_counter() - t0
+
+
+def campaign_rate(cells, workers=None):
+    """A campaign step over `cells` ((problem, axes, R, code) tuples) on a
+    pool of single-threaded worker processes, the way coldcore's campaign
+    runs one cell per process: largest cells first, the pool started (and
+    every worker's library loaded) outside the timed region.  Returns
+    (instances/s, wall seconds, summed cell seconds, workers)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    workers = workers or os.cpu_count() or 1
+    order = sorted(cells, key=lambda c: -int(np.prod(c[1])))
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn"),
+                             initializer=_one_thread) as ex:
+        list(ex.map(_warm, [0.3] * workers))
+        t0 = time.perf_counter()
+        per = list(ex.map(cell_step, order, chunksize=1))
+        wall = time.perf_counter() - t0
+    return len(cells) / wall, wall, float(sum(per)), workers
