@@ -1,0 +1,160 @@
+"""CPU restatement of coldcore's explicit-incidence backends (plugin ABI 2).
+
+Test infrastructure only: the checker of the ABI-2 engine
+(``coldcore_b200/csrc/sparse_abi.cu``), never part of the product path.
+
+Restates, with the same integer semantics:
+
+* ``SparseIncidenceBackend`` (coldcore ``src/coldcore/incidence.py:89-298``):
+  n_cand candidates, each covering the d universe elements of one row of
+  an ``(n_cand, d)`` matrix.  ``recount`` scatters the solution's rows into
+  ``cnt`` (:189-191), ``gain_map`` / ``loss_map`` count deficient
+  (``cnt < mu``) / critical (``1 <= cnt <= mu``) elements per candidate
+  (:193-197, roles :180-187), ``ball_update`` adds ``delta`` per incidence
+  (:200-201), ``ball_gather`` answers the role counts for listed
+  candidates, any other target being the literal ``cnt == target``
+  (:203-220);
+* ``WeightedIncidenceBackend`` (``incidence.py:301-419``): CSR rows with
+  per-incidence weights ``w >= 1`` and universe weights ``uw >= 1``; an
+  update adds ``delta * w``; the fields are the exact weighted marginals
+  (:374-384): gain ``uw * min(w, max(0, mu - cnt))``, loss
+  ``uw * (max(0, mu - cnt + w) - max(0, mu - cnt))`` where ``cnt >= w``,
+  other targets literal and unweighted; ``uncovered`` is
+  ``sum uw * max(0, mu - cnt)`` (:407-409);
+* the shared queries of ``DenseFieldBackend`` (``src/coldcore/protocol.py``):
+  ``count_eq`` literal over the universe, ``map_max`` (0 for an empty or
+  non-positive map), ``map_hist`` (positive v in bin
+  ``(v - 1) * nbins // vmax``, clipped to the last), ``map_extract``
+  (every candidate with ``map >= thr``, the true count even past the cap).
+
+Pinned against the reference's own backends by ``tests/golden/
+incidence_golden.npz`` (``tests/golden/make_incidence_golden.py``) and
+against the dict-of-lists brute force below.
+"""
+import numpy as np
+
+
+class IncidenceOracle:
+    """Dense (n_cand, d) incidence rows."""
+
+    def __init__(self, inc, n_univ, mu=1):
+        self.inc = np.ascontiguousarray(inc, dtype=np.int64)
+        self.n_cand, self.d = self.inc.shape
+        self.n_univ, self.mu = int(n_univ), int(mu)
+        self.cnt = np.zeros(self.n_univ, dtype=np.int64)
+        self.map = np.zeros(self.n_cand, dtype=np.int64)
+
+    # ---- roles (incidence.py:180-187)
+    def role(self, c, target):
+        if target == 0:
+            return c < self.mu
+        if target == 1:
+            return (c >= 1) & (c <= self.mu)
+        return c == target
+
+    def rows_of(self, idx):
+        return self.inc[np.asarray(idx, dtype=np.int64).ravel()]
+
+    def recount(self, idx):
+        self.cnt[:] = 0
+        self.ball_update(idx, 1)
+
+    def ball_update(self, idx, delta):
+        np.add.at(self.cnt, self.rows_of(idx).ravel(), int(delta))
+
+    def ball_gather(self, idx, target):
+        rows = self.rows_of(idx)
+        return self.role(self.cnt[rows], int(target)).sum(axis=1)
+
+    def field(self, target):
+        self.map[:] = self.ball_gather(np.arange(self.n_cand), target)
+
+    def gain_map(self):
+        self.field(0)
+
+    def loss_map(self):
+        self.field(1)
+
+    def uncovered(self):
+        return int(np.maximum(self.mu - self.cnt, 0).sum())
+
+    # ---- queries shared by both forms
+    def count_eq(self, target):
+        return int((self.cnt == target).sum())
+
+    def map_max(self):
+        return int(max(0, self.map.max(initial=0)))
+
+    def map_hist(self, nbins, vmax):
+        v = self.map[self.map > 0]
+        b = np.minimum((v - 1) * nbins // vmax, nbins - 1)
+        return np.bincount(b, minlength=nbins)[:nbins]
+
+    def map_extract(self, thr):
+        idx = np.flatnonzero(self.map >= thr)
+        return idx, self.map[idx], len(idx)
+
+
+class WeightedIncidenceOracle(IncidenceOracle):
+    """CSR rows with incidence weights w and universe weights uw."""
+
+    def __init__(self, indptr, indices, w, n_univ, uw=None, mu=1):
+        self.indptr = np.asarray(indptr, dtype=np.int64)
+        self.indices = np.asarray(indices, dtype=np.int64)
+        self.w = np.asarray(w, dtype=np.int64)
+        self.n_cand = len(self.indptr) - 1
+        self.n_univ, self.mu = int(n_univ), int(mu)
+        self.uw = (np.ones(self.n_univ, dtype=np.int64) if uw is None
+                   else np.asarray(uw, dtype=np.int64))
+        self.cnt = np.zeros(self.n_univ, dtype=np.int64)
+        self.map = np.zeros(self.n_cand, dtype=np.int64)
+
+    def _row(self, c):
+        s, e = self.indptr[c], self.indptr[c + 1]
+        return self.indices[s:e], self.w[s:e]
+
+    def ball_update(self, idx, delta):
+        for c in np.asarray(idx, dtype=np.int64).ravel():
+            u, w = self._row(int(c))
+            np.add.at(self.cnt, u, w * int(delta))
+
+    def values(self, u, w, target):
+        """Per-incidence contributions (incidence.py:374-384)."""
+        c = self.cnt[u]
+        if target == 0:
+            return self.uw[u] * np.minimum(w, np.maximum(0, self.mu - c))
+        if target == 1:
+            return (self.uw[u] * (np.maximum(0, self.mu - c + w)
+                                  - np.maximum(0, self.mu - c)) * (c >= w))
+        return (c == target).astype(np.int64)
+
+    def ball_gather(self, idx, target):
+        out = []
+        for c in np.asarray(idx, dtype=np.int64).ravel():
+            u, w = self._row(int(c))
+            out.append(int(self.values(u, w, int(target)).sum()))
+        return np.asarray(out, dtype=np.int64)
+
+    def uncovered(self):
+        return int((self.uw * np.maximum(self.mu - self.cnt, 0)).sum())
+
+
+def brute_cnt(rows, n_univ, sol):
+    """Multiplicities by explicit loops over the solution's rows."""
+    c = [0] * n_univ
+    for s in sol:
+        for u in rows[int(s)]:
+            c[int(u)] += 1
+    return np.asarray(c, dtype=np.int64)
+
+
+def brute_gather(rows, cnt, mu, cands, target):
+    """Role counts by explicit loops (incidence.py:180-187)."""
+    def role(c):
+        if target == 0:
+            return c < mu
+        if target == 1:
+            return 1 <= c <= mu
+        return c == target
+    return np.asarray([sum(role(int(cnt[int(u)])) for u in rows[int(w)])
+                       for w in cands], dtype=np.int64)

@@ -66,3 +66,18 @@ def cell_id(problem, axes, R, mu):
 
 def key(*parts):
     return "__".join(str(p) for p in parts)
+
+
+def incidence_golden():
+    """The reference's explicit-incidence backends on seeded cells
+    (make_incidence_golden.py)."""
+    if "incidence" not in _cache:
+        _cache["incidence"] = dict(np.load(os.path.join(
+            HERE, "incidence_golden.npz")))
+    return _cache["incidence"]
+
+
+def incidence_cells():
+    """Cell keys of incidence_golden(): dense*, design*, weighted*."""
+    keys = {k.split("/")[0] for k in incidence_golden()}
+    return sorted(keys)
