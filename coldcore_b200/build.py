@@ -15,6 +15,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(PKG, "libcoldcore_covering.so")
+SPARSE_LIB = os.path.join(PKG, "libcoldcore_sparse.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -58,7 +59,28 @@ def build(verbose=False, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_sparse(verbose, extra)
     return LIB
+
+
+def build_sparse(verbose=False, extra=()):
+    """The explicit-incidence engine (plugin ABI 2), its own library as in
+    the reference: ``csrc/sparse/*.cu`` -> ``libcoldcore_sparse.so``."""
+    os.makedirs(OBJ, exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "sparse", "*.cu")))
+    headers = [os.path.join(ROOT, "include", "coldcore_b200", "sparse.h")]
+    res = [_compile(s, headers, list(extra)) for s in srcs]
+    objs = [o for o, _ in res]
+    if verbose:
+        for _, log in res:
+            if log:
+                print(log)
+    if _newer(SPARSE_LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", SPARSE_LIB] + objs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return SPARSE_LIB
 
 
 if __name__ == "__main__":

@@ -1,0 +1,356 @@
+"""Explicit-incidence cells on the B200: the Python side of plugin ABI 2.
+
+Mirrors coldcore's ``src/coldcore/incidence_gpu.py`` (the ctypes binding of
+``sparse_*``) with the same classes, arguments, methods and errors, over
+this engine's ``libcoldcore_sparse.so``:
+
+* :class:`GpuIncidenceBackend` — dense rows, ``incidence_gpu.py:98-283``;
+* :class:`GpuWeightedIncidenceBackend` — weighted CSR rows,
+  ``incidence_gpu.py:286-360``;
+* :class:`IncidenceSpace` — the one-axis stand-in for a product space that
+  the search core reads (``src/coldcore/incidence.py:48-86``).
+
+Placement: ``cnt``, ``map`` and the query buffers are in HBM.  The
+incidence goes to HBM when the cell fits the budget (``hbm_budget``, else
+env ``COLDCORE_HBM_BUDGET``, default 160 GB of the B200's 180), else to
+managed memory that prefers the host (``inc_mode=1``; reported as 2).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .gpu import _check
+
+_libs = {}
+
+_LL = ctypes.c_longlong
+_I32P = ctypes.POINTER(ctypes.c_int32)
+_I64P = ctypes.POINTER(ctypes.c_int64)
+_LLP = ctypes.POINTER(_LL)
+
+PLUGIN_NAME = "libcoldcore_sparse.so"
+HBM_BUDGET = int(os.environ.get("COLDCORE_HBM_BUDGET", 160 * 10 ** 9))
+
+
+def _bind(path):
+    lib = ctypes.CDLL(path)
+    if not hasattr(lib, "sparse_init") or lib.sparse_abi_version() != 2:
+        raise RuntimeError(f"{path} is not a plugin of ABI 2")
+    I = ctypes.c_int
+    sig = {
+        "sparse_abi_version": (I, []),
+        "sparse_init": (I, [_LL, I, _LL, _I32P, I, I, _LLP, _LLP]),
+        "sparse_init_csr": (I, [_LL, _LL, _LL, _I64P, _I32P, _I32P, _I32P, I,
+                                I, _LLP, _LLP]),
+        "sparse_free": (I, []),
+        "sparse_set_mu": (I, [I]),
+        "sparse_get_mu": (I, []),
+        "sparse_inc_mode": (I, []),
+        "sparse_is_csr": (I, []),
+        "sparse_field": (I, [I]),
+        "sparse_recount": (I, [_LLP, _LL]),
+        "sparse_ball_update": (I, [_LLP, _LL, I]),
+        "sparse_ball_gather": (I, [_LLP, _LL, I, _I32P]),
+        "sparse_map_read_at": (I, [_LLP, _LL, _I32P]),
+        "sparse_read_cnt": (I, [_LL, _LL, _I32P]),
+        "sparse_map_max": (I, [_I32P]),
+        "sparse_map_hist": (I, [I, ctypes.c_int32, _I32P]),
+        "sparse_map_extract": (_LL, [ctypes.c_int32, _I64P, _I32P, I]),
+        "sparse_count_eq": (_LL, [I]),
+        "sparse_count_deficit": (_LL, []),
+        "sparse_dev_bytes": (_LL, []),
+        "sparse_host_bytes": (_LL, []),
+        "sparse_b200_stream": (_LL, []),
+        "sparse_b200_row_lanes": (I, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def default_sparse_plugin_path():
+    """``COLDCORE_SPARSE_PLUGIN_PATH`` if set, else the in-tree library."""
+    env = os.environ.get("COLDCORE_SPARSE_PLUGIN_PATH")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        PLUGIN_NAME)
+
+
+def load_sparse_plugin(path=None):
+    """Load (and cache) the ABI-2 library; raises when it is missing."""
+    path = os.path.abspath(path or default_sparse_plugin_path())
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"engine library not built: {path} "
+                "(run `python -m coldcore_b200.build`)")
+        _libs[path] = _bind(path)
+    return _libs[path]
+
+
+class IncidenceSpace:
+    """One axis of ``size`` candidates standing in for a product space: a
+    "word" is a one-digit row ``(idx,)`` (coldcore ``incidence.py:48-86``)."""
+
+    def __init__(self, size):
+        self.size = int(size)
+        if self.size < 1:
+            raise ValueError("IncidenceSpace needs at least one candidate")
+        self.n = 1
+        self.axes = [self.size]
+        self.q = self.size
+        self.pow_q = np.array([1], dtype=np.int64)
+
+    def word_index(self, words):
+        return np.asarray(words, dtype=np.int64).reshape(-1)
+
+    def index_word(self, idx):
+        return np.asarray(idx, dtype=np.int64).reshape(-1, 1)
+
+    def all_words(self):
+        return np.arange(self.size, dtype=np.int64)[:, None]
+
+    def __repr__(self):
+        return f"IncidenceSpace({self.size})"
+
+
+def _ll(name, r):
+    if r < 0:
+        raise RuntimeError(f"{name} rc={r}")
+    return int(r)
+
+
+class GpuIncidenceBackend:
+    """One dense explicit-incidence cell resident on the B200.
+
+    inc: (n_cand, d) integer array, entries in [0, n_univ), uploaded at
+    init; n_univ, mu, extract_cap as for coldcore's host backend;
+    inc_mode None | 0 | 1 (None: by size against the HBM budget)."""
+
+    indep_dist = None
+    supports_hist = True
+
+    def __init__(self, inc, n_univ, mu=1, extract_cap=1 << 22, inc_mode=None,
+                 plugin_path=None, hbm_budget=None):
+        inc = np.asarray(inc)
+        if inc.ndim != 2 or not np.issubdtype(inc.dtype, np.integer):
+            raise ValueError("inc must be a 2-D integer array (n_cand, d)")
+        self.n_univ = int(n_univ)
+        if not (1 <= self.n_univ <= np.iinfo(np.int32).max):
+            raise ValueError("n_univ must be in 1..2^31-1 (int32 indices)")
+        if inc.size and (int(inc.min()) < 0 or int(inc.max()) >= self.n_univ):
+            raise ValueError("incidence entries must lie in [0, n_univ)")
+        inc = np.ascontiguousarray(inc, dtype=np.int32)
+        self.n_cand, self.d = (int(x) for x in inc.shape)
+        self.mu = int(mu)
+        if self.mu < 1:
+            raise ValueError("mu must be >= 1")
+        self.space = IncidenceSpace(self.n_cand)
+        self.extract_cap = int(extract_cap)
+        budget = HBM_BUDGET if hbm_budget is None else int(hbm_budget)
+        inc_bytes = self.n_cand * self.d * 4
+        other = (self.n_cand + self.n_univ) * 4 + self.extract_cap * 12
+        if inc_mode is None:
+            inc_mode = 0 if inc_bytes + other <= budget else 1
+        if inc_mode not in (0, 1):
+            raise ValueError("inc_mode must be 0 (HBM) or 1 (pinned host)")
+        self._lib = lib = load_sparse_plugin(plugin_path)
+        bd, bh = _LL(0), _LL(0)
+        self._closed = True
+        _check("sparse_init", lib.sparse_init(
+            self.n_cand, self.d, self.n_univ, inc.ctypes.data_as(_I32P),
+            int(inc_mode), self.extract_cap, ctypes.byref(bd),
+            ctypes.byref(bh)))
+        self._closed = False
+        self._after_init(bd, bh)
+
+    def _after_init(self, bd, bh):
+        _check("sparse_set_mu", self._lib.sparse_set_mu(self.mu))
+        self.inc_mode = int(self._lib.sparse_inc_mode())
+        self.gpu_bytes = bd.value
+        self.host_bytes = bh.value
+
+    def close(self):
+        if not self._closed:
+            self._lib.sparse_free()
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _idx(idx):
+        return np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64).ravel()
+
+    # ---- fields
+    def recount(self, idx):
+        idx = self._idx(idx)
+        _check("sparse_recount", self._lib.sparse_recount(
+            idx.ctypes.data_as(_LLP), len(idx)))
+
+    def gain_map(self):
+        _check("sparse_field(gain)", self._lib.sparse_field(0))
+
+    def loss_map(self):
+        _check("sparse_field(loss)", self._lib.sparse_field(1))
+
+    # ---- incremental
+    def ball_update(self, idx, delta):
+        idx = self._idx(idx)
+        _check("sparse_ball_update", self._lib.sparse_ball_update(
+            idx.ctypes.data_as(_LLP), len(idx), int(delta)))
+
+    def ball_gather(self, idx, target):
+        """target is a coverage ROLE: 0 = deficient (cnt < mu), 1 =
+        critical (1 <= cnt <= mu), anything else = literal cnt == target."""
+        idx = self._idx(idx)
+        out = np.empty(len(idx), dtype=np.int32)
+        _check("sparse_ball_gather", self._lib.sparse_ball_gather(
+            idx.ctypes.data_as(_LLP), len(idx), int(target),
+            out.ctypes.data_as(_I32P)))
+        return out
+
+    # ---- queries
+    def count_eq(self, target):
+        return _ll("sparse_count_eq", self._lib.sparse_count_eq(int(target)))
+
+    def uncovered(self):
+        """Total deficit sum max(0, mu - cnt) (x uw when weighted)."""
+        return _ll("sparse_count_deficit", self._lib.sparse_count_deficit())
+
+    def map_max(self):
+        v = ctypes.c_int32(0)
+        _check("sparse_map_max", self._lib.sparse_map_max(ctypes.byref(v)))
+        return int(v.value)
+
+    def map_hist(self, nbins, vmax):
+        out = np.zeros(nbins, dtype=np.int32)
+        _check("sparse_map_hist", self._lib.sparse_map_hist(
+            int(nbins), int(vmax), out.ctypes.data_as(_I32P)))
+        return out
+
+    def map_extract(self, thr, cap=None):
+        cap = min(cap or self.extract_cap, self.extract_cap)
+        oi = np.empty(max(cap, 1), dtype=np.int64)
+        ov = np.empty(max(cap, 1), dtype=np.int32)
+        found = _ll("sparse_map_extract", self._lib.sparse_map_extract(
+            int(thr), oi.ctypes.data_as(_I64P), ov.ctypes.data_as(_I32P),
+            cap))
+        m = min(found, cap)
+        return oi[:m], ov[:m], found
+
+    def map_read_at(self, idx):
+        idx = self._idx(idx)
+        out = np.empty(len(idx), dtype=np.int32)
+        _check("sparse_map_read_at", self._lib.sparse_map_read_at(
+            idx.ctypes.data_as(_LLP), len(idx), out.ctypes.data_as(_I32P)))
+        return out
+
+    def map_all(self):
+        return self.map_read_at(np.arange(self.n_cand, dtype=np.int64))
+
+    def read_cnt(self, off=0, length=None):
+        """A range of cnt over the universe, clipped like a numpy slice."""
+        off = max(0, int(off))
+        hi = (self.n_univ if length is None
+              else min(self.n_univ, off + int(length)))
+        n = max(0, hi - off)
+        out = np.empty(n, dtype=np.int32)
+        if n:
+            _check("sparse_read_cnt", self._lib.sparse_read_cnt(
+                off, n, out.ctypes.data_as(_I32P)))
+        return out.astype(np.uint16)
+
+    def deficient_universe(self, limit, rng=None):
+        """Up to ``limit`` universe elements with cnt < mu (sorted, or a
+        random subset when ``rng`` is given)."""
+        cnt = np.empty(self.n_univ, dtype=np.int32)
+        _check("sparse_read_cnt", self._lib.sparse_read_cnt(
+            0, self.n_univ, cnt.ctypes.data_as(_I32P)))
+        u = np.flatnonzero(cnt < self.mu)
+        if rng is not None and len(u) > limit:
+            u = np.sort(rng.choice(u, size=int(limit), replace=False))
+        return u[:limit].astype(np.int64)
+
+    def verify(self, idx):
+        """Feasibility of ``idx`` from a fresh device recount (overwrites
+        cnt)."""
+        self.recount(idx)
+        return self.uncovered() == 0
+
+    def __repr__(self):
+        return (f"{type(self).__name__}(n_cand={self.n_cand}, d={self.d}, "
+                f"n_univ={self.n_univ}, mu={self.mu}, "
+                f"inc_mode={getattr(self, 'inc_mode', None)})")
+
+
+class GpuWeightedIncidenceBackend(GpuIncidenceBackend):
+    """A weighted CSR cell (coldcore ``WeightedIncidenceBackend`` on the
+    GPU): the exact weighted marginals, ``uncovered`` the weighted
+    deficiency."""
+
+    def __init__(self, indptr, indices, w, n_univ, uw=None, mu=1,
+                 extract_cap=1 << 22, inc_mode=None, plugin_path=None,
+                 hbm_budget=None):
+        indptr = np.ascontiguousarray(indptr, dtype=np.int64).ravel()
+        indices = np.ascontiguousarray(indices, dtype=np.int32).ravel()
+        w = np.ascontiguousarray(w, dtype=np.int32).ravel()
+        self.n_univ = int(n_univ)
+        if not (1 <= self.n_univ <= np.iinfo(np.int32).max):
+            raise ValueError("n_univ must be in 1..2^31-1 (int32 indices)")
+        if len(indptr) < 2 or indptr[0] != 0 or indptr[-1] != len(indices) or (
+                np.diff(indptr) < 0).any():
+            raise ValueError("indptr is not a valid CSR offset array")
+        if len(w) != len(indices) or (w < 1).any():
+            raise ValueError("w must match indices and be >= 1")
+        if indices.size and (int(indices.min()) < 0
+                             or int(indices.max()) >= self.n_univ):
+            raise ValueError("indices must lie in [0, n_univ)")
+        uw = (np.ones(self.n_univ, dtype=np.int32) if uw is None
+              else np.ascontiguousarray(uw, dtype=np.int32).ravel())
+        if len(uw) != self.n_univ or (uw < 1).any():
+            raise ValueError("uw must have n_univ entries >= 1")
+        self.n_cand = len(indptr) - 1
+        self.nnz = len(indices)
+        self.d = None
+        self.row_len = np.diff(indptr)
+        self.mu = int(mu)
+        if self.mu < 1:
+            raise ValueError("mu must be >= 1")
+        self.space = IncidenceSpace(self.n_cand)
+        self.extract_cap = int(extract_cap)
+        budget = HBM_BUDGET if hbm_budget is None else int(hbm_budget)
+        inc_bytes = self.nnz * 8 + (self.n_cand + 1) * 8
+        other = (self.n_cand + 2 * self.n_univ) * 4 + self.extract_cap * 12
+        if inc_mode is None:
+            inc_mode = 0 if inc_bytes + other <= budget else 1
+        if inc_mode not in (0, 1):
+            raise ValueError("inc_mode must be 0 (HBM) or 1 (pinned host)")
+        self._lib = lib = load_sparse_plugin(plugin_path)
+        bd, bh = _LL(0), _LL(0)
+        self._closed = True
+        _check("sparse_init_csr", lib.sparse_init_csr(
+            self.n_cand, self.n_univ, self.nnz, indptr.ctypes.data_as(_I64P),
+            indices.ctypes.data_as(_I32P), w.ctypes.data_as(_I32P),
+            uw.ctypes.data_as(_I32P), int(inc_mode), self.extract_cap,
+            ctypes.byref(bd), ctypes.byref(bh)))
+        self._closed = False
+        self._after_init(bd, bh)
+
+    def __repr__(self):
+        return (f"{type(self).__name__}(n_cand={self.n_cand}, nnz={self.nnz}, "
+                f"n_univ={self.n_univ}, mu={self.mu}, "
+                f"inc_mode={getattr(self, 'inc_mode', None)})")

@@ -1,0 +1,138 @@
+"""The explicit-incidence engine (plugin ABI 2) on the B200 against the
+reference's own backends (golden fixtures from ``make_incidence_golden.py``)
+and the oracle: every field, gather, update and query, dense and weighted
+CSR cells, both placements.  Integer work: bit-exact."""
+import numpy as np
+import pytest
+
+from coldcore_b200.incidence import (GpuIncidenceBackend,
+                                     GpuWeightedIncidenceBackend)
+from golden_data import incidence_cells, incidence_golden
+from oracle.incidence_oracle import IncidenceOracle, WeightedIncidenceOracle
+
+pytestmark = pytest.mark.gpu
+
+
+def open_cell(g, key, inc_mode, cap=16):
+    meta = g[key + "/meta"]
+    n_univ, mu = int(meta[0]), int(meta[1])
+    if key.startswith("weighted"):
+        args = (g[key + "/indptr"], g[key + "/indices"], g[key + "/w"], n_univ)
+        return (GpuWeightedIncidenceBackend(*args, uw=g[key + "/uw"], mu=mu,
+                                            extract_cap=cap,
+                                            inc_mode=inc_mode),
+                WeightedIncidenceOracle(*args, uw=g[key + "/uw"], mu=mu))
+    return (GpuIncidenceBackend(g[key + "/inc"], n_univ, mu=mu,
+                                extract_cap=cap, inc_mode=inc_mode),
+            IncidenceOracle(g[key + "/inc"], n_univ, mu=mu))
+
+
+@pytest.mark.parametrize("inc_mode", [0, 1])
+@pytest.mark.parametrize("key", incidence_cells())
+def test_engine_reproduces_the_reference(key, inc_mode):
+    g = incidence_golden()
+    cap = 16
+    b, o = open_cell(g, key, inc_mode, cap)
+    with b:
+        assert b.inc_mode in (0, 2) and b.space.size == o.n_cand
+        assert b.inc_mode == (0 if inc_mode == 0 else 2)
+        for r in range(3):
+            p = f"{key}/{r}/"
+            sol = g[p + "sol"]
+            b.recount(sol)
+            o.recount(sol)
+            assert np.array_equal(b.read_cnt(), g[p + "cnt"].astype(np.uint16))
+            assert b.uncovered() == int(g[p + "uncovered"])
+            assert [b.count_eq(t) for t in range(4)] == \
+                g[p + "count_eq"].tolist()
+            n_univ = o.n_univ
+            assert np.array_equal(b.read_cnt(2, 6), o.cnt[2:8])
+            assert np.array_equal(b.read_cnt(n_univ - 2, 9), o.cnt[n_univ - 2:])
+            assert len(b.read_cnt(n_univ + 3, 2)) == 0
+            every = np.arange(o.n_cand)
+            for fld in ("gain", "loss"):
+                getattr(b, fld + "_map")()
+                getattr(o, fld + "_map")()
+                assert np.array_equal(b.map_read_at(every), g[p + fld])
+                assert np.array_equal(b.map_all(), o.map)
+                assert b.map_max() == o.map_max()
+                mx = max(1, o.map_max())
+                for nbins in (1, 7, 1024):
+                    assert np.array_equal(b.map_hist(nbins, mx),
+                                          o.map_hist(nbins, mx))
+                for thr in (0, 1, mx // 2, mx):
+                    want, _, found = o.map_extract(thr)
+                    gi, gv, gf = b.map_extract(thr)
+                    assert gf == found and len(gi) == min(found, cap)
+                    assert np.array_equal(o.map[gi], gv)
+                    if found <= cap:
+                        assert sorted(gi.tolist()) == want.tolist()
+            for t in (0, 1, 2, 5):
+                assert np.array_equal(b.ball_gather(g[p + "probe"], t),
+                                      g[p + f"gather{t}"])
+            assert b.ball_gather(g[p + "probe"][:0], 0).shape == (0,)
+            b.ball_update(g[p + "add"], +1)
+            b.ball_update(g[p + "add"][:3], -1)
+            o.ball_update(g[p + "add"], +1)
+            o.ball_update(g[p + "add"][:3], -1)
+            assert np.array_equal(b.read_cnt(), g[p + "upd_cnt"].astype(
+                np.uint16))
+            o.recount(sol)
+            assert b.verify(sol) == (o.uncovered() == 0)
+
+
+def test_bad_candidates_are_rejected_before_any_change():
+    g = incidence_golden()
+    b, o = open_cell(g, "design1", 0)
+    with b:
+        sol = g["design1/0/sol"]
+        b.recount(sol)
+        before = b.read_cnt().copy()
+        for bad in ([0, o.n_cand], [-1], [5, 2 ** 40]):
+            with pytest.raises(RuntimeError):
+                b.ball_update(bad, +1)
+            with pytest.raises(RuntimeError):
+                b.ball_gather(bad, 0)
+            with pytest.raises(RuntimeError):
+                b.map_read_at(bad)
+            with pytest.raises(RuntimeError):
+                b.recount(bad)
+        assert np.array_equal(b.read_cnt(), before)
+        b.recount([])
+        assert b.uncovered() == o.n_univ * int(g["design1/meta"][1])
+
+
+def test_row_lanes_follow_the_row_length():
+    from coldcore_b200.incidence import load_sparse_plugin
+    lib = load_sparse_plugin()
+    for d, lanes in ((1, 1), (3, 4), (6, 8), (10, 16), (33, 32)):
+        rng = np.random.default_rng(d)
+        inc = np.stack([rng.choice(64, d, replace=False) for _ in range(50)])
+        with GpuIncidenceBackend(inc, 64):
+            assert lib.sparse_b200_row_lanes() == lanes
+
+
+def test_covering_design_fields_against_the_oracle():
+    """C(16,6,3): 8,008 blocks x 20 triples over 560 triples, mu = 2."""
+    from itertools import combinations
+    from math import comb
+    v, k, t = 16, 6, 3
+    blocks = list(combinations(range(v), k))
+    # colex rank of a sorted t-subset: sum C(s_j, j + 1)
+    inc = np.array([[sum(comb(s[j], j + 1) for j in range(t))
+                     for s in combinations(b, t)] for b in blocks],
+                   dtype=np.int32)
+    n_univ = comb(v, t)
+    rng = np.random.default_rng(16)
+    o = IncidenceOracle(inc, n_univ, mu=2)
+    with GpuIncidenceBackend(inc, n_univ, mu=2) as b:
+        for M in (0, 40, 400):
+            sol = rng.choice(len(blocks), M, replace=False)
+            b.recount(sol)
+            o.recount(sol)
+            assert np.array_equal(b.read_cnt().astype(np.int64), o.cnt)
+            assert b.uncovered() == o.uncovered()
+            for fld in ("gain_map", "loss_map"):
+                getattr(b, fld)()
+                getattr(o, fld)()
+                assert np.array_equal(b.map_all(), o.map)
