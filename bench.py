@@ -541,6 +541,14 @@ def run_b200(args, dist):
         line["same_cells"] = same
     if not args.no_batch:
         line["batched"] = measure_batch(args, dist)
+    if not args.no_incidence and dist.world == 1:
+        # the explicit-incidence engine (plugin ABI 2) on a covering design;
+        # a failure here is reported in its own object, not the line's
+        try:
+            from coldcore_b200.incidence_bench import measure as inc_measure
+            line["incidence"] = inc_measure()
+        except Exception as e:           # noqa: BLE001
+            line["incidence"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_lns and dist.world == 1:
         line["lns"] = measure_lns(args)
     print(json.dumps(line), flush=True)
@@ -555,6 +563,7 @@ def main():
     ap.add_argument("--cell", default=HEADLINE, choices=sorted(CELLS))
     ap.add_argument("--no-also", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-incidence", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-lns", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")

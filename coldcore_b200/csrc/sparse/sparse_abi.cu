@@ -25,7 +25,9 @@
 #include <climits>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -72,9 +74,17 @@ Cell C;
 cudaStream_t g_s = nullptr;
 int g_mu = 1;                      // kept across cells like the reference's
 
+// CTAs for `threads` threads, at most CC_SPARSE_BLOCKS_PER_SM per SM
+// (default 32: four waves of resident 256-thread CTAs, which ran the
+// C(30,8,4) field 12% faster than one wave); every kernel strides its loop
+// over the grid, so any grid covers all the work
 int grid_for(long long threads) {
   long long b = (threads + kThreads - 1) / kThreads;
-  const long long cap = (long long)C.sms * (2048 / kThreads);
+  const char *e = getenv("CC_SPARSE_BLOCKS_PER_SM");
+  long long per = e ? atoll(e) : 32;
+  if (per < 1) per = 1;
+  if (per > 64) per = 64;
+  const long long cap = (long long)C.sms * per;
   if (b > cap) b = cap;
   return (int)(b < 1 ? 1 : b);
 }
@@ -114,11 +124,14 @@ __device__ __forceinline__ long long wval(int c, int w, int u, int target,
 
 // Row sums over candidates i < m (row words[i], or i itself when words is
 // null) into out[i]: L lanes per row, 32 / L rows per warp.  The group loop
-// is uniform across the warp, so every lane reaches the shuffles.
+// is uniform across the warp, so every lane reaches the shuffles.  L is a
+// compile-time stride, so a lane's loads of its row entries (and then of
+// their counters) issue together instead of one dependent pair at a time.
+template <int L>
 __global__ void k_rows_dense(const int32_t *__restrict__ inc, int d,
                              const int32_t *__restrict__ cnt,
                              const long long *__restrict__ words, long long m,
-                             int target, int mu, int L,
+                             int target, int mu,
                              int32_t *__restrict__ out) {
   const int lane = threadIdx.x & 31, seg = lane / L, sl = lane % L;
   const int P = 32 / L;
@@ -132,6 +145,7 @@ __global__ void k_rows_dense(const int32_t *__restrict__ inc, int d,
     if (i < m) {
       const long long r = words ? words[i] : i;
       const int32_t *row = inc + r * d;
+#pragma unroll 4
       for (int j = sl; j < d; j += L) s += role(cnt[row[j]], target, mu);
     }
     for (int o = L >> 1; o > 0; o >>= 1)
@@ -140,13 +154,14 @@ __global__ void k_rows_dense(const int32_t *__restrict__ inc, int d,
   }
 }
 
+template <int L>
 __global__ void k_rows_csr(const int64_t *__restrict__ indptr,
                            const int32_t *__restrict__ indices,
                            const int32_t *__restrict__ w,
                            const int32_t *__restrict__ uw,
                            const int32_t *__restrict__ cnt,
                            const long long *__restrict__ words, long long m,
-                           int target, int mu, int L,
+                           int target, int mu,
                            int32_t *__restrict__ out) {
   const int lane = threadIdx.x & 31, seg = lane / L, sl = lane % L;
   const int P = 32 / L;
@@ -160,6 +175,7 @@ __global__ void k_rows_csr(const int64_t *__restrict__ indptr,
     if (i < m) {
       const long long r = words ? words[i] : i;
       const long long e = indptr[r + 1];
+#pragma unroll 4
       for (long long j = indptr[r] + sl; j < e; j += L) {
         const int u = indices[j];
         s += wval(cnt[u], w[j], uw[u], target, mu);
@@ -394,12 +410,21 @@ int launch_rows(const long long *words, long long m, int target,
                 int32_t *out) {
   const int L = C.lanes, P = 32 / L;
   const int grid = grid_for((m + P - 1) / P * 32);
-  if (C.csr)
-    k_rows_csr<<<grid, kThreads, 0, g_s>>>(C.indptr, C.inc, C.w, C.uw, C.cnt,
-                                           words, m, target, g_mu, L, out);
-  else
-    k_rows_dense<<<grid, kThreads, 0, g_s>>>(C.inc, C.d, C.cnt, words, m,
-                                             target, g_mu, L, out);
+#define CC_ROWS(LL)                                                         \
+  case LL:                                                                  \
+    if (C.csr)                                                              \
+      k_rows_csr<LL><<<grid, kThreads, 0, g_s>>>(                           \
+          C.indptr, C.inc, C.w, C.uw, C.cnt, words, m, target, g_mu, out);  \
+    else                                                                    \
+      k_rows_dense<LL><<<grid, kThreads, 0, g_s>>>(                         \
+          C.inc, C.d, C.cnt, words, m, target, g_mu, out);                  \
+    break;
+  switch (L) {
+    CC_ROWS(1) CC_ROWS(2) CC_ROWS(4) CC_ROWS(8) CC_ROWS(16) CC_ROWS(32)
+    default:
+      return -2;                     // lanes_for gives powers of two <= 32
+  }
+#undef CC_ROWS
   SK(cudaGetLastError());
   return 0;
 }
@@ -427,6 +452,47 @@ long long read_acc() {
   SK(cudaMemcpyAsync(&v, C.acc, 8, cudaMemcpyDeviceToHost, g_s));
   SK(cudaStreamSynchronize(g_s));
   return (long long)v;
+}
+
+// ------------------------------------------------- covering designs
+// C(v,k,t) rows built on the device, in the reference's layout
+// (coldcore src/coldcore/problems/covering_design.py:95-135): candidate c is
+// the k-subset of colex rank c (s_0 < ... < s_{k-1}, c = sum C(s_j, j+1));
+// its row lists, for the t-subsets of block POSITIONS in lex order (pos,
+// d x t), the colex rank sum_j C(s[pos_j], j+1) of that t-subset.
+constexpr int kDesignMaxV = 128, kDesignMaxK = 32;
+constexpr long long kBinomSat = 1LL << 62;   // binomials saturate here
+
+__global__ void k_design_rows(int v, int k, int t, long long ncand, int d,
+                              const unsigned char *__restrict__ pos,
+                              const long long *__restrict__ binom,
+                              int32_t *inc) {
+  extern __shared__ long long B[];            // (v + 1) x (k + 1)
+  const int K1 = k + 1, nb = (v + 1) * K1;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) B[i] = binom[i];
+  __syncthreads();
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       c < ncand; c += gs) {
+    int s[kDesignMaxK];
+    long long rem = c;
+    int a = v - 1;
+    for (int j = k - 1; j >= 0; j--) {
+      // the largest a with C(a, j+1) <= rem; C(j, j+1) = 0 stops the walk
+      // at a = j at the latest, and every later a lies below this one
+      while (B[a * K1 + j + 1] > rem) a--;
+      s[j] = a;
+      rem -= B[a * K1 + j + 1];
+      a--;
+    }
+    int32_t *row = inc + c * d;
+    for (int col = 0; col < d; col++) {
+      const unsigned char *p = pos + (long long)col * t;
+      long long r = 0;
+      for (int j = 0; j < t; j++) r += B[s[p[j]] * K1 + j + 1];
+      row[col] = (int32_t)r;
+    }
+  }
 }
 
 }  // namespace
@@ -511,6 +577,93 @@ int sparse_init_csr(long long n_cand, long long n_univ, long long nnz,
   if ((rc = alloc_fields(extract_cap))) { free_all(); return rc; }
   if (bytes_dev) *bytes_dev = C.dev_bytes;
   if (bytes_host) *bytes_host = C.host_bytes;
+  return 0;
+}
+
+int sparse_b200_init_design(int v, int k, int t, int inc_mode,
+                            int extract_cap, long long *bytes_dev,
+                            long long *bytes_host) {
+  if (C.live) return -1;
+  if (v < 1 || v > kDesignMaxV || k < 1 || k > v || k > kDesignMaxK ||
+      t < 1 || t > k || inc_mode < 0 || inc_mode > 1 || extract_cap < 1)
+    return -2;
+  const int K1 = k + 1;
+  std::vector<long long> B((size_t)(v + 1) * K1, 0);
+  for (int a = 0; a <= v; a++) {
+    B[(size_t)a * K1] = 1;
+    for (int b = 1; b <= k && b <= a; b++) {
+      const long long x = B[(size_t)(a - 1) * K1 + b - 1] +
+                          B[(size_t)(a - 1) * K1 + b];
+      B[(size_t)a * K1 + b] = x > kBinomSat ? kBinomSat : x;
+    }
+  }
+  const long long ncand = B[(size_t)v * K1 + k];
+  const long long dd = B[(size_t)k * K1 + t];
+  const long long nuniv = B[(size_t)v * K1 + t];
+  if (ncand >= kBinomSat || nuniv > INT_MAX || dd > (1 << 20)) return -2;
+  if (ncand > LLONG_MAX / 4 / dd) return -2;
+  const int d = (int)dd;
+  // the t-subsets of block positions 0..k-1, lex order
+  std::vector<unsigned char> pos((size_t)d * t);
+  std::vector<int> p(t);
+  for (int j = 0; j < t; j++) p[j] = j;
+  for (int col = 0; col < d; col++) {
+    for (int j = 0; j < t; j++) pos[(size_t)col * t + j] = (unsigned char)p[j];
+    int j = t - 1;
+    while (j >= 0 && p[j] == k - t + j) j--;
+    if (j < 0) break;
+    p[j]++;
+    for (int i = j + 1; i < t; i++) p[i] = p[i - 1] + 1;
+  }
+  int rc = begin_cell(ncand, nuniv, inc_mode);
+  if (rc) { free_all(); return rc; }
+  C.d = d;
+  C.lanes = lanes_for(d);
+  long long *dB = nullptr;
+  unsigned char *dpos = nullptr;
+  cudaError_t e = cudaSuccess;
+  if ((rc = alloc_inc((void **)&C.inc, (size_t)ncand * d * 4, inc_mode,
+                      nullptr)))
+    goto fail;
+  e = cudaMalloc((void **)&dB, B.size() * 8);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&dpos, pos.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dB, B.data(), B.size() * 8, cudaMemcpyHostToDevice,
+                        g_s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dpos, pos.data(), pos.size(), cudaMemcpyHostToDevice,
+                        g_s);
+  if (e == cudaSuccess) {
+    k_design_rows<<<grid_for(ncand), kThreads, B.size() * 8, g_s>>>(
+        v, k, t, ncand, d, dpos, dB, C.inc);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_s);
+  if (dB) cudaFree(dB);
+  if (dpos) cudaFree(dpos);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "coldcore_b200 sparse: design build: %s\n",
+            cudaGetErrorString(e));
+    rc = -(100 + (int)e);
+    goto fail;
+  }
+  if ((rc = alloc_fields(extract_cap))) goto fail;
+  if (bytes_dev) *bytes_dev = C.dev_bytes;
+  if (bytes_host) *bytes_host = C.host_bytes;
+  return 0;
+fail:
+  free_all();
+  return rc;
+}
+
+int sparse_b200_read_rows(long long c0, long long n, int32_t *out) {
+  if (!C.live) return -1;
+  if (C.csr || c0 < 0 || n < 0 || c0 + n > C.ncand) return -2;
+  if (n == 0) return 0;
+  if (!out) return -2;
+  SK(cudaMemcpyAsync(out, C.inc + c0 * C.d, (size_t)n * C.d * 4,
+                     cudaMemcpyDeviceToHost, g_s));
+  SK(cudaStreamSynchronize(g_s));
   return 0;
 }
 

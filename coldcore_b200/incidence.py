@@ -63,8 +63,14 @@ def _bind(path):
         "sparse_host_bytes": (_LL, []),
         "sparse_b200_stream": (_LL, []),
         "sparse_b200_row_lanes": (I, []),
+        "sparse_b200_init_design": (I, [I, I, I, I, I, _LLP, _LLP]),
+        "sparse_b200_read_rows": (I, [_LL, _LL, _I32P]),
     }
     for name, (res, args) in sig.items():
+        if not hasattr(lib, name):
+            if name.startswith("sparse_b200_"):
+                continue                # this engine's additions only
+            raise RuntimeError(f"{path} lacks {name}")
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
@@ -354,3 +360,52 @@ class GpuWeightedIncidenceBackend(GpuIncidenceBackend):
         return (f"{type(self).__name__}(n_cand={self.n_cand}, nnz={self.nnz}, "
                 f"n_univ={self.n_univ}, mu={self.mu}, "
                 f"inc_mode={getattr(self, 'inc_mode', None)})")
+
+
+class GpuCoveringDesignBackend(GpuIncidenceBackend):
+    """A covering design C(v,k,t) (mu-fold) whose incidence is built on the
+    B200 (``sparse_b200_init_design``), in the layout of coldcore's
+    ``problems.covering_design.build_incidence``: candidates are the
+    k-subsets of {0..v-1} by colex rank, universe elements the t-subsets,
+    row c the ranks of block c's t-subsets.  The host never holds the
+    C(v,k) x C(k,t) matrix."""
+
+    def __init__(self, v, k, t, mu=1, extract_cap=1 << 22, inc_mode=0,
+                 plugin_path=None):
+        from math import comb
+        self.v, self.k, self.t = int(v), int(k), int(t)
+        if not (1 <= self.t <= self.k <= self.v):
+            raise ValueError("need 1 <= t <= k <= v")
+        self.mu = int(mu)
+        if self.mu < 1:
+            raise ValueError("mu must be >= 1")
+        if inc_mode not in (0, 1):
+            raise ValueError("inc_mode must be 0 (HBM) or 1 (pinned host)")
+        self.n_cand = comb(self.v, self.k)
+        self.d = comb(self.k, self.t)
+        self.n_univ = comb(self.v, self.t)
+        self.space = IncidenceSpace(self.n_cand)
+        self.extract_cap = int(extract_cap)
+        self._lib = lib = load_sparse_plugin(plugin_path)
+        if not hasattr(lib, "sparse_b200_init_design"):
+            raise RuntimeError("the loaded ABI-2 library builds no designs")
+        bd, bh = _LL(0), _LL(0)
+        self._closed = True
+        _check("sparse_b200_init_design", lib.sparse_b200_init_design(
+            self.v, self.k, self.t, int(inc_mode), self.extract_cap,
+            ctypes.byref(bd), ctypes.byref(bh)))
+        self._closed = False
+        self._after_init(bd, bh)
+
+    def rows(self, c0=0, n=None):
+        """Incidence rows [c0, c0 + n) as an (n, d) int32 array."""
+        n = self.n_cand - c0 if n is None else int(n)
+        out = np.empty((n, self.d), dtype=np.int32)
+        _check("sparse_b200_read_rows", self._lib.sparse_b200_read_rows(
+            int(c0), n, out.ctypes.data_as(_I32P)))
+        return out
+
+    def __repr__(self):
+        return (f"{type(self).__name__}(C({self.v},{self.k},{self.t}), "
+                f"mu={self.mu}, n_cand={self.n_cand}, d={self.d}, "
+                f"n_univ={self.n_univ})")

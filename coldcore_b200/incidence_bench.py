@@ -1,0 +1,127 @@
+"""Field throughput of the explicit-incidence engine on a covering design.
+
+One step = a gain field and a loss field over every candidate of C(v,k,t)
+(default C(30,8,4): 5,852,925 blocks x 70 triples, a 1.64 GB incidence,
+27,405 universe elements) after a recount of a seeded solution, the
+incidence built on the device.  Reported per field: milliseconds, and GB/s
+of its algorithmic bytes (the incidence read once, the map written once,
+cnt read once), with the reference's own ABI-2 kernels
+(``oracle/_ref/libref_sparse.so``, built from ``src/plugins/sparse/
+sparse.cu``) on the same incidence when that library is present.
+
+    python -m coldcore_b200.incidence_bench [--v 30 --k 8 --t 4 --reps 20]
+"""
+import argparse
+import json
+import os
+import statistics
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "libref_sparse.so")
+
+
+def _warm(b, seconds=0.3):
+    """Fields until `seconds` have passed: clocks settle before timing."""
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        b.gain_map()
+        b.loss_map()
+
+
+def _time_fields(b, stream, reps):
+    """Mean ms of gain + loss fields, CUDA events on `stream`."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        b.gain_map()
+        b.loss_map()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / (2 * reps)
+
+
+def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True):
+    """Both cells stay resident and are timed in alternation, `rounds`
+    times each after a warm-up; the medians are reported."""
+    import torch
+
+    from .incidence import GpuCoveringDesignBackend, GpuIncidenceBackend
+    rng = np.random.default_rng(v * 100 + k * 10 + t)
+    out = {"design": f"C({v},{k},{t})"}
+    with GpuCoveringDesignBackend(v, k, t) as b:
+        n_cand, d, n_univ = b.n_cand, b.d, b.n_univ
+        sol = rng.choice(n_cand, max(1, n_cand // 2000), replace=False)
+        b.recount(sol)
+        stream = torch.cuda.ExternalStream(int(b._lib.sparse_b200_stream()))
+        ref = None
+        if with_ref and os.path.exists(REF):
+            ref = GpuIncidenceBackend(b.rows(), n_univ, plugin_path=REF)
+        try:
+            if ref is not None:
+                ref.recount(sol)
+                _warm(ref)
+            _warm(b)
+            ours, theirs = [], []
+            for _ in range(rounds):
+                ours.append(_time_fields(b, stream, reps))
+                if ref is not None:
+                    theirs.append(_time_fields(ref, torch.cuda.default_stream(),
+                                               reps))
+            # the same engine with one CTA wave per SM instead of four
+            os.environ["CC_SPARSE_BLOCKS_PER_SM"] = "8"
+            try:
+                _warm(b, 0.1)
+                wide = [_time_fields(b, stream, reps) for _ in range(rounds)]
+            finally:
+                os.environ.pop("CC_SPARSE_BLOCKS_PER_SM", None)
+            b.gain_map()
+            sample = np.arange(0, n_cand, 997)
+            gain = b.map_read_at(sample)
+            same = None
+            if ref is not None:
+                ref.gain_map()
+                same = bool(np.array_equal(ref.map_read_at(sample), gain))
+        finally:
+            if ref is not None:
+                ref.close()
+    ms = statistics.median(ours)
+    by = n_cand * (d + 1) * 4 + n_univ * 4
+    out.update({"n_cand": n_cand, "d": d, "n_univ": n_univ,
+                "incidence_gb": round(n_cand * d * 4 / 1e9, 3),
+                "solution": len(sol), "ms_per_field": round(ms, 4),
+                "ms_rounds": [round(x, 4) for x in ours],
+                "ms_rounds_8_ctas_per_sm": [round(x, 4) for x in wide],
+                "GBps": round(by / (ms * 1e-3) / 1e9, 1),
+                "algorithmic_bytes_per_field": by})
+    if theirs:
+        rms = statistics.median(theirs)
+        out["reference_plugin"] = {
+            "library": "oracle/_ref/libref_sparse.so (reference "
+                       "src/plugins/sparse/sparse.cu, nvcc -O3 sm_100a)",
+            "ms_per_field": round(rms, 4),
+            "ms_rounds": [round(x, 4) for x in theirs],
+            "GBps": round(by / (rms * 1e-3) / 1e9, 1),
+            "same_gain_sample": same,
+            "speedup": round(rms / ms, 2)}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--v", type=int, default=30)
+    ap.add_argument("--k", type=int, default=8)
+    ap.add_argument("--t", type=int, default=4)
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--no-ref", action="store_true")
+    a = ap.parse_args()
+    print(json.dumps(measure(a.v, a.k, a.t, a.reps, with_ref=not a.no_ref)))
+
+
+if __name__ == "__main__":
+    main()

@@ -114,6 +114,21 @@ CCS_API long long sparse_b200_stream(void);
  * update kernels (a power of two <= 32, chosen from the row length) */
 CCS_API int       sparse_b200_row_lanes(void);
 
+/* a covering-design cell C(v,k,t) whose rows are built on the device
+ * (v <= 128, k <= 32, C(v,t) < 2^31, C(k,t) <= 2^20), in the layout of
+ * coldcore's build_incidence (src/coldcore/problems/covering_design.py:
+ * 95-135): candidate c = the k-subset of colex rank c, universe element u =
+ * the t-subset of colex rank u, row c = the ranks of its t-subsets, block
+ * positions in lex order.  Saves building and uploading C(v,k) x C(k,t)
+ * entries on the host. */
+CCS_API int       sparse_b200_init_design(int v, int k, int t, int inc_mode,
+                                          int extract_cap,
+                                          long long *bytes_dev,
+                                          long long *bytes_host);
+/* rows [c0, c0+n) of a dense cell, n x d int32 */
+CCS_API int       sparse_b200_read_rows(long long c0, long long n,
+                                        int32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

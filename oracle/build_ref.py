@@ -1,6 +1,6 @@
 #!/usr/bin/env python3
-"""Build the reference's own covering plugin for sm_100a (test and
-comparison infrastructure only).
+"""Build the reference's own plugins for sm_100a (test and comparison
+infrastructure only).
 
 The reference's ABI-v1 plugin is one CUDA translation unit,
 ``src/plugins/covering/dct_hc.cu`` (with the ``dctcore_*.cuh`` headers
@@ -12,9 +12,13 @@ the reference's CMake build), into ``oracle/_ref/libref_covering.so``:
 The library exports the same ``dct_*`` symbols as this engine, so the GPU
 tests can pin the engine's fields against the reference's own kernels on
 the same B200, and ``bench.py`` can time the reference's kernels on the
-cells they accept (axes <= 16, n <= 16, <= 65,535 occurrences).  Nothing
-here is linked into the engine; the reference source stays outside the
-repository, and the built library is git-ignored.
+cells they accept (axes <= 16, n <= 16, <= 65,535 occurrences).
+
+Likewise the ABI-2 plugin, ``src/plugins/sparse/sparse.cu`` (one file),
+becomes ``oracle/_ref/libref_sparse.so`` (``build_sparse``), the
+reference side of the explicit-incidence comparison.  Nothing here is
+linked into the engine; the reference source stays outside the
+repository, and the built libraries are git-ignored.
 """
 import os
 import subprocess
@@ -23,6 +27,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT = os.path.join(OUT_DIR, "libref_covering.so")
+SPARSE_OUT = os.path.join(OUT_DIR, "libref_sparse.so")
 REF_SRC = os.environ.get("COLDCORE_REF_SRC", "/root/reference/src")
 
 
@@ -46,5 +51,24 @@ def build(force=False):
     return OUT
 
 
+def build_sparse(force=False):
+    src = os.path.join(REF_SRC, "plugins", "sparse", "sparse.cu")
+    if not os.path.exists(src):
+        if os.path.exists(SPARSE_OUT):
+            return SPARSE_OUT
+        raise FileNotFoundError(src)
+    if os.path.exists(SPARSE_OUT) and not force and \
+            os.path.getmtime(SPARSE_OUT) >= os.path.getmtime(src):
+        return SPARSE_OUT
+    os.makedirs(OUT_DIR, exist_ok=True)
+    cmd = ["nvcc", "-O3", "-std=c++17",
+           "-gencode", "arch=compute_100a,code=sm_100a",
+           "-shared", "-Xcompiler", "-fPIC", src, "-o", SPARSE_OUT + ".tmp"]
+    subprocess.run(cmd, check=True)
+    os.replace(SPARSE_OUT + ".tmp", SPARSE_OUT)
+    return SPARSE_OUT
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv))
+    print(build_sparse(force="--force" in sys.argv))

@@ -1,7 +1,7 @@
 """CPU restatement of coldcore's explicit-incidence backends (plugin ABI 2).
 
 Test infrastructure only: the checker of the ABI-2 engine
-(``coldcore_b200/csrc/sparse_abi.cu``), never part of the product path.
+(``coldcore_b200/csrc/sparse/sparse_abi.cu``), never part of the product path.
 
 Restates, with the same integer semantics:
 
@@ -158,3 +158,22 @@ def brute_gather(rows, cnt, mu, cands, target):
         return c == target
     return np.asarray([sum(role(int(cnt[int(u)])) for u in rows[int(w)])
                        for w in cands], dtype=np.int64)
+
+
+def colex_rank(subset):
+    """Colex rank of a sorted subset: sum_j C(s_j, j + 1)
+    (coldcore ``problems/covering_design.py:59-73``)."""
+    from math import comb
+    return sum(comb(int(s), j + 1) for j, s in enumerate(sorted(subset)))
+
+
+def design_incidence(v, k, t):
+    """The C(v,k,t) incidence in coldcore's layout
+    (``problems/covering_design.py:95-135``): rows in colex order of the
+    blocks, columns the block's t-subsets by lex order of their positions,
+    entries their colex ranks.  Plain loops: small designs only."""
+    from itertools import combinations
+    blocks = sorted(combinations(range(v), k), key=colex_rank)
+    subs = list(combinations(range(k), t))
+    return np.array([[colex_rank([b[p] for p in s]) for s in subs]
+                     for b in blocks], dtype=np.int64)

@@ -91,3 +91,13 @@ def test_map_queries():
     assert found == 3
     o.map[:] = 0
     assert o.map_max() == 0 and o.map_hist(4, 1).tolist() == [0, 0, 0, 0]
+
+
+def test_design_builder_matches_the_reference():
+    """The restated C(v,k,t) builder gives the reference's
+    build_incidence matrices (the golden design cells)."""
+    from oracle.incidence_oracle import design_incidence
+    g = incidence_golden()
+    for key in [k for k in incidence_cells() if k.startswith("design")]:
+        v, k, t = (int(x) for x in g[key + "/meta"][2:5])
+        assert np.array_equal(design_incidence(v, k, t), g[key + "/inc"])
