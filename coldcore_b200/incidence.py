@@ -201,6 +201,13 @@ class GpuIncidenceBackend:
     def _idx(idx):
         return np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64).ravel()
 
+    # ---- the index set the search core walks (coldcore protocol.py:83-87)
+    def word_index(self, words):
+        return self.space.word_index(words)
+
+    def index_word(self, idx):
+        return self.space.index_word(idx)
+
     # ---- fields
     def recount(self, idx):
         idx = self._idx(idx)

@@ -34,15 +34,54 @@ against the dict-of-lists brute force below.
 import numpy as np
 
 
-class IncidenceOracle:
-    """Dense (n_cand, d) incidence rows."""
+class _OneAxis:
+    """The one-axis index set a search core walks (incidence.py:48-86)."""
 
-    def __init__(self, inc, n_univ, mu=1):
+    def __init__(self, size):
+        self.size, self.n, self.axes = int(size), 1, [int(size)]
+
+    def index_word(self, idx):
+        return np.asarray(idx, dtype=np.int64).reshape(-1, 1)
+
+    def word_index(self, words):
+        return np.asarray(words, dtype=np.int64).reshape(-1)
+
+
+class IncidenceOracle:
+    """Dense (n_cand, d) incidence rows, with the backend protocol the
+    search core asks (fields, gathers, updates, map queries)."""
+
+    indep_dist = None
+
+    def __init__(self, inc, n_univ, mu=1, extract_cap=1 << 22):
         self.inc = np.ascontiguousarray(inc, dtype=np.int64)
         self.n_cand, self.d = self.inc.shape
         self.n_univ, self.mu = int(n_univ), int(mu)
         self.cnt = np.zeros(self.n_univ, dtype=np.int64)
         self.map = np.zeros(self.n_cand, dtype=np.int64)
+        self.space = _OneAxis(self.n_cand)
+        self.extract_cap = int(extract_cap)
+
+    def index_word(self, idx):
+        return self.space.index_word(idx)
+
+    def word_index(self, words):
+        return self.space.word_index(words)
+
+    def map_read_at(self, idx):
+        return self.map[np.atleast_1d(np.asarray(idx, dtype=np.int64))]
+
+    def map_all(self):
+        return self.map
+
+    def read_cnt(self, off=0, length=None):
+        length = self.n_univ - off if length is None else length
+        return self.cnt[off:off + length].astype(np.uint16)
+
+    def verify(self, idx):
+        c = np.zeros(self.n_univ, dtype=np.int64)
+        np.add.at(c, self.rows_of(idx).ravel(), 1)
+        return bool((c >= self.mu).all())
 
     # ---- roles (incidence.py:180-187)
     def role(self, c, target):
@@ -90,9 +129,13 @@ class IncidenceOracle:
         b = np.minimum((v - 1) * nbins // vmax, nbins - 1)
         return np.bincount(b, minlength=nbins)[:nbins]
 
-    def map_extract(self, thr):
+    def map_extract(self, thr, cap=None):
+        """Ascending candidates with map >= thr, the first min(found, cap)
+        of them, and the true count (protocol.py:201-208 without the
+        optional shuffle)."""
+        cap = min(cap or self.extract_cap, self.extract_cap)
         idx = np.flatnonzero(self.map >= thr)
-        return idx, self.map[idx], len(idx)
+        return idx[:cap], self.map[idx[:cap]], len(idx)
 
 
 class WeightedIncidenceOracle(IncidenceOracle):
@@ -108,6 +151,8 @@ class WeightedIncidenceOracle(IncidenceOracle):
                    else np.asarray(uw, dtype=np.int64))
         self.cnt = np.zeros(self.n_univ, dtype=np.int64)
         self.map = np.zeros(self.n_cand, dtype=np.int64)
+        self.space = _OneAxis(self.n_cand)
+        self.extract_cap = 1 << 22
 
     def _row(self, c):
         s, e = self.indptr[c], self.indptr[c + 1]

@@ -204,3 +204,22 @@ def test_engine_equals_the_reference_plugin():
                 res.append(out)
         for a, c in zip(*res):
             assert np.array_equal(a, c)
+
+
+def test_design_search_on_the_engine():
+    """The restated search core on the B200 engine: C(13,4,2) = 13 (the
+    reference's own GPU case, tests/test_incidence.py:221-233)."""
+    import time
+
+    from coldcore_b200.incidence import GpuCoveringDesignBackend
+    from coldcore_b200.search import Searcher
+    with GpuCoveringDesignBackend(13, 4, 2) as b:
+        s = Searcher(b, seed=1, deadline=time.time() + 90)
+        s.build_reserve_s = s.loop_reserve_s = 0.0
+        s.load(np.zeros(0, dtype=np.int64))
+        assert s.greedy_fill(10 ** 6) == 0
+        M = s.descend(floor=13, notch_budget_s=20, step0=1, reserve_s=0.0,
+                      min_notch_s=1.0)
+        assert M <= 13 and s.verify_full() == 0
+        o = IncidenceOracle(b.rows(), b.n_univ)
+        assert o.verify(s.code)
