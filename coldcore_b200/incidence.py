@@ -369,6 +369,63 @@ class GpuWeightedIncidenceBackend(GpuIncidenceBackend):
                 f"inc_mode={getattr(self, 'inc_mode', None)})")
 
 
+# ------------------------------------------------ covering-design helpers
+def _binomials(v, r):
+    """C[a, b] for 0 <= a <= v, 0 <= b <= r, saturating at 2^62 (only
+    ranks below C(v, k) are ever unranked, and those fit)."""
+    C = np.zeros((v + 1, r + 1), dtype=np.int64)
+    C[:, 0] = 1
+    sat = np.int64(1) << 62
+    for a in range(1, v + 1):
+        C[a, 1:] = np.minimum(C[a - 1, :-1] + C[a - 1, 1:], sat)
+    return C
+
+
+def design_blocks(v, k, idx):
+    """The k-subsets of {0..v-1} with colex ranks ``idx``: an (m, k)
+    int64 array of sorted elements.  Position j from the top is the
+    largest a with C(a, j+1) <= the remaining rank (the combinatorial
+    number system; coldcore ``problems/covering_design.py:76-92``)."""
+    idx = np.atleast_1d(np.asarray(idx, dtype=np.int64))
+    C = _binomials(v, k)
+    rem = idx.ravel().copy()
+    out = np.empty((len(rem), k), dtype=np.int64)
+    for j in range(k - 1, -1, -1):
+        col = C[:, j + 1]
+        a = np.searchsorted(col, rem, side="right") - 1
+        out[:, j] = a
+        rem -= col[a]
+    return out.reshape(idx.shape + (k,))
+
+
+def subset_ranks(S):
+    """Colex ranks of sorted subsets (rows of S): sum_j C(s_j, j+1)."""
+    S = np.asarray(S, dtype=np.int64)
+    C = _binomials(int(S.max(initial=0)) + 1, S.shape[-1])
+    return sum(C[S[..., j], j + 1] for j in range(S.shape[-1]))
+
+
+def _shared(A, B):
+    """|A n B| for broadcastable rows of distinct elements."""
+    return (A[..., :, None] == B[..., None, :]).any(axis=-1).sum(axis=-1)
+
+
+def block_distance(v, k, a, b):
+    """k - |A n B| for blocks of colex ranks a, b (broadcast): the block
+    metric of coldcore's covering designs (covering_design.py:206-219)."""
+    A, B = design_blocks(v, k, a), design_blocks(v, k, b)
+    return (k - _shared(A, B)).astype(np.int64)
+
+
+def universe_distance(v, k, t, idx, univ):
+    """t - |B n T| for every block in idx and t-subset in univ,
+    (len(idx), len(univ)); 0 exactly when the block covers the t-subset
+    (covering_design.py:221-229)."""
+    B = design_blocks(v, k, np.atleast_1d(idx))[:, None, :]
+    T = design_blocks(v, t, np.atleast_1d(univ))[None, :, :]
+    return (t - _shared(B, T)).astype(np.int64)
+
+
 class GpuCoveringDesignBackend(GpuIncidenceBackend):
     """A covering design C(v,k,t) (mu-fold) whose incidence is built on the
     B200 (``sparse_b200_init_design``), in the layout of coldcore's
@@ -403,6 +460,32 @@ class GpuCoveringDesignBackend(GpuIncidenceBackend):
             ctypes.byref(bd), ctypes.byref(bh)))
         self._closed = False
         self._after_init(bd, bh)
+
+    # ---- locality hooks the search core uses when present (coldcore
+    # problems/covering_design.py:206-229): the block metric
+    @property
+    def indep_dist(self):
+        """Blocks farther apart than k - t share no t-subset."""
+        return self.k - self.t
+
+    def distance(self, a, b):
+        return block_distance(self.v, self.k, a, b)
+
+    def universe_distance(self, idx, univ):
+        return universe_distance(self.v, self.k, self.t, idx, univ)
+
+    def rank_block(self, idx):
+        """Candidate indices -> (m, k) sorted 0-based blocks."""
+        return design_blocks(self.v, self.k, np.ravel(idx))
+
+    def block_rank(self, blocks):
+        """(m, k) 0-based blocks (any element order) -> candidates."""
+        S = np.sort(np.atleast_2d(np.asarray(blocks, dtype=np.int64)), axis=1)
+        if S.shape[1] != self.k or (S.size and (S.min() < 0
+                                                or S.max() >= self.v)):
+            raise ValueError(f"blocks must be (m, {self.k}) with elements "
+                             f"in 0..{self.v - 1}")
+        return subset_ranks(S)
 
     def rows(self, c0=0, n=None):
         """Incidence rows [c0, c0 + n) as an (n, d) int32 array."""

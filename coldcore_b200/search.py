@@ -288,9 +288,17 @@ class Searcher:
         self.stats["transforms"] += 1
         return self.b.map_read_at(self.code)
 
-    def _near(self, centre_digits):
-        """Jittered digit-Hamming distance of every incumbent to a word."""
-        d = (self._digits(self.code) != centre_digits[None, :]).sum(axis=1)
+    def _near(self, centre):
+        """Jittered distance of every incumbent to the word ``centre``: the
+        backend's own metric when it has one (the locality hook of
+        coldcore's protocol, e.g. the block metric of a covering design,
+        search.py:581-583), else the digit-Hamming distance."""
+        dist = getattr(self.b, "distance", None)
+        if dist is not None:
+            d = np.asarray(dist(self.code, int(centre)), dtype=np.int64)
+        else:
+            c = self._digits(np.array([centre]))[0]
+            d = (self._digits(self.code) != c[None, :]).sum(axis=1)
         return d + self.rng.random(len(self.code))
 
     def _pick(self, k, mode):
@@ -299,7 +307,7 @@ class Searcher:
         if mode == "random":
             return self.rng.choice(m, size=k, replace=False)
         if mode == "cluster":
-            centre = self._digits(self.code[self.rng.integers(m)][None])[0]
+            centre = int(self.code[self.rng.integers(m)])
             return np.argsort(self._near(centre))[:k]
         if mode == "hole":
             self.b.gain_map()
@@ -309,8 +317,7 @@ class Searcher:
                 oi, _ov, _found = self.b.map_extract(max(1, mx // 2), cap=4096)
                 if len(oi):
                     anchor = int(oi[self.rng.integers(len(oi))])
-                    centre = self._digits(np.array([anchor]))[0]
-                    return np.argsort(self._near(centre))[:k]
+                    return np.argsort(self._near(anchor))[:k]
             mode = "low"                         # no hole: fall back
         lo = np.asarray(self.losses(), dtype=np.float64)
         jit = self.rng.exponential(scale=max(1.0, lo.mean() * 0.15), size=m)
@@ -350,12 +357,17 @@ class Searcher:
                 break
             self.rng.shuffle(zeros)
             sep = b.indep_dist
-            if sep is not None and sep < self.b.space.n:
-                digs = self._digits(self.code[zeros])
+            dist = getattr(b, "distance", None)
+            if sep is not None and (dist is not None or sep < self.b.space.n):
+                cand = self.code[zeros]
+                digs = None if dist is not None else self._digits(cand)
                 keep = [0]
                 for i in range(1, len(zeros)):
-                    far = (digs[keep] != digs[i][None, :]).sum(axis=1) > sep
-                    if far.all():
+                    if dist is not None:        # the backend's own metric
+                        d = np.asarray(dist(cand[np.array(keep)], cand[i]))
+                    else:
+                        d = (digs[keep] != digs[i][None, :]).sum(axis=1)
+                    if (d > sep).all():
                         keep.append(i)
                 pick = zeros[np.array(keep)]
             else:

@@ -222,3 +222,24 @@ def design_incidence(v, k, t):
     subs = list(combinations(range(k), t))
     return np.array([[colex_rank([b[p] for p in s]) for s in subs]
                      for b in blocks], dtype=np.int64)
+
+
+class DesignOracle(IncidenceOracle):
+    """A covering design C(v,k,t) (mu-fold) with the block metric of
+    coldcore's design backend (``problems/covering_design.py:200-229``):
+    distance k - |A n B|, removal independence beyond k - t."""
+
+    def __init__(self, v, k, t, mu=1):
+        from itertools import combinations
+        from math import comb
+        super().__init__(design_incidence(v, k, t), comb(v, t), mu=mu)
+        self.v, self.k, self.t = v, k, t
+        self.blocks = np.array(sorted(combinations(range(v), k),
+                                      key=colex_rank), dtype=np.int64)
+        self.indep_dist = k - t
+
+    def distance(self, a, b):
+        A = self.blocks[np.asarray(a, dtype=np.int64)]
+        B = self.blocks[np.asarray(b, dtype=np.int64)]
+        shared = (A[..., :, None] == B[..., None, :]).any(axis=-1).sum(axis=-1)
+        return (self.k - shared).astype(np.int64)

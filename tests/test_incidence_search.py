@@ -45,3 +45,56 @@ def test_mu_fold_design_search():
                   min_notch_s=1.0)
     assert M <= 14 and s.verify_full() == 0
     assert b.verify(s.code)
+
+
+@pytest.mark.parametrize("v,k,t,opt", [(7, 3, 2, 7), (8, 4, 3, 14),
+                                       (13, 4, 2, 13)])
+def test_search_with_the_block_metric(v, k, t, opt):
+    """Cluster / hole ruins and batched peel use the design's own metric
+    when the backend has one (the protocol's locality hooks)."""
+    from oracle.incidence_oracle import DesignOracle
+    b = DesignOracle(v, k, t)
+    s = Searcher(b, seed=3, deadline=time.time() + 120)
+    s.build_reserve_s = s.loop_reserve_s = 0.0
+    s.load(np.zeros(0, dtype=np.int64))
+    assert s.greedy_fill(10 ** 6) == 0
+    s.peel()
+    assert s.verify_full() == 0
+    for mode in ("cluster", "hole"):
+        removed = s.ruin(3, mode)
+        assert len(removed) == 3
+        s.greedy_fill(10 ** 6)
+        assert s.verify_full() == 0
+    M = s.descend(floor=opt, notch_budget_s=20, step0=1, reserve_s=0.0,
+                  min_notch_s=1.0)
+    assert M <= opt and s.verify_full() == 0 and b.verify(s.code)
+
+
+def test_design_metric_helpers():
+    from coldcore_b200.incidence import (block_distance, design_blocks,
+                                         subset_ranks, universe_distance)
+    from oracle.incidence_oracle import DesignOracle, colex_rank
+    v, k, t = 9, 4, 2
+    o = DesignOracle(v, k, t)
+    every = np.arange(len(o.blocks))
+    assert np.array_equal(design_blocks(v, k, every), o.blocks)
+    assert np.array_equal(subset_ranks(o.blocks), every)
+    rng = np.random.default_rng(9)
+    idx = rng.choice(len(every), 40)
+    D = block_distance(v, k, idx[:, None], idx[None, :])
+    assert np.array_equal(D, o.distance(idx[:, None], idx[None, :]))
+    assert (D == D.T).all() and (np.diag(D) == 0).all()
+    u = rng.choice(o.n_univ, 6)
+    ud = universe_distance(v, k, t, idx, u)
+    for i in range(40):
+        for j in range(6):
+            assert (ud[i, j] == 0) == (u[j] in o.inc[idx[i]])
+    # farther apart than k - t: no shared t-subset
+    for i in range(40):
+        for j in range(40):
+            if D[i, j] > k - t:
+                assert not set(o.inc[idx[i]]) & set(o.inc[idx[j]])
+    assert colex_rank([0, 1, 2, 3]) == 0
+    big = design_blocks(30, 8, [0, 5852924])
+    assert big[0].tolist() == list(range(8))
+    assert big[1].tolist() == list(range(22, 30))
