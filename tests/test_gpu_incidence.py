@@ -223,3 +223,59 @@ def test_design_search_on_the_engine():
         assert M <= 13 and s.verify_full() == 0
         o = IncidenceOracle(b.rows(), b.n_univ)
         assert o.verify(s.code)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3, 5, 8, 9, 16, 17, 31, 32, 33, 64, 70])
+def test_every_row_width_against_the_oracle(d):
+    """Each lanes-per-row form (1..32 lanes, rows longer than a warp):
+    fields, gathers and updates equal the oracle's."""
+    rng = np.random.default_rng(d)
+    n_univ, n_cand = 150, 301
+    inc = np.stack([rng.choice(n_univ, d, replace=False)
+                    for _ in range(n_cand)])
+    o = IncidenceOracle(inc, n_univ, mu=2)
+    with GpuIncidenceBackend(inc, n_univ, mu=2) as b:
+        sol = rng.choice(n_cand, 40, replace=False)
+        b.recount(sol)
+        o.recount(sol)
+        assert np.array_equal(b.read_cnt().astype(np.int64), o.cnt)
+        for t in (0, 1, 3):
+            o.field(t)
+            assert b._lib.sparse_field(t) == 0
+            assert np.array_equal(b.map_all(), o.map)
+            probe = rng.choice(n_cand, 37)
+            assert np.array_equal(b.ball_gather(probe, t),
+                                  o.ball_gather(probe, t))
+        add = rng.choice(n_cand, 9)
+        b.ball_update(add, +1)
+        o.ball_update(add, +1)
+        assert np.array_equal(b.read_cnt().astype(np.int64), o.cnt)
+
+
+@pytest.mark.parametrize("mean_len", [1, 3, 6, 12, 24, 40])
+def test_every_csr_row_width_against_the_oracle(mean_len):
+    rng = np.random.default_rng(100 + mean_len)
+    n_univ, n_cand = 120, 257
+    lens = rng.integers(0, 2 * mean_len + 1, n_cand)
+    lens = np.minimum(lens, n_univ)
+    indptr = np.concatenate(([0], np.cumsum(lens)))
+    indices = np.concatenate([rng.choice(n_univ, int(k), replace=False)
+                              for k in lens])
+    w = rng.integers(1, 4, len(indices))
+    uw = rng.integers(1, 5, n_univ)
+    o = WeightedIncidenceOracle(indptr, indices, w, n_univ, uw=uw, mu=3)
+    with GpuWeightedIncidenceBackend(indptr, indices, w, n_univ, uw=uw,
+                                     mu=3) as b:
+        sol = rng.choice(n_cand, 30, replace=False)
+        b.recount(sol)
+        o.recount(sol)
+        assert np.array_equal(b.read_cnt().astype(np.int64), o.cnt)
+        assert b.uncovered() == o.uncovered()
+        for t in (0, 1, 2):
+            probe = rng.choice(n_cand, 29)
+            assert np.array_equal(b.ball_gather(probe, t),
+                                  o.ball_gather(probe, t))
+        b.gain_map()
+        assert np.array_equal(b.map_all(), o.ball_gather(np.arange(n_cand), 0))
+        b.loss_map()
+        assert np.array_equal(b.map_all(), o.ball_gather(np.arange(n_cand), 1))
