@@ -43,6 +43,16 @@ RUIN_PRIOR = {"low": 1.0, "hole": 2.0, "cluster": 1.0, "random": 1.0}
 #: fixed selection: a uniform draw from this list (search.py:65)
 FIXED_DRAW = ("low", "hole", "hole", "cluster", "random")
 SELECTIONS = ("fixed", "adaptive", "learned")
+#: the opt-in deficit-targeted operator (``lns(..., deficit=True)``):
+#: weighted like ``hole`` in both the prior and the fixed list
+#: (search.py:57-66)
+RUIN_OPS_EXT = RUIN_OPS + ("deficit",)
+RUIN_PRIOR_EXT = dict(RUIN_PRIOR, deficit=2.0)
+FIXED_DRAW_DEFICIT = FIXED_DRAW + ("deficit", "deficit")
+#: uncovered words the deficit operator aims at, and counters read per
+#: scan of cnt (search.py:80-81)
+DEFICIT_WORDS = 4
+SCAN_CHUNK = 1 << 24
 
 
 def _rng_for(seed):
@@ -69,15 +79,24 @@ class OperatorBandit:
         self.uses = np.zeros(len(self.ops), dtype=np.int64)
         self.reward = np.zeros(len(self.ops))
 
-    def probabilities(self):
+    def probabilities(self, boost=None):
+        """``boost``: optional {op: factor} hint applied to the scores
+        (lifted to the floor first, so a crushed score can come back)
+        before normalising (search.py:131-149)."""
         w = np.maximum(self.score, 0.0)
         k = len(self.ops)
+        if boost:
+            w = w.copy()
+            for op, f in boost.items():
+                if op in self.ops:
+                    i = self.ops.index(op)
+                    w[i] = max(w[i], self.floor) * float(f)
         if w.sum() <= 0:
             return np.full(k, 1.0 / k)
         return self.floor / k + (1.0 - self.floor) * w / w.sum()
 
-    def select(self):
-        i = int(self.rng.choice(len(self.ops), p=self.probabilities()))
+    def select(self, boost=None):
+        i = int(self.rng.choice(len(self.ops), p=self.probabilities(boost)))
         self.uses[i] += 1
         return self.ops[i]
 
@@ -138,6 +157,8 @@ class Searcher:
         self.stats = {"transforms": 0, "placements": 0, "removals": 0,
                       "rounds": 0, "recounts": 0, "accepts": 0,
                       "learned_rounds": 0, "fallback_rounds": 0}
+        self._scan_off = 0                 # rotating start of the cnt scan
+        self._deficit_cache = (None, None)
 
     # ------------------------------------------------ state
     def time_left(self):
@@ -301,9 +322,75 @@ class Searcher:
             d = (self._digits(self.code) != c[None, :]).sum(axis=1)
         return d + self.rng.random(len(self.code))
 
-    def _pick(self, k, mode):
+    # ------------------------------------------------ the deficit itself
+    def supports_deficit(self):
+        """The backend can hand back cnt (search.py:471-478)."""
+        return hasattr(self.b, "read_cnt")
+
+    def uncovered_words(self, limit=DEFICIT_WORDS, chunk=SCAN_CHUNK,
+                        scan_cap=None):
+        """Up to ``limit`` currently deficient words (search.py:480-528):
+        the backend's own ``deficient_universe`` when it has one, else a
+        chunked scan of cnt from a rotating offset, cached against the
+        solution that produced it.  Empty means none found within the cap,
+        never that nothing is uncovered."""
+        if not self.supports_deficit() or self.uncov == 0:
+            return np.zeros(0, dtype=np.int64)
+        exact = getattr(self.b, "deficient_universe", None)
+        if exact is not None:
+            return np.asarray(exact(limit, self.rng), dtype=np.int64)
+        key = (len(self.code), self.uncov,
+               hash(np.ascontiguousarray(self.code).tobytes()))
+        ckey, cval = self._deficit_cache
+        if ckey == key and cval is not None and len(cval) >= min(
+                limit, self.uncov):
+            return cval[:limit]
+        size = self.b.space.size
+        mu = getattr(self.b, "mu", 1)
+        chunk = max(1, int(chunk))
+        budget = size if scan_cap is None else min(size, int(scan_cap))
+        found = []
+        off = int(self._scan_off) % size
+        read = 0
+        while read < budget and len(found) < limit:
+            take = min(chunk, size - off, budget - read)
+            hit = np.flatnonzero(np.asarray(self.b.read_cnt(off, take)) < mu)
+            if len(hit):
+                got = hit[:limit - len(found)] + off
+                found.extend(int(v) for v in got)
+                self._scan_off = (int(got[-1]) + 1) % size
+            read += take
+            off = (off + take) % size
+        if len(found) < limit:
+            self._scan_off = 0                 # exhausted: restart the sweep
+        out = np.array(sorted(found), dtype=np.int64)
+        if len(out):
+            self._deficit_cache = (key, out)
+        return out
+
+    def _pick(self, k, mode, deficit_pool=3):
         """Positions (into ``self.code``) that ``mode`` removes."""
         m = len(self.code)
+        if mode == "deficit":
+            # k incumbents drawn from the ~3k nearest to the words that are
+            # actually uncovered (search.py:552-576); none found: ``hole``
+            tgt = self.uncovered_words()
+            if not len(tgt):
+                return self._pick(k, "hole")
+            self.stats["deficit_ruins"] = self.stats.get("deficit_ruins",
+                                                         0) + 1
+            udist = getattr(self.b, "universe_distance", None)
+            if udist is not None:
+                d = np.asarray(udist(self.code, tgt), dtype=np.int64).min(
+                    axis=1)
+            else:
+                digs, tw = self._digits(self.code), self._digits(tgt)
+                d = np.full(m, np.iinfo(np.int32).max, dtype=np.int64)
+                for t in tw:
+                    np.minimum(d, (digs != t[None, :]).sum(axis=1), out=d)
+            order = np.argsort(d + self.rng.random(m))
+            near = order[:min(m, max(deficit_pool * k, k + 8))]
+            return self.rng.choice(near, size=k, replace=False)
         if mode == "random":
             return self.rng.choice(m, size=k, replace=False)
         if mode == "cluster":
@@ -382,11 +469,15 @@ class Searcher:
 
     # ------------------------------------------------ LNS at fixed M
     def lns(self, M, round_budget_s, kmin=8, kmax=None, select="fixed",
-            log_every=20, stall_s=None):
+            log_every=20, stall_s=None, deficit=False, deficit_hint=3,
+            deficit_boost=4.0):
         """Ruin/recreate rounds at fixed M until feasible or out of budget
         (search.py:672-784).  A round that ends worse than it started is
         rejected (the best snapshot is restored) except with probability
-        0.1.  Returns the final uncovered count (0 = solved)."""
+        0.1.  ``deficit=True`` adds the deficit-targeted ruin to the
+        selection and, within ``deficit_hint`` of feasible, favours it
+        (half the fixed draws; a ``deficit_boost`` hint to the bandit).
+        Returns the final uncovered count (0 = solved)."""
         if select not in SELECTIONS:
             raise ValueError(f"unknown ruin selection: {select!r}")
         if select == "learned" and self.proposer is None:
@@ -398,7 +489,15 @@ class Searcher:
         if len(self.code) < M:
             self.greedy_fill(M)
         self._snapshot()
-        bandit = OperatorBandit(self.rng) if select != "fixed" else None
+        modes = FIXED_DRAW_DEFICIT if deficit else FIXED_DRAW
+        if select == "fixed":
+            bandit = None
+        elif deficit:
+            bandit = OperatorBandit(self.rng, ops=RUIN_OPS_EXT,
+                                    prior=RUIN_PRIOR_EXT)
+        else:
+            bandit = OperatorBandit(self.rng)
+        hint = {"deficit": deficit_boost} if deficit else None
         r = 0
         while self.uncov > 0:
             now = time.time()
@@ -409,9 +508,13 @@ class Searcher:
                 break
             pre, pre_best = self.uncov, self.best_uncov
             k = int(self.rng.integers(kmin, kmax + 1))
+            near = deficit and self.uncov <= deficit_hint
             pick = None
             if select == "fixed":
-                mode = FIXED_DRAW[int(self.rng.integers(len(FIXED_DRAW)))]
+                if near and self.rng.random() < 0.5:
+                    mode = "deficit"
+                else:
+                    mode = modes[int(self.rng.integers(len(modes)))]
             else:
                 mode = None
                 if select == "learned":
@@ -422,7 +525,7 @@ class Searcher:
                     else:
                         self.stats["fallback_rounds"] += 1
                 if mode is None:
-                    mode = bandit.select()
+                    mode = bandit.select(hint if near else None)
             if self.move_log is not None:
                 self.move_log(self, "pre", k=k, mode=mode)
             if mode == "learned" or self.move_log is not None:

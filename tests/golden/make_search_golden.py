@@ -20,6 +20,11 @@ ascending indices, so a seeded run is deterministic):
 
 Output: ``search_traces.json`` (committed; nothing at test time reads the
 reference).
+
+With ``--deficit`` it writes ``search_deficit_traces.json`` instead: the
+opt-in deficit-targeted ruin (``ruin(k, "deficit")`` after three ``low``
+removals, so that words are uncovered) and ``lns(..., deficit=True)``
+with both selections, from the same starting points.
 """
 import json
 import os
@@ -91,5 +96,42 @@ def main():
         json.dump(out, f)
 
 
+def main_deficit():
+    out = []
+    for problem, axes, R, mu, seed in CELLS:
+        t = built(problem, axes, R, mu, seed)
+        t.peel()
+        t.ruin(3, "low")
+        pre = t.uncovered_words().tolist()
+        removed = t.ruin(3, "deficit")
+        ruin = {"targets": [int(w) for w in pre],
+                "removed": sorted(int(w) for w in removed),
+                "uncov": int(t.uncov),
+                "deficit_ruins": int(t.stats.get("deficit_ruins", 0))}
+        lns = {}
+        for select in ("fixed", "adaptive"):
+            t = built(problem, axes, R, mu, seed)
+            t.peel()
+            M = len(t.code) - 1
+            t.ruin(1, "low")
+            unc = t.lns(M, round_budget_s=20.0, kmin=2, kmax=4,
+                        select=select, log_every=0, deficit=True)
+            lns[select] = {"M": M, "uncov": int(unc), "solved": unc == 0,
+                           "rounds": int(t.stats["rounds"]),
+                           "deficit_ruins": int(t.stats.get("deficit_ruins",
+                                                            0)),
+                           "code": t.code.tolist()}
+        out.append({"problem": problem, "axes": axes, "R": R, "mu": mu,
+                    "seed": seed, "ruin": ruin, "lns": lns})
+        print(problem, axes, R, mu, ruin["removed"],
+              {k: (v["uncov"], v["rounds"], v["deficit_ruins"])
+               for k, v in lns.items()}, flush=True)
+    with open(os.path.join(HERE, "search_deficit_traces.json"), "w") as f:
+        json.dump(out, f)
+
+
 if __name__ == "__main__":
-    main()
+    if "--deficit" in sys.argv:
+        main_deficit()
+    else:
+        main()

@@ -12,8 +12,8 @@ import os
 import numpy as np
 import pytest
 
-from coldcore_b200.search import (FIXED_DRAW, RUIN_OPS, OperatorBandit,
-                                  Searcher)
+from coldcore_b200.search import (FIXED_DRAW, RUIN_OPS, RUIN_OPS_EXT,
+                                  RUIN_PRIOR_EXT, OperatorBandit, Searcher)
 from oracle.dp_oracle import OracleBackend
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -161,3 +161,50 @@ def test_move_log_sees_every_round():
     for ev, info in events:
         if ev == "ruin":
             assert len(info["pick"]) == len(set(info["pick"].tolist()))
+
+
+with open(os.path.join(HERE, "golden", "search_deficit_traces.json")) as f:
+    DEFICIT_TRACES = json.load(f)
+
+
+@pytest.mark.parametrize("t", DEFICIT_TRACES, ids=_id)
+def test_deficit_ruin_matches_reference(t):
+    """The opt-in deficit-targeted ruin: the same uncovered words found by
+    the rotating cnt scan, the same incumbents removed."""
+    s = _built(t)
+    s.peel()
+    s.ruin(3, "low")
+    assert s.uncovered_words().tolist() == t["ruin"]["targets"]
+    removed = s.ruin(3, "deficit")
+    assert sorted(removed.tolist()) == t["ruin"]["removed"]
+    assert s.uncov == t["ruin"]["uncov"]
+    assert s.stats.get("deficit_ruins", 0) == t["ruin"]["deficit_ruins"]
+
+
+@pytest.mark.parametrize("t", DEFICIT_TRACES, ids=_id)
+@pytest.mark.parametrize("select", ["fixed", "adaptive"])
+def test_deficit_lns_matches_reference(t, select):
+    g = t["lns"][select]
+    if not g["solved"]:
+        pytest.skip("the reference run hit its time budget (not replayable)")
+    s = _built(t)
+    s.peel()
+    s.ruin(1, "low")
+    unc = s.lns(g["M"], round_budget_s=120.0, kmin=2, kmax=4, select=select,
+                log_every=0, deficit=True)
+    assert unc == 0
+    assert s.stats["rounds"] == g["rounds"]
+    assert s.stats.get("deficit_ruins", 0) == g["deficit_ruins"]
+    assert s.code.tolist() == g["code"]
+
+
+def test_bandit_boost_hint():
+    b = OperatorBandit(np.random.default_rng(0), ops=RUIN_OPS_EXT,
+                       prior=RUIN_PRIOR_EXT)
+    p0 = b.probabilities()
+    p1 = b.probabilities({"deficit": 4.0})
+    i = RUIN_OPS_EXT.index("deficit")
+    assert np.isclose(p1.sum(), 1.0) and p1[i] > p0[i]
+    for _ in range(300):
+        b.update("deficit", 0.0)
+    assert b.probabilities({"deficit": 4.0})[i] > b.probabilities()[i]
