@@ -584,7 +584,8 @@ class Searcher:
 
     # ------------------------------------------------ notch descent
     def descend(self, floor=1, notch_budget_s=300.0, step0=4, step_cap=1024,
-                kmin=8, kmax=None, select="fixed", reserve_s=30.0,
+                kmin=8, kmax=None, select="fixed", deficit=False,
+                reserve_s=30.0,
                 min_notch_s=20.0, fail_limit=3):
         """From a feasible solution, try M - step; halve the step on a
         failed notch, double it on a success in under a quarter of the
@@ -608,7 +609,7 @@ class Searcher:
                 break
             self.ruin(len(self.code) - target, "low")
             unc = self.lns(target, budget, kmin=kmin, kmax=kmax,
-                           select=select, log_every=0)
+                           select=select, log_every=0, deficit=deficit)
             if unc == 0 and self.verify_full() == 0:
                 self.peel()
                 if self.verify_full() != 0:

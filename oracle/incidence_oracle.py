@@ -78,6 +78,14 @@ class IncidenceOracle:
         length = self.n_univ - off if length is None else length
         return self.cnt[off:off + length].astype(np.uint16)
 
+    def deficient_universe(self, limit, rng=None):
+        """Up to ``limit`` universe elements with cnt < mu, sorted; a random
+        subset of them when ``rng`` is given (incidence.py:232-238)."""
+        u = np.flatnonzero(self.cnt < self.mu)
+        if rng is not None and len(u) > limit:
+            u = np.sort(rng.choice(u, size=int(limit), replace=False))
+        return u[:limit].astype(np.int64)
+
     def verify(self, idx):
         c = np.zeros(self.n_univ, dtype=np.int64)
         np.add.at(c, self.rows_of(idx).ravel(), 1)
@@ -237,6 +245,19 @@ class DesignOracle(IncidenceOracle):
         self.blocks = np.array(sorted(combinations(range(v), k),
                                       key=colex_rank), dtype=np.int64)
         self.indep_dist = k - t
+
+    def universe_distance(self, idx, univ):
+        """t - |B n T|: 0 exactly where block covers the t-subset
+        (covering_design.py:221-229)."""
+        from itertools import combinations
+        if not hasattr(self, "_tsets"):
+            self._tsets = np.array(sorted(combinations(range(self.v), self.t),
+                                          key=colex_rank), dtype=np.int64)
+        B = self.blocks[np.atleast_1d(np.asarray(idx, dtype=np.int64))]
+        T = self._tsets[np.atleast_1d(np.asarray(univ, dtype=np.int64))]
+        shared = (B[:, None, :, None] == T[None, :, None, :]).any(
+            axis=-1).sum(axis=-1)
+        return (self.t - shared).astype(np.int64)
 
     def distance(self, a, b):
         A = self.blocks[np.asarray(a, dtype=np.int64)]

@@ -98,3 +98,23 @@ def test_design_metric_helpers():
     big = design_blocks(30, 8, [0, 5852924])
     assert big[0].tolist() == list(range(8))
     assert big[1].tolist() == list(range(22, 30))
+
+
+def test_deficit_ruin_on_a_design():
+    """The deficit ruin aims at the uncovered t-subsets through the
+    design's own hooks (deficient_universe, universe_distance): C(10,4,3)
+    reaches its optimum of 30 (the reference's locality case,
+    tests/test_incidence.py:495-510)."""
+    from oracle.incidence_oracle import DesignOracle
+    b = DesignOracle(10, 4, 3)
+    u = b.universe_distance([0, 1], np.arange(b.n_univ))
+    assert ((u == 0).sum(axis=1) == 4).all()          # C(4,3) per block
+    s = Searcher(b, seed=3, deadline=time.time() + 120)
+    s.build_reserve_s = s.loop_reserve_s = 0.0
+    s.load(np.zeros(0, dtype=np.int64))
+    assert s.greedy_fill(10 ** 6) == 0
+    s.peel()
+    M = s.descend(floor=30, notch_budget_s=30, step0=1, reserve_s=0.0,
+                  min_notch_s=1.0, deficit=True)
+    assert M <= 30 and s.verify_full() == 0 and b.verify(s.code)
+    assert s.stats.get("deficit_ruins", 0) > 0
