@@ -357,6 +357,37 @@ def measure_cell(cell, args, dist, timed=True):
         b.close()
 
 
+def measure_batch_small(args):
+    """A campaign of many small cells, where a persistent launch pays:
+    1,024 seeded cells of 10^3..10^5 words (otherwise as measure_batch).
+    Persistent graph launch against one launch per pass per cell."""
+    import torch
+
+    from coldcore_b200.batch import BatchEngine
+    from coldcore_b200.workloads import batch_cells
+    cells = batch_cells(1024, seed=11, lo=3.0, hi=5.0)
+    out = {"cells": len(cells),
+           "words": int(sum(int(np.prod(a)) for _, a, _, _ in cells))}
+    with BatchEngine() as b:
+        for p, a, R, code in cells:
+            b.add(p, a, R, code)
+        b.build(0)
+        for mode, key in ((0, "persistent"), (1, "per_pass_launches")):
+            for _ in range(2):
+                b.run(mode)
+            torch.cuda.synchronize()
+            reps = max(3, args.steps // 4)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                b.run(mode)
+            dt = (time.perf_counter() - t0) / reps
+            out[key] = {"ms_per_step": round(1e3 * dt, 3),
+                        "instances_per_s": round(len(cells) / dt, 1)}
+    out["speedup"] = round(out["persistent"]["instances_per_s"]
+                           / out["per_pass_launches"]["instances_per_s"], 2)
+    return out
+
+
 def form_name(f):
     """Schedule form flags of one launch (GpuBackend.plan_forms) as text."""
     names = [("pipe", 1), ("pack", 2), ("in16", 4), ("out16", 8),
@@ -551,6 +582,12 @@ def run_b200(args, dist):
             line["incidence"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_lns and dist.world == 1:
         line["lns"] = measure_lns(args)
+    if not args.no_batch:
+        # last, so that nothing else depends on it
+        try:
+            line["batched_small"] = measure_batch_small(args)
+        except Exception as e:           # noqa: BLE001
+            line["batched_small"] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
 
 
