@@ -426,6 +426,50 @@ def universe_distance(v, k, t, idx, univ):
     return (t - _shared(B, T)).astype(np.int64)
 
 
+def block_neighbours(v, k, idx, radius=1, m=None, rng=None):
+    """Blocks at block distance ``radius`` from block ``idx``
+    (covering_design.py:231-257): every one of the k (v-k) single swaps
+    at radius 1 (``m`` of them sampled when given), and a sample of up to
+    ``m`` (default 64) distinct ``radius``-fold swaps beyond that."""
+    B = design_blocks(v, k, [int(idx)])[0]
+    outside = np.setdiff1d(np.arange(v, dtype=np.int64), B)
+    r = int(radius)
+    if r < 1 or r > min(k, v - k):
+        return np.zeros(0, dtype=np.int64)
+    if r == 1:
+        n = k * (v - k)
+        rows = np.repeat(B[None, :], n, axis=0)
+        rows[np.arange(n), np.repeat(np.arange(k), v - k)] = np.tile(outside,
+                                                                     k)
+        res = subset_ranks(np.sort(rows, axis=1))
+        if m is not None and int(m) < n:
+            rng = np.random.default_rng() if rng is None else rng
+            res = rng.choice(res, size=int(m), replace=False)
+        return res
+    m = 64 if m is None else int(m)
+    if m <= 0:
+        return np.zeros(0, dtype=np.int64)
+    rng = np.random.default_rng() if rng is None else rng
+    drop = np.argsort(rng.random((m, k)), axis=1)[:, :r]
+    add = np.argsort(rng.random((m, v - k)), axis=1)[:, :r]
+    rows = np.repeat(B[None, :], m, axis=0)
+    rows[np.arange(m)[:, None], drop] = outside[add]
+    return np.unique(subset_ranks(np.sort(rows, axis=1)))
+
+
+def candidates_covering(v, k, t, univ_idx):
+    """Every block containing the t-subset ``univ_idx``, sorted: its
+    C(v-t, k-t) completions (covering_design.py:259-269)."""
+    from itertools import combinations
+    T = design_blocks(v, t, [int(univ_idx)])[0]
+    rest = np.setdiff1d(np.arange(v, dtype=np.int64), T)
+    tails = np.array(list(combinations(rest.tolist(), k - t)),
+                     dtype=np.int64).reshape(-1, k - t)
+    rows = np.concatenate([np.repeat(T[None, :], len(tails), axis=0), tails],
+                          axis=1)
+    return np.sort(subset_ranks(np.sort(rows, axis=1)))
+
+
 def read_cover(path, v, k):
     """A cover file in the La Jolla repository's format -> candidate
     indices (colex ranks): one block per line, k distinct elements in
@@ -522,6 +566,12 @@ class GpuCoveringDesignBackend(GpuIncidenceBackend):
             raise ValueError(f"blocks must be (m, {self.k}) with elements "
                              f"in 0..{self.v - 1}")
         return subset_ranks(S)
+
+    def neighbours(self, idx, radius=1, m=None, rng=None):
+        return block_neighbours(self.v, self.k, idx, radius, m, rng)
+
+    def candidates_covering(self, univ_idx):
+        return candidates_covering(self.v, self.k, self.t, univ_idx)
 
     def read_cover(self, path):
         return read_cover(path, self.v, self.k)

@@ -154,3 +154,27 @@ def test_cover_file_round_trip(tmp_path):
     open(fano, "w").write("1 2 3\n1 4 5\n1 6 7\n2 4 6\n2 5 7\n3 4 7\n3 5 6\n")
     from oracle.incidence_oracle import DesignOracle
     assert DesignOracle(7, 3, 2).verify(read_cover(fano, 7, 3))
+
+
+def test_block_neighbourhoods_and_coverers():
+    """The remaining locality hooks of the design layer
+    (covering_design.py:231-269), against the design oracle."""
+    from math import comb
+
+    from coldcore_b200.incidence import block_neighbours, candidates_covering
+    from oracle.incidence_oracle import DesignOracle
+    v, k, t = 9, 4, 2
+    o = DesignOracle(v, k, t)
+    rng = np.random.default_rng(9)
+    c = int(rng.integers(len(o.blocks)))
+    n1 = block_neighbours(v, k, c, 1)
+    assert len(n1) == k * (v - k) == len(np.unique(n1))
+    assert (o.distance(n1, c) == 1).all() and c not in n1
+    assert len(block_neighbours(v, k, c, 1, m=7, rng=rng)) == 7
+    n2 = block_neighbours(v, k, c, 2, m=50, rng=rng)
+    assert 0 < len(n2) <= 50 and (o.distance(n2, c) == 2).all()
+    assert len(block_neighbours(v, k, c, 99)) == 0
+    for u in rng.choice(o.n_univ, 4):
+        cc = candidates_covering(v, k, t, int(u))
+        assert len(cc) == comb(v - t, k - t)
+        assert np.array_equal(cc, np.flatnonzero((o.inc == u).any(axis=1)))
