@@ -577,7 +577,13 @@ def run_b200(args, dist):
         # a failure here is reported in its own object, not the line's
         try:
             from coldcore_b200.incidence_bench import measure as inc_measure
-            line["incidence"] = inc_measure()
+            cpu_field = None
+            if not args.no_cpu:
+                from oracle.cport import inc_field
+
+                def cpu_field(rows, cnt, out):     # the CPU baseline leg
+                    inc_field(rows, cnt, 0, out=out)
+            line["incidence"] = inc_measure(cpu_field=cpu_field)
         except Exception as e:           # noqa: BLE001
             line["incidence"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_lns and dist.world == 1:

@@ -46,9 +46,13 @@ def _time_fields(b, stream, reps):
     return e0.elapsed_time(e1) / (2 * reps)
 
 
-def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True):
+def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True,
+            cpu_field=None):
     """Both cells stay resident and are timed in alternation, `rounds`
-    times each after a warm-up; the medians are reported."""
+    times each after a warm-up; the medians are reported.  ``cpu_field``
+    (optional, the caller's CPU baseline): ``cpu_field(rows, cnt, out)``
+    computes the gain field of the host copy of the incidence; it is
+    timed over three calls and checked against the engine's field."""
     import torch
 
     from .incidence import GpuCoveringDesignBackend, GpuIncidenceBackend
@@ -59,9 +63,11 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True):
         sol = rng.choice(n_cand, max(1, n_cand // 2000), replace=False)
         b.recount(sol)
         stream = torch.cuda.ExternalStream(int(b._lib.sparse_b200_stream()))
+        host_rows = b.rows()
+        host_cnt = b.read_cnt().astype(np.int32)
         ref = None
         if with_ref and os.path.exists(REF):
-            ref = GpuIncidenceBackend(b.rows(), n_univ, plugin_path=REF)
+            ref = GpuIncidenceBackend(host_rows, n_univ, plugin_path=REF)
         try:
             if ref is not None:
                 ref.recount(sol)
@@ -90,6 +96,15 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True):
         finally:
             if ref is not None:
                 ref.close()
+    cpu_ms = cpu_same = None
+    if cpu_field is not None:
+        out_map = np.empty(n_cand, dtype=np.int32)
+        cpu_field(host_rows, host_cnt, out_map)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            cpu_field(host_rows, host_cnt, out_map)
+        cpu_ms = (time.perf_counter() - t0) / 3 * 1e3
+        cpu_same = bool(np.array_equal(out_map[sample], gain))
     ms = statistics.median(ours)
     by = n_cand * (d + 1) * 4 + n_univ * 4
     out.update({"n_cand": n_cand, "d": d, "n_univ": n_univ,
@@ -99,6 +114,13 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True):
                 "ms_rounds_8_ctas_per_sm": [round(x, 4) for x in wide],
                 "GBps": round(by / (ms * 1e-3) / 1e9, 1),
                 "algorithmic_bytes_per_field": by})
+    if cpu_ms is not None:
+        out["cpu_baseline"] = {
+            "value": round(by / (cpu_ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+            "cores": os.cpu_count(), "kind": "port",
+            "sample": f"3 gain fields of {out['design']}, C restatement on "
+                      f"all host threads, {cpu_ms:.1f} ms each",
+            "same_gain_sample": cpu_same}
     if theirs:
         rms = statistics.median(theirs)
         out["reference_plugin"] = {

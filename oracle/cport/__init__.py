@@ -37,7 +37,20 @@ def lib():
                                       ctypes.c_int, ctypes.c_int, P]
         _lib.cc_seed_code.argtypes = [P, ctypes.c_longlong, ctypes.c_longlong,
                                       P]
+        _lib.cc_inc_field.argtypes = [P, ctypes.c_longlong, ctypes.c_int, P,
+                                      ctypes.c_int, ctypes.c_int, P]
     return _lib
+
+
+def inc_field(inc, cnt, target, mu=1, out=None):
+    """Field over dense incidence rows on the host threads (the reference's
+    SparseIncidenceBackend field, incidence.py:160-197)."""
+    inc = np.ascontiguousarray(inc, dtype=np.int32)
+    cnt = np.ascontiguousarray(cnt, dtype=np.int32)
+    out = np.empty(len(inc), dtype=np.int32) if out is None else out
+    lib().cc_inc_field(inc.ctypes.data, len(inc), inc.shape[1],
+                       cnt.ctypes.data, int(target), int(mu), out.ctypes.data)
+    return out
 
 
 class CPortCell:

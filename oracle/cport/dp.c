@@ -165,3 +165,22 @@ void cc_seed_code(const long long *code, long long M, long long X,
   memset(A, 0, sizeof(int32_t) * X);
   for (long long i = 0; i < M; i++) A[code[i]]++;
 }
+
+/* Explicit incidence (coldcore src/coldcore/incidence.py:160-220): the
+ * field over dense rows, map[c] = #{u in row c : role(cnt[u])} with role 0
+ * deficient (cnt < mu), 1 critical (1 <= cnt <= mu), other targets the
+ * literal cnt == target; rows split over the host threads. */
+void cc_inc_field(const int32_t *inc, long long ncand, int d,
+                  const int32_t *cnt, int target, int mu, int32_t *map) {
+#pragma omp parallel for schedule(static)
+  for (long long c = 0; c < ncand; c++) {
+    const int32_t *row = inc + c * d;
+    int32_t s = 0;
+    for (int j = 0; j < d; j++) {
+      const int v = cnt[row[j]];
+      s += target == 0 ? v < mu : target == 1 ? (v >= 1 && v <= mu)
+                                              : v == target;
+    }
+    map[c] = s;
+  }
+}

@@ -41,3 +41,16 @@ def test_campaign_pool_runs_every_cell():
     rate, wall, busy, workers = campaign_rate(cells, workers=2)
     assert workers == 2 and wall > 0 and busy > 0
     assert rate == pytest.approx(len(cells) / wall)
+
+
+def test_incidence_field_port_equals_the_oracle():
+    from oracle.cport import inc_field
+    from oracle.incidence_oracle import IncidenceOracle
+    rng = np.random.default_rng(3)
+    for d in (1, 6, 33):
+        inc = np.stack([rng.choice(90, d, replace=False) for _ in range(200)])
+        o = IncidenceOracle(inc, 90, mu=2)
+        o.recount(rng.choice(200, 30, replace=False))
+        for t in (0, 1, 3):
+            o.field(t)
+            assert np.array_equal(inc_field(inc, o.cnt, t, mu=2), o.map)
