@@ -5,11 +5,12 @@ One step = a gain field and a loss field over every candidate of C(v,k,t)
 27,405 universe elements) after a recount of a seeded solution, the
 incidence built on the device.  Reported per field: milliseconds, and GB/s
 of its algorithmic bytes (the incidence read once, the map written once,
-cnt read once), with the reference's own ABI-2 kernels
-(``oracle/_ref/libref_sparse.so``, built from ``src/plugins/sparse/
-sparse.cu``) on the same incidence when that library is present.
+cnt read once).  Given another ABI-2 library (``--ref PATH``, e.g. the
+reference's own ``src/plugins/sparse/sparse.cu`` built for sm_100a), its
+kernels are timed in alternation on the same incidence.
 
     python -m coldcore_b200.incidence_bench [--v 30 --k 8 --t 4 --reps 20]
+                                            [--ref PATH]
 """
 import argparse
 import json
@@ -19,8 +20,6 @@ import time
 
 import numpy as np
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.path.join(ROOT, "oracle", "_ref", "libref_sparse.so")
 
 
 def _warm(b, seconds=0.3):
@@ -46,7 +45,7 @@ def _time_fields(b, stream, reps):
     return e0.elapsed_time(e1) / (2 * reps)
 
 
-def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True,
+def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
             cpu_field=None):
     """Both cells stay resident and are timed in alternation, `rounds`
     times each after a warm-up; the medians are reported.  ``cpu_field``
@@ -66,8 +65,8 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True,
         host_rows = b.rows()
         host_cnt = b.read_cnt().astype(np.int32)
         ref = None
-        if with_ref and os.path.exists(REF):
-            ref = GpuIncidenceBackend(host_rows, n_univ, plugin_path=REF)
+        if ref_path:
+            ref = GpuIncidenceBackend(host_rows, n_univ, plugin_path=ref_path)
         try:
             if ref is not None:
                 ref.recount(sol)
@@ -124,8 +123,7 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, with_ref=True,
     if theirs:
         rms = statistics.median(theirs)
         out["reference_plugin"] = {
-            "library": "oracle/_ref/libref_sparse.so (reference "
-                       "src/plugins/sparse/sparse.cu, nvcc -O3 sm_100a)",
+            "library": os.path.basename(ref_path),
             "ms_per_field": round(rms, 4),
             "ms_rounds": [round(x, 4) for x in theirs],
             "GBps": round(by / (rms * 1e-3) / 1e9, 1),
@@ -140,9 +138,10 @@ def main():
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--t", type=int, default=4)
     ap.add_argument("--reps", type=int, default=20)
-    ap.add_argument("--no-ref", action="store_true")
+    ap.add_argument("--ref", default=None,
+                    help="another ABI-2 library to time beside the engine")
     a = ap.parse_args()
-    print(json.dumps(measure(a.v, a.k, a.t, a.reps, with_ref=not a.no_ref)))
+    print(json.dumps(measure(a.v, a.k, a.t, a.reps, ref_path=a.ref)))
 
 
 if __name__ == "__main__":
