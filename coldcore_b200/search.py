@@ -9,7 +9,10 @@ This module restates the part of coldcore's search core
 * ``peel``: zero-loss removal in independent batches (search.py:621-670);
 * ``lns``: fixed-M LNS with ``select="fixed"`` (the record mix) or
   ``"adaptive"`` (:class:`OperatorBandit`), search.py:672-784;
-* ``descend``: the notch ladder, v0.2 schedule (search.py:1757-1918).
+* ``descend``: the notch ladder, v0.2 schedule (search.py:1757-1918);
+* ``anneal``: the swap-neighbourhood polish at fixed M (LAHC or
+  Metropolis), over the "pool" or the local "shell" neighbourhood,
+  costed exactly by the backend's ``swap_eval`` (search.py:787-1360).
 
 The random draws happen in the reference's order, so with a backend whose
 ``map_extract`` returns ascending indices (the CPU backends) a seeded run
@@ -53,6 +56,12 @@ FIXED_DRAW_DEFICIT = FIXED_DRAW + ("deficit", "deficit")
 #: scan of cnt (search.py:80-81)
 DEFICIT_WORDS = 4
 SCAN_CHUNK = 1 << 24
+#: shell-polish defaults (search.py:70-90): sampled distance-2 words,
+#: top-of-gain draws and uniform draws per move, the cheapest incumbents
+#: a move drops from, the top-gain pool cap and the pool-neighbourhood cap
+SHELL2, SHELL_TOP, SHELL_RAND, SHELL_TOPK = 128, 48, 8, 24
+SHELL_POOL_CAP = 4096
+POOL_CAP = 1 << 14
 
 
 def _rng_for(seed):
@@ -159,6 +168,8 @@ class Searcher:
                       "learned_rounds": 0, "fallback_rounds": 0}
         self._scan_off = 0                 # rotating start of the cnt scan
         self._deficit_cache = (None, None)
+        self._sh1 = None                   # per-axis shell displacements
+        self.stats.update({"moves": 0})
 
     # ------------------------------------------------ state
     def time_left(self):
@@ -631,3 +642,370 @@ class Searcher:
                 step = max(1, step // 2)
                 self.load(solved)
         return M
+
+    # ------------------------------------------------ polish at fixed M
+    def _rng_pass(self, seed):
+        """The stream a pass draws from: the searcher's own, or a fresh
+        one for an explicit seed (search.py:214-229)."""
+        return self.rng if seed is None else _rng_for(seed)
+
+    def _gain_pool(self):
+        """Every word of positive exact gain, up to the pool cap
+        (search.py:787-799)."""
+        self.b.gain_map()
+        self.stats["transforms"] += 1
+        if self.b.map_max() <= 0:
+            return np.zeros(0, dtype=np.int64)
+        cap = min(POOL_CAP, self.b.extract_cap)
+        idx, _v, _f = self.b.map_extract(1, cap=cap)
+        return np.asarray(idx, dtype=np.int64)
+
+    def _top_gain_pool(self, work, cap=SHELL_POOL_CAP):
+        """The top of the gain map, at the histogram threshold that keeps
+        about ``cap`` words, minus the incumbents (search.py:871-902)."""
+        b = self.b
+        b.gain_map()
+        self.stats["transforms"] += 1
+        mx = b.map_max()
+        if mx <= 0:
+            return np.zeros(0, dtype=np.int64)
+        thr = 1
+        if mx > 1 and getattr(b, "supports_hist", True):
+            hist = b.map_hist(1024, mx)
+            csum = np.cumsum(hist[::-1])[::-1]
+            good = np.flatnonzero(csum <= cap)
+            if len(good):
+                thr = max(1, int(good[0]) * mx // 1024 + 1)
+        idx, _v, _f = b.map_extract(thr, cap=min(cap, b.extract_cap))
+        idx = np.asarray(idx, dtype=np.int64)
+        return idx[~np.isin(idx, work)] if len(idx) else idx
+
+    def _shell1(self, idx):
+        """Every word at digit distance 1 from ``idx`` (one coordinate to
+        every other value), or the backend's own radius-1 neighbours
+        (search.py:818-852)."""
+        nb = getattr(self.b, "neighbours", None)
+        if nb is not None:
+            return np.asarray(nb(int(idx), 1), dtype=np.int64)
+        sp = self.b.space
+        if self._sh1 is None:
+            self._sh1 = []
+            for p in range(sp.n):
+                a, pw = int(sp.axes[p]), int(sp.pow_q[p])
+                v = np.arange(a, dtype=np.int64)
+                self._sh1.append(np.stack([(v[v != d] - d) * pw
+                                           for d in range(a)]))
+        d = (idx // np.asarray(sp.pow_q)) % np.asarray(sp.axes, dtype=np.int64)
+        out = [idx + self._sh1[p][d[p]] for p in range(sp.n)]
+        return np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
+
+    def _shell_k(self, idx, k, m, rng):
+        """``m`` sampled words at digit distance <= k (search.py:854-869)."""
+        nb = getattr(self.b, "neighbours", None)
+        if nb is not None:
+            return np.asarray(nb(int(idx), k, m, rng), dtype=np.int64)
+        sp = self.b.space
+        if m <= 0 or k <= 0 or k > sp.n:
+            return np.zeros(0, dtype=np.int64)
+        ax = np.asarray(sp.axes, dtype=np.int64)
+        pw = np.asarray(sp.pow_q, dtype=np.int64)
+        movable = np.flatnonzero(ax > 1)
+        if not len(movable):
+            return np.zeros(0, dtype=np.int64)
+        out = np.full(m, idx, dtype=np.int64)
+        for _ in range(k):
+            p = movable[rng.integers(0, len(movable), size=m)]
+            a = ax[p]
+            v = rng.integers(0, a - 1)
+            cur = (out // pw[p]) % a
+            v = v + (v >= cur)                   # skip the current digit
+            out = out + (v - cur) * pw[p]
+        return out
+
+    def _polish_start(self, M):
+        """Trim or fill to M words and reset the best snapshot."""
+        if len(self.code) > M:
+            self.ruin(len(self.code) - M, "low")
+        if len(self.code) < M and self.uncov > 0:
+            self.greedy_fill(M)
+        self.best_uncov = self.best_code = None
+        self._snapshot()
+
+    def anneal(self, M, budget_s, mode="lahc", t0=1.0, t_end=0.05,
+               lahc_len=50, pool_refresh=64, sample=8, seed=None,
+               log_every=0, neighbourhood="pool", n_shell2=SHELL2,
+               n_top=SHELL_TOP, n_rand=SHELL_RAND, w_topk=SHELL_TOPK,
+               w_random_p=0.25, greedy_p=0.5, loss_refresh=48,
+               restart_stale=15000, verify_every=1):
+        """Swap-neighbourhood polish at fixed M that accepts regressions
+        (search.py:1091-1235).  A move drops one incumbent and adds one
+        candidate, costed exactly: uncov + loss(w) - gain(v | w removed).
+        ``mode`` "lahc" (late acceptance over ``lahc_len`` moves) or
+        "anneal" (Metropolis, geometric cooling ``t0`` -> ``t_end`` over
+        the budget).  ``neighbourhood`` "pool": the cheapest of ``sample``
+        random incumbents against the best of ``sample`` draws from the
+        positive-gain pool; "shell": one of the ``w_topk`` cheapest
+        incumbents against its whole distance-1 shell, sampled distance-2
+        words, top-of-gain and uniform draws, all costed in one
+        ``swap_eval``.  Returns the final uncovered count."""
+        if mode not in ("anneal", "lahc"):
+            raise ValueError(f"unknown polish mode: {mode!r}")
+        if neighbourhood not in ("pool", "shell"):
+            raise ValueError(f"unknown neighbourhood: {neighbourhood!r}")
+        if int(pool_refresh) < 1:
+            raise ValueError("pool_refresh must be >= 1")
+        saved = self.rng
+        self.rng = rng = self._rng_pass(seed)
+        try:
+            self.stats["polish_neighbourhood"] = neighbourhood
+            if neighbourhood == "shell":
+                return self._shift_anneal(
+                    M, budget_s, mode, t0, t_end, lahc_len,
+                    int(pool_refresh), log_every, rng, n_shell2, n_top,
+                    n_rand, w_topk, w_random_p, greedy_p, loss_refresh,
+                    restart_stale, verify_every)
+            return self._pool_anneal(M, budget_s, mode, t0, t_end, lahc_len,
+                                     int(pool_refresh), sample, log_every,
+                                     rng)
+        finally:
+            self.rng = saved
+
+    def _accept_many(self, costs, uncov, bound, mode, t0, t_end, elapsed,
+                     budget_s, rng):
+        if mode == "lahc":
+            return np.flatnonzero(costs <= max(bound, uncov))
+        temp = t0 * (t_end / t0) ** min(1.0, elapsed / max(budget_s, 1e-9))
+        dl = (costs - uncov).astype(np.float64)
+        return np.flatnonzero((dl <= 0) | (rng.random(len(dl)) < np.exp(
+            -np.maximum(dl, 0.0) / max(temp, 1e-9))))
+
+    def _pool_anneal(self, M, budget_s, mode, t0, t_end, lahc_len, period,
+                     sample, log_every, rng):
+        """The "pool" neighbourhood (search.py:1237-1360)."""
+        b = self.b
+        self._polish_start(M)
+        if self.uncov == 0 or not len(self.code):
+            return self.uncov
+        work = np.asarray(self.code, dtype=np.int64).copy()
+        codeset = set(work.tolist())
+        pool = np.zeros(0, dtype=np.int64)
+        since_refresh, starved = period, 0
+        hist = [float(self.uncov)] * max(1, int(lahc_len))
+        t_start = time.time()
+        i = moves = accepts = 0
+        while self.uncov > 0:
+            elapsed = time.time() - t_start
+            if elapsed > budget_s or self.time_left() < self.loop_reserve_s:
+                break
+            if since_refresh >= period or not len(pool):
+                self.code = work
+                pool = self._gain_pool()
+                exact = b.uncovered()
+                if exact != self.uncov:
+                    self.on_log(f"WARNING drift: incremental {self.uncov} "
+                                f"!= field {exact}; adopting field")
+                    self.uncov = exact
+                since_refresh = 0
+                if not len(pool):
+                    break
+            # drop: the cheapest of `sample` random incumbents
+            ns = min(sample, len(work))
+            ridx = rng.choice(len(work), size=ns, replace=False)
+            loss = b.ball_gather(work[ridx], 1).astype(np.float64)
+            j = int(np.argmin(loss + rng.random(ns)))
+            slot = int(ridx[j])
+            w = int(work[slot])
+            wa = np.array([w], dtype=np.int64)
+            b.ball_update(wa, -1)
+            codeset.discard(w)
+            # add: the best of `sample` pool draws, exact gains
+            ns = min(sample, len(pool))
+            draw = pool[rng.integers(0, len(pool), size=ns)]
+            cand = np.array([c for c in draw.tolist()
+                             if c != w and c not in codeset], dtype=np.int64)
+            if not len(cand):                    # stale pool exhausted
+                b.ball_update(wa, +1)
+                codeset.add(w)
+                since_refresh = period
+                pool = np.zeros(0, dtype=np.int64)
+                starved += 1
+                if starved > 2:
+                    break
+                continue
+            starved = 0
+            gain = b.ball_gather(cand, 0).astype(np.float64)
+            g = int(np.argmax(gain + rng.random(len(gain))))
+            v = int(cand[g])
+            b.ball_update(np.array([v], dtype=np.int64), +1)
+            cost = self.uncov + int(loss[j]) - int(gain[g])
+            moves += 1
+            if mode == "lahc":
+                ok = cost <= hist[i % len(hist)] or cost <= self.uncov
+            else:
+                delta = cost - self.uncov
+                temp = t0 * (t_end / t0) ** min(
+                    1.0, elapsed / max(budget_s, 1e-9))
+                ok = delta <= 0 or rng.random() < np.exp(
+                    -delta / max(temp, 1e-9))
+            if ok:
+                work[slot] = v
+                codeset.add(v)
+                self.uncov = cost
+                accepts += 1
+                since_refresh += 1
+                self.code = work
+                self._snapshot()
+            else:
+                b.ball_update(np.array([v], dtype=np.int64), -1)
+                b.ball_update(wa, +1)
+                codeset.add(w)
+            if mode == "lahc":
+                hist[i % len(hist)] = float(self.uncov)
+            i += 1
+            if log_every and i % log_every == 0:
+                self.on_log(f"{mode} M={M} move={i} acc={accepts} "
+                            f"uncov={self.uncov} best={self.best_uncov}")
+        self.stats["moves"] += moves
+        self.stats["accepts"] += accepts
+        return self._polish_end(np.sort(work))
+
+    def _polish_end(self, code):
+        """Adopt the final or the best state, recounted exactly."""
+        self.code = code
+        if self.uncov == 0:
+            self._snapshot()
+        elif self.best_code is not None and self.best_uncov < self.uncov:
+            self.code = np.sort(self.best_code)
+            self.b.recount(self.code)
+            self.stats["transforms"] += 1
+            self.uncov = self.b.uncovered()
+        return self.uncov
+
+    def _shift_anneal(self, M, budget_s, mode, t0, t_end, lahc_len, period,
+                      log_every, rng, n_shell2, n_top, n_rand, w_topk,
+                      w_random_p, greedy_p, loss_refresh, restart_stale,
+                      verify_every):
+        """The "shell" neighbourhood (search.py:904-1089)."""
+        from .gpu import swap_eval_generic
+        b = self.b
+        swap_eval = getattr(b, "swap_eval", None) or (
+            lambda d, c: swap_eval_generic(b, d, c))
+        self._polish_start(M)
+        if self.uncov == 0 or not len(self.code):
+            return self.uncov
+        work = np.sort(np.asarray(self.code, dtype=np.int64)).copy()
+        M = len(work)
+        self.code = work
+        uncov = int(self.uncov)
+        best_u, best_code = uncov, work.copy()
+        losses = self.losses().astype(np.int64)
+        pool = self._top_gain_pool(work)
+        t_start = time.time()
+        since_pool = since_loss = 0
+        hist = [float(uncov)] * max(1, int(lahc_len))
+        i = moves = accepts = drift = stale = 0
+        last_slot = -1
+        while uncov > 0:
+            elapsed = time.time() - t_start
+            if elapsed > budget_s or self.time_left() < self.loop_reserve_s:
+                break
+            # the word to move: one of the cheapest by exact loss, or now
+            # and then a uniform one
+            if rng.random() < w_random_p or len(losses) != M:
+                slot = int(rng.integers(M))
+            else:
+                k = min(int(w_topk), M)
+                cheap = np.argpartition(losses, k - 1)[:k]
+                slot = int(cheap[rng.integers(k)])
+            if slot == last_slot and M > 1:
+                slot = int(rng.integers(M))
+            w = int(work[slot])
+            wa = np.array([w], dtype=np.int64)
+            # candidates that can plug the hole w would leave
+            parts = [self._shell1(w)]
+            if n_shell2:
+                parts.append(self._shell_k(w, 2, int(n_shell2), rng))
+            if n_top and len(pool):
+                parts.append(pool[rng.integers(0, len(pool),
+                                               size=min(int(n_top),
+                                                        len(pool)))])
+            if n_rand:
+                parts.append(rng.integers(0, b.space.size, size=int(n_rand))
+                             .astype(np.int64))
+            cand = np.unique(np.concatenate(parts))
+            cand = cand[(cand != w) & ~np.isin(cand, work)]
+            if not len(cand):
+                i += 1
+                continue
+            # the drop and the whole batch, costed in one read-only call
+            lw_a, g_l = swap_eval(wa, [cand])
+            lw = int(lw_a[0])
+            gains = np.asarray(g_l[0]).astype(np.int64)
+            costs = uncov + lw - gains
+            moves += 1
+            ok = self._accept_many(costs, uncov, hist[i % len(hist)], mode,
+                                   t0, t_end, elapsed, budget_s, rng)
+            if len(ok):
+                if rng.random() < greedy_p:
+                    sub = ok[costs[ok] == costs[ok].min()]
+                    pick = int(sub[rng.integers(len(sub))])
+                else:
+                    pick = int(ok[rng.integers(len(ok))])
+                v = int(cand[pick])
+                b.ball_update(wa, -1)
+                b.ball_update(np.array([v], dtype=np.int64), +1)
+                work[slot] = v
+                uncov = int(costs[pick])
+                accepts += 1
+                since_pool += 1
+                since_loss += 1
+                last_slot = slot
+                if verify_every and accepts % verify_every == 0:
+                    exact = b.uncovered()
+                    if exact != uncov:
+                        drift += 1
+                        uncov = exact
+                if uncov < best_u:
+                    best_u, best_code = uncov, work.copy()
+                    stale = 0
+                    self.code, self.uncov = work, uncov
+                    self._snapshot()
+                    if uncov == 0:
+                        break
+            else:
+                last_slot = -1
+            if mode == "lahc":
+                hist[i % len(hist)] = float(uncov)
+            i += 1
+            stale += 1
+            if restart_stale and stale >= restart_stale:
+                # back to the best state, acceptance history restarted
+                work = best_code.copy()
+                b.recount(work)
+                self.stats["transforms"] += 1
+                uncov = b.uncovered()
+                hist = [float(uncov)] * len(hist)
+                losses = self.losses().astype(np.int64)
+                pool = self._top_gain_pool(work)
+                since_pool = since_loss = stale = 0
+                last_slot = -1
+                continue
+            if since_pool >= period:
+                pool = self._top_gain_pool(work)
+                since_pool = 0
+            if since_loss >= loss_refresh:
+                self.code = work
+                losses = self.losses().astype(np.int64)
+                since_loss = 0
+            if log_every and i % log_every == 0:
+                self.on_log(f"shift M={M} move={i} acc={accepts} "
+                            f"uncov={uncov} best={best_u}")
+        self.stats["moves"] += moves
+        self.stats["accepts"] += accepts
+        self.stats["shift_drift"] = self.stats.get("shift_drift", 0) + drift
+        self.code = np.sort(best_code if best_u < uncov else work)
+        b.recount(self.code)
+        self.stats["transforms"] += 1
+        self.uncov = b.uncovered()
+        self._snapshot()
+        return self.uncov

@@ -33,6 +33,7 @@ class Space:
         for j in range(1, self.n):
             self.pow[j] = self.pow[j - 1] * self.axes[j - 1]
         self.size = int(self.pow[-1] * self.axes[-1])
+        self.pow_q = self.pow                # the reference's name
 
     def digits(self, idx):
         idx = np.asarray(idx, dtype=np.int64).ravel()

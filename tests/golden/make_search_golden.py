@@ -21,6 +21,11 @@ ascending indices, so a seeded run is deterministic):
 Output: ``search_traces.json`` (committed; nothing at test time reads the
 reference).
 
+With ``--anneal`` it writes ``search_anneal_traces.json``: the
+swap-neighbourhood polish ``anneal(M, ..., mode="lahc")`` over the
+"pool" and "shell" neighbourhoods, one notch below the peeled size (a run
+that does not solve within its budget is marked ``"solved": false``).
+
 With ``--deficit`` it writes ``search_deficit_traces.json`` instead: the
 opt-in deficit-targeted ruin (``ruin(k, "deficit")`` after three ``low``
 removals, so that words are uncovered) and ``lns(..., deficit=True)``
@@ -130,8 +135,34 @@ def main_deficit():
         json.dump(out, f)
 
 
+def main_anneal():
+    out = []
+    for problem, axes, R, mu, seed in CELLS:
+        runs = {}
+        for nb in ("pool", "shell"):
+            t = built(problem, axes, R, mu, seed)
+            t.peel()
+            M = len(t.code) - 1
+            t.ruin(1, "low")
+            unc = t.anneal(M, 30.0, mode="lahc", neighbourhood=nb,
+                           log_every=0)
+            runs[nb] = {"M": M, "uncov": int(unc), "solved": unc == 0,
+                        "moves": int(t.stats["moves"]),
+                        "accepts": int(t.stats["accepts"]),
+                        "code": t.code.tolist()}
+        out.append({"problem": problem, "axes": axes, "R": R, "mu": mu,
+                    "seed": seed, "anneal": runs})
+        print(problem, axes, R, mu,
+              {k: (v["uncov"], v["moves"], v["accepts"])
+               for k, v in runs.items()}, flush=True)
+    with open(os.path.join(HERE, "search_anneal_traces.json"), "w") as f:
+        json.dump(out, f)
+
+
 if __name__ == "__main__":
     if "--deficit" in sys.argv:
         main_deficit()
+    elif "--anneal" in sys.argv:
+        main_anneal()
     else:
         main()
