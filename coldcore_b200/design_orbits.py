@@ -412,6 +412,9 @@ def orbit_search(v, k, t, group, budget_s=60.0, mu=1, seed=1,
 
     s = Searcher(q, seed=seed, deadline=time.time() + budget_s + reserve_s,
                  on_solved=solved)
+    # the reserve kept back from the deadline bounds the searcher's own
+    s.build_reserve_s = min(s.build_reserve_s, reserve_s)
+    s.loop_reserve_s = min(s.loop_reserve_s, reserve_s)
     try:
         s.load(np.zeros(0, dtype=np.int64))
         s.greedy_fill(10 ** 9)
@@ -424,3 +427,36 @@ def orbit_search(v, k, t, group, budget_s=60.0, mu=1, seed=1,
         if hasattr(q, "close"):
             q.close()
     return best["blocks"], s, q
+
+
+def release(v, k, t, blocks, budget_s, mu=1, seed=1, floor=1,
+            notch_budget_s=None, backend=None, reserve_s=30.0, step0=4):
+    """Free polish of a structured start (design_orbits.py:270-298): a
+    plain searcher on the full design (the engine's
+    ``GpuCoveringDesignBackend`` unless another class with the signature
+    (v, k, t, mu=...) is given) starts from the expanded blocks and runs
+    the notch descent.  Returns ``(blocks, searcher)``."""
+    from .search import Searcher
+    if backend is None:
+        from .incidence import GpuCoveringDesignBackend as backend
+    b = backend(v, k, t, mu=mu)
+    best = {"blocks": np.asarray(blocks, dtype=np.int64)}
+
+    def solved(M, idx):
+        best["blocks"] = np.asarray(idx, dtype=np.int64).copy()
+
+    s = Searcher(b, seed=seed, deadline=time.time() + budget_s + reserve_s,
+                 on_solved=solved)
+    s.build_reserve_s = min(s.build_reserve_s, reserve_s)
+    s.loop_reserve_s = min(s.loop_reserve_s, reserve_s)
+    try:
+        s.load(best["blocks"])
+        if s.uncov != 0:
+            raise ValueError("released solution is not feasible")
+        nb = notch_budget_s or max(1.0, budget_s / 6)
+        s.descend(floor=floor, notch_budget_s=nb, step0=step0,
+                  reserve_s=reserve_s, min_notch_s=min(20.0, nb))
+    finally:
+        if hasattr(b, "close"):
+            b.close()
+    return best["blocks"], s

@@ -122,3 +122,32 @@ def test_orbit_search_reaches_optimum(v, k, t, spec, opt):
     assert len(blocks) == opt
     assert DesignOracle(v, k, t).verify(blocks)
     assert comb(v, k) >= len(blocks)
+
+
+def test_release_keeps_feasibility_and_size():
+    from coldcore_b200.design_orbits import release
+    blocks, s, q = orbit_search(13, 4, 2, "cyclic", budget_s=5, seed=1,
+                                notch_budget_s=2, reserve_s=0.0,
+                                backend=WeightedIncidenceOracle)
+    rel, s2 = release(13, 4, 2, blocks, 5, seed=1, notch_budget_s=2, step0=1,
+                      reserve_s=0.0, backend=DesignOracle)
+    assert len(rel) <= len(blocks) == 13
+    assert DesignOracle(13, 4, 2).verify(rel)
+
+
+def test_free_greedy_c24_8_5_is_759():
+    """The exact greedy over all 735,471 blocks of C(24,8,5) finds the
+    759-block Steiner system S(5,8,24) (the reference's case,
+    tests/test_design_orbits.py:185-190)."""
+    from coldcore_b200.design_orbits import design_rows
+    from coldcore_b200.search import Searcher
+    from oracle.incidence_oracle import IncidenceOracle
+    b = IncidenceOracle(design_rows(24, 8, 5), comb(24, 5))
+    s = Searcher(b, seed=1)
+    s.build_reserve_s = s.loop_reserve_s = 0.0
+    s.load(np.zeros(0, dtype=np.int64))
+    assert s.greedy_fill(10 ** 9) == 0
+    assert len(s.code) == 759
+    cnt = np.zeros(comb(24, 5), dtype=np.int64)
+    np.add.at(cnt, b.inc[s.code].ravel(), 1)
+    assert (cnt == 1).all()                      # every 5-set exactly once
