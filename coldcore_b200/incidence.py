@@ -595,3 +595,17 @@ class GpuCoveringDesignBackend(GpuIncidenceBackend):
         return (f"{type(self).__name__}(C({self.v},{self.k},{self.t}), "
                 f"mu={self.mu}, n_cand={self.n_cand}, d={self.d}, "
                 f"n_univ={self.n_univ})")
+
+
+def CoveringDesignBackend(v, k, t, mu=1, device="gpu", **kw):
+    """coldcore's constructor name for a design cell
+    (``problems/covering_design.py:174-191``).  This engine serves the
+    device form only: ``device="gpu"`` gives a
+    :class:`GpuCoveringDesignBackend`; the reference's host forms ("cpu",
+    "ref") are its numpy backends, which this package does not ship."""
+    if device != "gpu":
+        raise ValueError(f"device {device!r}: this engine has the GPU form "
+                         "only (the host forms are coldcore's own numpy "
+                         "backends)")
+    kw.pop("keep_host", None)
+    return GpuCoveringDesignBackend(v, k, t, mu=mu, **kw)

@@ -124,3 +124,11 @@ def test_python_mirror_validates_like_the_reference():
     assert s.word_index(s.index_word([3, 4])).tolist() == [3, 4]
     with pytest.raises(ValueError):
         IncidenceSpace(0)
+
+
+def test_design_constructor_name_serves_the_gpu_form_only():
+    from coldcore_b200.incidence import CoveringDesignBackend
+    with pytest.raises(ValueError):
+        CoveringDesignBackend(7, 3, 2, device="cpu")
+    with pytest.raises(ValueError):
+        CoveringDesignBackend(7, 3, 2, device="ref")
