@@ -119,25 +119,32 @@ class Clocks:
         except Exception:
             self.proc.kill()
             return None
-        sm, mx, reasons = [], None, set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
-                 "sw_power_cap")
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for k, name in enumerate(names):
-                if f[5 + k].lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return parse_clock_samples(out)
+
+
+def parse_clock_samples(text):
+    """nvidia-smi samples (the Clocks.FIELDS columns, csv, no header, no
+    units) -> median SM clock, max clock and every throttle reason seen
+    active; None without a usable sample."""
+    sm, mx, reasons = [], None, set()
+    names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+             "sw_power_cap")
+    for line in text.strip().splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = float(f[2])
+        except ValueError:
+            continue
+        for k, name in enumerate(names):
+            if f[5 + k].lower().startswith("active"):
+                reasons.add(name)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(sm)}
 
 
 # ---------------------------------------------------------------- CPU arm
