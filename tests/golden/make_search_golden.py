@@ -35,8 +35,6 @@ import json
 import os
 import sys
 
-import numpy as np
-
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.environ.get("COLDCORE_REF_SRC", "/root/reference/src"))
 
