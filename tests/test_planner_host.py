@@ -6,6 +6,7 @@ the conditions the kernels index under, so a plan that broke one would read
 or write out of place on the device."""
 import math
 
+import numpy as np
 import pytest
 
 from coldcore_b200.gpu import plan_probe
@@ -167,3 +168,40 @@ def test_wide_window_cells_have_no_groups_and_bad_args_raise():
         plan_probe("hamming", [17, 2], 1, 1, 1)          # axis above 16
     with pytest.raises(RuntimeError):
         plan_probe("hamming", [2] * 4, 1, 1, 1, budget_kb=8)
+
+
+N_FUZZ = 300
+
+
+def test_planner_fuzz():
+    """Seeded random geometries (mixed radix, every family, up to 2^34
+    words): the same invariants on every plan."""
+    rng = np.random.default_rng(2026)
+    checked = 0
+    for _ in range(N_FUZZ):
+        problem = str(rng.choice(["hamming", "hamming", "lee", "torus_linf",
+                                  "grid_linf"]))
+        n = int(rng.integers(1, 13))
+        if problem == "torus_linf":
+            R = int(rng.integers(1, 3))
+            axes = [int(a) for a in rng.integers(2 * R + 1, 17, n)]
+        elif problem == "grid_linf":
+            R = int(rng.integers(1, 4))
+            axes = [int(a) for a in rng.integers(2, 17, n)]
+        else:
+            R = int(rng.integers(1, 8))
+            q = int(rng.integers(2, 17))
+            axes = ([q] * n if rng.random() < 0.6
+                    else [int(a) for a in rng.integers(2, 17, n)])
+        if math.prod(axes) > 1 << 34:
+            continue
+        layered = problem in ("hamming", "lee")
+        modes = MODES if layered else [m for m in MODES if m[1] != 3]
+        mode = modes[int(rng.integers(len(modes)))]
+        budget, pipe = KNOBS[int(rng.integers(len(KNOBS)))]
+        half = bool(rng.random() < 0.7)
+        plan = plan_probe(problem, axes, R, *mode, budget_kb=budget,
+                          pipe=pipe, half=half)
+        check_plan(plan, problem, axes, R, mode, budget, pipe, half)
+        checked += 1
+    assert checked > N_FUZZ * 0.8
