@@ -82,7 +82,8 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
             os.environ["CC_SPARSE_BLOCKS_PER_SM"] = "8"
             try:
                 _warm(b, 0.1)
-                wide = [_time_fields(b, stream, reps) for _ in range(rounds)]
+                one_wave = [_time_fields(b, stream, reps)
+                            for _ in range(rounds)]
             finally:
                 os.environ.pop("CC_SPARSE_BLOCKS_PER_SM", None)
             b.gain_map()
@@ -110,7 +111,7 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
                 "incidence_gb": round(n_cand * d * 4 / 1e9, 3),
                 "solution": len(sol), "ms_per_field": round(ms, 4),
                 "ms_rounds": [round(x, 4) for x in ours],
-                "ms_rounds_8_ctas_per_sm": [round(x, 4) for x in wide],
+                "ms_rounds_8_ctas_per_sm": [round(x, 4) for x in one_wave],
                 "GBps": round(by / (ms * 1e-3) / 1e9, 1),
                 "algorithmic_bytes_per_field": by})
     if cpu_ms is not None:
