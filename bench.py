@@ -392,6 +392,17 @@ def measure_batch_small(args):
                         "instances_per_s": round(len(cells) / dt, 1)}
     out["speedup"] = round(out["persistent"]["instances_per_s"]
                            / out["per_pass_launches"]["instances_per_s"], 2)
+    if not args.no_cpu:
+        from oracle.cport import campaign_rate     # the CPU baseline leg
+        rate, wall, busy, workers = campaign_rate(cells)
+        out["cpu_baseline"] = {
+            "value": round(rate, 2), "unit": "instances/s", "cores": workers,
+            "kind": "port",
+            "sample": f"all {len(cells)} cells, one step each, C restatement, "
+                      f"{workers} single-threaded spawned worker processes: "
+                      f"{wall:.1f} s wall, {busy:.1f} s busy"}
+        out["speedup_vs_cpu"] = round(
+            out["persistent"]["instances_per_s"] / rate, 1)
     return out
 
 
