@@ -90,15 +90,30 @@ struct GroupPlan {
 
 // planner.cu: schedule knobs and the group plan of one transform
 // pipe: see plan_groups; half: 16-bit planes between the launches
-struct Knobs { size_t budget; int pipe; int half = 0; };
+// pair: allow the pair first group (binary Hamming, 16-bit planes)
+struct Knobs { size_t budget; int pipe; int half = 0; int pair = 1; };
 struct PlanPtrs {
   int32_t *layers; long long plane; uint16_t *cnt;
   const long long *code; long long ncode; int32_t *map;
   uint16_t *layers16 = nullptr;   // u16 plane region (Knobs::half)
 };
+// An axis range of one transform: the launches cover axes [begin, end) of
+// g (end < 0: through the last axis).  reach0 is the distance reach of axes
+// applied by an earlier range (so the live layers at axis j are
+// min(reach0 + reach of axes [begin, j), R) + 1); `final` is false when
+// the range's layers feed a later range, which keeps the last launch's
+// plane width (16-bit planes) and writes only its live layers.
+struct AxisRange {
+  int begin = 0;
+  int end = -1;
+  long long reach0 = 0;
+  bool final = true;
+};
 std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
                                    const PlanPtrs &ptr, int src, int dst,
-                                   Knobs kn);
+                                   Knobs kn, AxisRange range = AxisRange());
+// distance reach of one axis: 1 for Hamming, floor(a/2) for Lee
+inline long long axis_reach(int prob, int a) { return prob == kLee ? a / 2 : 1; }
 
 // launchers (transform_*.cu)
 int launch_group(const GroupPlan &p, cudaStream_t s);

@@ -76,10 +76,9 @@ int occupancy_grid(const GroupPlan &p) {
 
 // Distance layers that can be nonzero after axes 0..j-1: each Hamming axis
 // adds at most 1 to the distance, each Lee axis at most floor(a/2).
-int live_layers(const Geometry &g, int j) {
-  long long reach = 0;
-  for (int i = 0; i < j; i++)
-    reach += g.prob == kLee ? g.ax[i] / 2 : 1;
+int live_layers(const Geometry &g, const AxisRange &r, int j) {
+  long long reach = r.reach0;
+  for (int i = r.begin; i < j; i++) reach += axis_reach(g.prob, g.ax[i]);
   return (int)std::min<long long>(reach, g.R) + 1;
 }
 
@@ -92,12 +91,14 @@ int live_layers(const Geometry &g, int j) {
 // HBM-facing ones have the widest strides.
 std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
                                    const PlanPtrs &ptr, int src, int dst,
-                                   Knobs kn) {
+                                   Knobs kn, AxisRange range) {
   std::vector<GroupPlan> out;
   const bool layered = R1 > 1;
   const size_t budget = kn.budget;
-  int j = 0;
-  while (j < g.n) {
+  const int end = range.end < 0 ? g.n : range.end;
+  if (range.begin < 0 || range.begin >= end || end > g.n) return {};
+  int j = range.begin;
+  while (j < end) {
     const int q = g.ax[j];
     int bm = 1;
     const int kid = pick_group_kernel(g.prob, q, R1, &bm);
@@ -113,9 +114,9 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     // the first group of a binary Hamming cell with 16-bit values: axis 0
     // is the word pair itself (inner = 2, applied as a swap-add inside each
     // lane) and the group's rounds run over axes 1.. on packed pairs
-    const bool pair = j == 0 && kn.half && kid >= 0 && g.prob == kHamming &&
-                      q == 2 && g.n >= 2 && g.ax[1] == 2 &&
-                      src != kSrcLayers;
+    const bool pair = j == 0 && kn.half && kn.pair && kid >= 0 &&
+                      g.prob == kHamming && q == 2 && end >= 2 &&
+                      g.ax[1] == 2 && src != kSrcLayers;
     const int j0 = j + (pair ? 1 : 0);     // first axis of the rounds
     base.pair_axis = pair ? 1 : 0;
     base.inner = pair ? 2 : g.pw[j];
@@ -128,7 +129,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     base.prob = g.prob;
     base.R = g.R;
     base.mu = g.mu;
-    base.src = j == 0 ? src : kSrcLayers;
+    base.src = j == range.begin ? src : kSrcLayers;
     // pipe 1 and 3 prefetch the cnt-reading first group; 3 also the last
     // group when it writes the 4-byte map (reads every layer, writes one
     // plane), decided below; 2 prefetches every group (16-bit layers only
@@ -143,7 +144,7 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
       a.W = W;
       long long mid = 1;
       for (;;) {
-        if (j0 + a.k >= g.n || a.k >= kMaxRounds) break;
+        if (j0 + a.k >= end || a.k >= kMaxRounds) break;
         const int qn = g.ax[j0 + a.k];
         if (kid >= 0 && qn != q) break;
         if (kid < 0 && qn > 16) break;
@@ -187,9 +188,9 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
     for (int t = 0; t < a.k; t++) a.qax[t] = g.ax[j0 + t];
     if (kid >= 0) set_rounds(a, q, bm);
     else a.nrounds = 0;
-    const bool last = j0 + a.k == g.n;
+    const bool last = j0 + a.k == end;
     a.dst = last ? dst : kDstLayers;
-    a.out16 = kn.half && !last;
+    a.out16 = kn.half && !(last && range.final);
     if (kn.pipe == 3 && kid >= 0 && last && dst != kDstLayers &&
         a.src == kSrcLayers && !a.in16) {
       // read-heavy last group: prefetch its tiles too (if they still fit)
@@ -197,9 +198,10 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
       t.pipe = 1;
       if (group_smem_bytes(t, R1) <= budget) a.pipe = 1;
     }
-    a.lin = layered ? live_layers(g, j) : 1;
-    a.lout = layered ? live_layers(g, j0 + a.k) : 1;
-    if (last && dst == kDstLayers) a.lout = R1;   // every layer, zeros too
+    a.lin = layered ? live_layers(g, range, j) : 1;
+    a.lout = layered ? live_layers(g, range, j0 + a.k) : 1;
+    if (last && range.final && dst == kDstLayers)
+      a.lout = R1;                                // every layer, zeros too
     a.pmode = kPredEq;
     a.ptarget = 0;
     GroupPlan p;

@@ -95,6 +95,15 @@ def _bind(path):
         "dct_b200_layers_at": (I, [_LLP, I, _I32P]),
         "dct_b200_greedy_fill": (I, [I, _LLP, _LLP]),
         "dct_b200_last_timings": (I, [ctypes.POINTER(ctypes.c_float), I]),
+        "dct_b200_ooc_plan": (I, [I, I, ctypes.POINTER(I), I, I, I, _LL, _LL,
+                                  _LL, I, _LLP, I]),
+        "dct_b200_ooc_record": (_LL, [I, I, ctypes.POINTER(I), I, I, I, I,
+                                      _LLP, _LL, _LL, I, _LLP, _LL]),
+        "dct_b200_ooc_transform": (I, [I, I, ctypes.POINTER(I), I, I, I, I,
+                                       _LLP, _LL, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, _LL,
+                                       _LL, I,
+                                       ctypes.POINTER(ctypes.c_float)]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):

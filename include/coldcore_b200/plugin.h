@@ -251,6 +251,51 @@ CCP_API int  dct_b200_greedy_fill(int max_add, long long *placed,
                                   long long *deficit);
 CCP_API int  dct_b200_read_layer(int d, long long off, long long len, int32_t *out);
 
+/* ---- out-of-core (ooc) cells: distance layers in host memory ----
+ * Replaces the reference's host placement of the layer planes
+ * (layers_mode 1/2: src/plugins/covering/dctcore_core.cuh:86-119, chosen
+ * by src/coldcore/gpu.py:253-260 when |X|(4(R+1)+2) bytes exceed the HBM
+ * budget), whose kernels read the planes over GH200's coherent C2C.  Here
+ * the planes sit in caller-owned (pinned) host memory and one transform
+ * streams them through two device pieces in two phases: slabs of the low
+ * axes 0..s-1 (device to host), then column blocks of the high axes
+ * s..n-1 (host to device); cnt, the map and the code stay in HBM.  The
+ * modes are dct_transform's (plugin.h:84-88): init 0 the code (host words,
+ * any order, a multiset under the counter rule), 1 gain / 2 loss from cnt
+ * (device, |X| uint16) at multiplicity mu; out 1 the int32 map and 2 cnt
+ * (device, |X| words), 3 every layer (the host planes, int32, plane d at
+ * host + d|X|).  device_budget bounds the bytes allocated on the device;
+ * min_width (0: 32) the narrowest column block.  Torus / grid axes above 16
+ * are not streamed (-3); -2 when no split fits the budget.
+ *
+ * info (17 values): split s, P_low, P_high, slab rows, slabs, column width,
+ * columns, piece words, piece plane stride, 16-bit host planes, planes
+ * carried between the phases, host bytes needed, device bytes, bytes over
+ * the host link, ball size, R+1 (or 1), host bytes per plane word. */
+CCP_API int  dct_b200_ooc_plan(int problem, int n, const int *ax, int R,
+                               int init_mode, int out_mode, long long M,
+                               long long maxmult, long long device_budget,
+                               int min_width, long long *info, int cap);
+/* The schedule without a device: rows of 20 values, one per copy, fill,
+ * scatter, launch and stream join, in issue order; returns the row count
+ * (rows beyond cap_rows are counted, not written). */
+CCP_API long long dct_b200_ooc_record(int problem, int n, const int *ax,
+                                      int R, int init_mode, int out_mode,
+                                      int mu, const long long *code,
+                                      long long M, long long device_budget,
+                                      int min_width, long long *rows,
+                                      long long cap_rows);
+/* One streamed transform; ms (2 floats, may be NULL) receives the device
+ * time of each phase.  Synchronizes the device on entry and returns when
+ * the result is in place. */
+CCP_API int  dct_b200_ooc_transform(int problem, int n, const int *ax, int R,
+                                    int init_mode, int out_mode, int mu,
+                                    const long long *code, long long M,
+                                    const uint16_t *cnt, void *out,
+                                    void *host, long long host_bytes,
+                                    long long device_budget, int min_width,
+                                    float *ms);
+
 #ifdef __cplusplus
 }
 #endif
