@@ -58,6 +58,12 @@ struct State {
   uint32_t *owner = nullptr;
   int use_owner = 0;
   int layers_mode = 0, cnt_mode = 0;
+  // layers_mode 1: the R+1 layer planes in pinned host memory (plane d at
+  // h_layers + d*|X|), streamed by every transform (outofcore.cu); the
+  // device keeps plane 0 alone, the map
+  bool streamed = false;
+  int32_t *h_layers = nullptr;
+  long long h_layers_bytes = 0;
   // support tables, SoA slots
   int32_t *tbl = nullptr, *tbl2 = nullptr;
   int slots = 0, slots2 = 0;
@@ -294,6 +300,7 @@ void free_all() {
   F(S.d_ext64); F(S.d_extv); F(S.zbuf); F(S.d_found);
   F(S.d_swap); F(S.d_list); FH(S.h_swap);
   F(S.d_greedy); F(S.d_placed); F(S.d_fresh); FH(S.h_placed);
+  FH(S.h_layers);
   FH(S.h_words); FH(S.h_out); FH(S.h_scalar);
   S.~State();
   new (&S) State();
@@ -410,7 +417,43 @@ void set_predicate(int init_mode, int *pm, int *pt) {
   }
 }
 
+// Device bytes a streamed transform may allocate: CC_OOC_BUDGET_KB, else
+// 80% of the free device memory less 256 MiB.
+long long ooc_budget() {
+  if (const char *e = getenv("CC_OOC_BUDGET_KB")) return atoll(e) << 10;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return std::max(0LL, (long long)(fr / 10 * 8) - (256LL << 20));
+}
+
+// A transform of a layers_mode-1 cell: the code (uploaded, sorted) or cnt
+// in, the map (plane 0) or cnt out on the device, or every layer out into
+// the host planes.
+int run_streamed(int init_mode, int out_mode) {
+  CC_CK(cudaStreamSynchronize(g_stream));
+  void *out = out_mode == 1 ? static_cast<void *>(S.layers)
+              : out_mode == 2 ? static_cast<void *>(S.cnt) : nullptr;
+  float ms[2] = {0, 0};
+  const long long M = init_mode == 0 ? S.codeM : 0;
+  const int rc = dct_b200_ooc_transform(
+      S.g.prob, S.g.n, S.g.ax, S.g.R, init_mode, out_mode, g_mu,
+      M ? S.up_sorted.data() : nullptr, M, S.cnt, out, S.h_layers,
+      S.h_layers_bytes, ooc_budget(), 0, ms);
+  if (rc) return rc;
+  g_last_n = 0;
+  if (timing_on()) {
+    g_last_ms[0] = ms[0];
+    g_last_ms[1] = ms[1];
+    g_last_n = 2;
+  }
+  return 0;
+}
+
 int run_transform(int init_mode, int out_mode) {
+  if (S.streamed) return run_streamed(init_mode, out_mode);
   Plan &P = plan_for(init_mode, out_mode);
   int pm, pt;
   set_predicate(init_mode, &pm, &pt);
@@ -540,7 +583,7 @@ std::vector<long long> grouping_key(const Plan &P) {
 // integers, so tuning runs are ordinary transforms.  CC_TUNE=0 turns it
 // off; explicit CC_PIPE / CC_SMEM_BUDGET_KB settings also pin the schedule.
 int autotune(int init_mode, int out_mode) {
-  if (S.tuned[init_mode][out_mode]) return 0;
+  if (S.streamed || S.tuned[init_mode][out_mode]) return 0;
   S.tuned[init_mode][out_mode] = true;
   const char *te = getenv("CC_TUNE");
   if ((te && atoi(te) == 0) || getenv("CC_PIPE") ||
@@ -654,8 +697,29 @@ int init_common(int problem, int n, const int *ax, int R, long long len,
   S.cnt_mode = cnt_mode;
   S.use_owner = use_owner;
   S.len = len;
-  if (dev_alloc((void **)&S.layers, (size_t)S.plane * S.nplanes * 4,
-                layers_mode)) { free_all(); return -3; }
+  // layers_mode 1, the reference's host placement of the layer planes
+  // (dctcore_core.cuh:86-119): pinned host planes streamed through the
+  // device (cells with a two-phase split, i.e. group-transform cells of
+  // two or more axes); otherwise, and for mode 2, managed planes
+  bool wide = false;
+  for (int i = 0; i < n; i++) wide = wide || ax[i] > 16;
+  S.streamed = layers_mode == 1 && n >= 2 && !wide;
+  if (S.streamed) {
+    if (dev_alloc((void **)&S.layers, (size_t)S.plane * 4, 0)) {
+      free_all(); return -3;
+    }
+    S.h_layers_bytes = (long long)S.R1 * space * 4;
+    if (cudaHostAlloc((void **)&S.h_layers, (size_t)S.h_layers_bytes,
+                      cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      S.h_layers = nullptr;
+      fprintf(stderr, "coldcore_b200: pinned host planes of %lld bytes "
+              "failed\n", S.h_layers_bytes);
+      free_all(); return -3;
+    }
+    S.bytes_host += S.h_layers_bytes;
+  } else if (dev_alloc((void **)&S.layers, (size_t)S.plane * S.nplanes * 4,
+                       layers_mode)) { free_all(); return -3; }
   S.cnt_len = round_up(space, kPlaneAlign);
   if (dev_alloc((void **)&S.cnt, (size_t)S.cnt_len * 2, cnt_mode)) {
     free_all(); return -4;
@@ -1600,6 +1664,13 @@ int dct_b200_layers_at(const long long *idx, int k, int32_t *out) {
   if (!S.live || !S.layered_out || (k && !out)) return -1;
   if (k <= 0) return 0;
   if (!valid_words(idx, k)) return -1;
+  if (S.streamed) {
+    const long long X = S.g.space;
+    for (int i = 0; i < k; i++)
+      for (int d = 0; d < S.R1; d++)
+        out[(long long)i * S.R1 + d] = S.h_layers[d * X + idx[i]];
+    return 0;
+  }
   const long long cap = kStageCap / S.R1;
   for (long long off = 0; off < k; off += cap) {
     const int nb = (int)std::min<long long>(cap, k - off);
@@ -1642,6 +1713,10 @@ int dct_b200_read_layer(int d, long long off, long long len, int32_t *out) {
   if (!S.live || !S.layered_out || d < 0 || d >= S.R1 || off < 0 ||
       len < 0 || off + len > S.g.space || (len && !out))
     return -1;
+  if (len && S.streamed) {
+    memcpy(out, S.h_layers + d * S.g.space + off, (size_t)len * 4);
+    return 0;
+  }
   if (len)
     CC_CK(cudaMemcpyAsync(out, S.layers + d * S.plane + off,
                           (size_t)len * 4, cudaMemcpyDeviceToHost, g_stream));

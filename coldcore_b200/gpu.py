@@ -216,8 +216,10 @@ class GpuBackend:
     """One problem cell resident on the B200 (coldcore ``gpu.py:207-537``).
 
     problem: "hamming", "torus_linf", "lee" or "grid_linf"; mu: covering
-    multiplicity; layers_mode / cnt_mode: 0 = HBM, 1 / 2 = managed memory
-    (None = HBM).
+    multiplicity; layers_mode: 0 = HBM, 1 = pinned host planes streamed
+    through the device by each transform (cells of two or more axes up to
+    16; others fall back to managed memory), 2 = managed memory; cnt_mode:
+    0 = HBM, 1 / 2 = managed memory (None = HBM).
     """
 
     def __init__(self, axes, R, problem="hamming", plugin_path=None,

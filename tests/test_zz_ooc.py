@@ -97,3 +97,49 @@ def test_h2_22_3_against_the_in_memory_engine():
                                _budget(4, 1 << 18, 1, 0),
                                cnt=_cnt_tensor(cnt))
         assert np.array_equal(got.cpu().numpy(), want), init_mode
+
+
+def _session(axes, R, problem, layers_mode, code):
+    """Every transform kind and the reads after them, on one engine cell."""
+    from coldcore_b200.gpu import GpuBackend
+    r = {}
+    with GpuBackend(axes, R, problem, layers_mode=layers_mode) as g:
+        g.recount(code)
+        r["cnt"] = g.read_cnt().copy()
+        r["unc"] = g.uncovered()
+        g.gain_map()
+        r["gain"] = g.map_all().copy()
+        r["gain_max"] = g.map_max()
+        g.loss_map()
+        r["loss"] = g.map_all().copy()
+        if problem in ("hamming", "lee"):
+            g.layers_map(0)
+            r["layers"] = np.stack([g.layer(d) for d in range(R + 1)])
+            r["at"] = g.layers_at(code[:7])
+        g.ball_update(code[:2], -1)
+        g.gain_map()
+        r["gain2"] = g.map_all().copy()
+        r["ext"] = np.sort(g.map_extract(1)[0])
+    return r
+
+
+# (family, axes, R, device KB): every transform of the session in at least
+# two pieces (14-36 slabs, 12-41 columns on the layered cells)
+HOST_CELLS = [("hamming", [3] * 9, 2, 48), ("lee", [6] * 6, 3, 72),
+              ("torus_linf", [7, 9, 11], 2, 8), ("grid_linf", [8, 8, 8], 2, 4)]
+
+
+@pytest.mark.parametrize("problem,axes,R,kb", HOST_CELLS,
+                         ids=lambda v: str(v).replace(" ", ""))
+def test_host_placement_matches_hbm(problem, axes, R, kb, monkeypatch):
+    """layers_mode 1 (host planes, streamed) through the ordinary ABI: the
+    same counts, maps, layers and queries as the HBM cell, with a device
+    budget small enough for many pieces."""
+    rng = np.random.default_rng(11)
+    X = int(np.prod(axes))
+    code = rng.choice(X, X // 40, replace=False)
+    want = _session(axes, R, problem, 0, code)
+    monkeypatch.setenv("CC_OOC_BUDGET_KB", str(kb))
+    got = _session(axes, R, problem, 1, code)
+    for k in want:
+        assert np.array_equal(np.asarray(got[k]), np.asarray(want[k])), k
