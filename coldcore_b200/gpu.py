@@ -24,6 +24,11 @@ from .space import ProductSpace
 
 _libs = {}
 
+# HBM budget of the automatic placement (bytes): COLDCORE_HBM_BUDGET, as in
+# coldcore (src/coldcore/gpu.py:31-33), defaulting to most of a B200's
+# 180 GB with room for tables, staging and other tenants.
+HBM_BUDGET = int(float(os.environ.get("COLDCORE_HBM_BUDGET", 160e9)))
+
 _LL = ctypes.c_longlong
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _LLP = ctypes.POINTER(_LL)
@@ -111,6 +116,19 @@ def _bind(path):
             f.restype = res
             f.argtypes = args
     return lib
+
+
+def placement(size, nlayers, budget=None):
+    """(layers_mode, cnt_mode) for a cell of ``size`` words: everything in
+    HBM when ``size * (4 * nlayers + 2)`` bytes fit the budget, else the
+    layer planes in host memory, streamed (mode 1); cnt stays in HBM while
+    it and the device map plane (6 bytes a word) fit, else managed.  The
+    rule of coldcore's policy (``src/coldcore/gpu.py:253-260``) with the
+    map plane counted, since a streamed cell keeps it on the device."""
+    budget = HBM_BUDGET if budget is None else budget
+    layers_mode = 0 if size * (4 * nlayers + 2) <= budget else 1
+    cnt_mode = 0 if layers_mode == 0 or size * 6 <= budget else 1
+    return layers_mode, cnt_mode
 
 
 def default_plugin_path():
@@ -219,7 +237,9 @@ class GpuBackend:
     multiplicity; layers_mode: 0 = HBM, 1 = pinned host planes streamed
     through the device by each transform (cells of two or more axes up to
     16; others fall back to managed memory), 2 = managed memory; cnt_mode:
-    0 = HBM, 1 / 2 = managed memory (None = HBM).
+    0 = HBM, 1 / 2 = managed memory.  None picks both by ``placement``
+    (HBM whenever the cell fits ``COLDCORE_HBM_BUDGET``).  Cells that take
+    the wide table (more than 16 axes, or axes above 16) are always in HBM.
     """
 
     def __init__(self, axes, R, problem="hamming", plugin_path=None,
@@ -240,6 +260,12 @@ class GpuBackend:
         self._ext_bufs = None
         self._closed = True
         axes = self.space.axes
+        auto_l, auto_c = placement(
+            self.space.size,
+            1 if problem in ("torus_linf", "grid_linf") else self.R + 1)
+        layers_mode = auto_l if layers_mode is None else layers_mode
+        cnt_mode = auto_c if cnt_mode is None else cnt_mode
+        self.layers_mode, self.cnt_mode = layers_mode, cnt_mode
         by = _LL(0)
         ax = (ctypes.c_int * self.space.n)(*axes)
         pid = PROBLEM_IDS[problem]

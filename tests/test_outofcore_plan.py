@@ -360,3 +360,16 @@ def test_schedule_pieces_and_traffic(lib):
     link += (h2d[:, 8] * h2d[:, 9]).sum()
     assert link == info["link_bytes"]
     assert set(rows[ops == ooc.OP_LAUNCH, 1]) <= {0, 1}
+
+
+def test_automatic_placement():
+    """coldcore's placement rule on a B200 budget: HBM while the whole cell
+    fits, else host layer planes (streamed) with cnt and the map in HBM,
+    and managed cnt only when even those 6 bytes a word do not fit."""
+    from coldcore_b200.gpu import placement
+    assert placement(3 ** 16, 5, budget=160e9) == (0, 0)       # H3(16,4)
+    assert placement(2 ** 34, 4, budget=160e9) == (1, 0)       # 309 GB
+    assert placement(2 ** 34, 4, budget=320e9) == (0, 0)
+    assert placement(10 ** 10, 6, budget=160e9) == (1, 0)      # K_10(10,5)
+    assert placement(3 * 10 ** 10, 6, budget=160e9) == (1, 1)
+    assert placement(1, 1, budget=0) == (1, 1)
