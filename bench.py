@@ -588,12 +588,24 @@ def run_b200(args, dist):
         line["also"] = also
     if same:
         line["same_cells"] = same
-    if not args.no_batch:
-        line["batched"] = measure_batch(args, dist)
-    if not args.no_incidence and dist.world == 1:
-        # the explicit-incidence engine (plugin ABI 2) on a covering design;
-        # a failure here is reported in its own object, not the line's
+    # the secondary legs, each reporting a failure in its own object: the
+    # ones measured before first, then the newer ones, so that an error in
+    # a later leg cannot cost an earlier one its numbers
+    def leg(key, fn):
         try:
+            line[key] = fn()
+        except Exception as e:           # noqa: BLE001
+            line[key] = {"error": f"{type(e).__name__}: {e}"}
+
+    if not args.no_batch:
+        leg("batched", lambda: measure_batch(args, dist))
+    if not args.no_lns and dist.world == 1:
+        leg("lns", lambda: measure_lns(args))
+    if not args.no_batch:
+        leg("batched_small", lambda: measure_batch_small(args))
+    if not args.no_incidence and dist.world == 1:
+        # the explicit-incidence engine (plugin ABI 2) on a covering design
+        def incidence():
             from coldcore_b200.incidence_bench import measure as inc_measure
             cpu_field = None
             if not args.no_cpu:
@@ -601,17 +613,8 @@ def run_b200(args, dist):
 
                 def cpu_field(rows, cnt, out):     # the CPU baseline leg
                     inc_field(rows, cnt, 0, out=out)
-            line["incidence"] = inc_measure(cpu_field=cpu_field)
-        except Exception as e:           # noqa: BLE001
-            line["incidence"] = {"error": f"{type(e).__name__}: {e}"}
-    if not args.no_lns and dist.world == 1:
-        line["lns"] = measure_lns(args)
-    if not args.no_batch:
-        # last, so that nothing else depends on it
-        try:
-            line["batched_small"] = measure_batch_small(args)
-        except Exception as e:           # noqa: BLE001
-            line["batched_small"] = {"error": f"{type(e).__name__}: {e}"}
+            return inc_measure(cpu_field=cpu_field)
+        leg("incidence", incidence)
     print(json.dumps(line), flush=True)
 
 
