@@ -373,3 +373,58 @@ def test_automatic_placement():
     assert placement(10 ** 10, 6, budget=160e9) == (1, 0)      # K_10(10,5)
     assert placement(3 * 10 ** 10, 6, budget=160e9) == (1, 1)
     assert placement(1, 1, budget=0) == (1, 1)
+
+
+def test_engine_schedule_fuzz(lib):
+    """Seeded random cells (every family, mixed radix, up to 20,000 words),
+    piece capacities, column widths, modes and multiplicities: each
+    schedule that plans replays to the oracle's result."""
+    rng = np.random.default_rng(2027)
+    ran = 0
+    for _ in range(80):
+        problem = str(rng.choice(["hamming", "lee", "torus_linf",
+                                  "grid_linf"]))
+        R = int(rng.integers(1, 5))
+        lo = 2 * R + 1 if problem == "torus_linf" else 2
+        n = int(rng.integers(2, 8))
+        axes = [int(a) for a in rng.integers(lo, 17, n)]
+        if problem in ("hamming", "lee") and rng.random() < 0.5:
+            axes = [axes[0]] * n
+        X = prod(axes)
+        if X > 20000 or X < 16:
+            continue
+        layered = problem in ("hamming", "lee")
+        R1 = R + 1 if layered else 1
+        modes = [m for m in MODES if layered or m[1] != 3]
+        init_mode, out_mode = modes[int(rng.integers(len(modes)))]
+        mu = 1 if init_mode == 0 else int(rng.integers(1, 4))
+        o = OracleBackend(axes, R, problem, mu=mu)
+        code = rng.choice(X, max(1, X // int(rng.integers(10, 60))),
+                          replace=False)
+        o.recount(code)
+        cnt = o.cnt.copy()
+        if cnt.max() > 65535:
+            continue
+        M = len(code) if init_mode == 0 else 0
+        cap = int(rng.integers(16, X + 64))
+        mw = int(rng.choice([1, 4, 8, 32]))
+        budget = _budget(R1, cap, out_mode, M)
+        try:
+            info = ooc.ooc_plan(problem, axes, R, init_mode, out_mode, budget,
+                                M=M, maxmult=1, min_width=mw)
+        except RuntimeError:
+            continue
+        rows = ooc.ooc_record(problem, axes, R, init_mode, out_mode, budget,
+                              code=code, mu=mu, min_width=mw)
+        got = replay(rows, problem, axes, R, init_mode, out_mode, mu, info,
+                     code, cnt)
+        if init_mode == 1:
+            o.gain_map()
+        elif init_mode == 2:
+            o.loss_map()
+        want = (o.layers() if out_mode == 3
+                else o.cnt if init_mode == 0 else o.map)
+        assert np.array_equal(got, want), (problem, axes, R, init_mode,
+                                           out_mode, mu, cap, mw)
+        ran += 1
+    assert ran >= 30
