@@ -289,13 +289,13 @@ __global__ void k_scatter_slab(int32_t *plane0, const long long *code,
 }
 
 // Issues the schedule's operations: on the device, or as rows of kRecFields
-// values (record mode, rec != nullptr).
+// values (record mode).
 struct Exec {
   char *base[kNumBufs] = {};
   cudaStream_t st[2] = {nullptr, nullptr};
   cudaEvent_t join[2] = {nullptr, nullptr};
   cudaEvent_t mark[3] = {nullptr, nullptr, nullptr};
-  std::vector<long long> *rec = nullptr;
+  bool rec = false;
   long long rows = 0, cap_rows = 0;
   long long *out_rows = nullptr;
 
@@ -560,9 +560,8 @@ long long dct_b200_ooc_record(int problem, int n, const int *ax, int R,
   int rc = make_cell(problem, n, ax, R, init_mode, out_mode, mu, M, mx,
                      device_budget, min_width, &c);
   if (rc) return rc;
-  std::vector<long long> dummy;
   Exec x;
-  x.rec = &dummy;
+  x.rec = true;
   x.out_rows = rows;
   x.cap_rows = rows ? cap_rows : 0;
   rc = run_schedule(c, x, sorted.data());
