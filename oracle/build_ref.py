@@ -35,7 +35,7 @@ def build(force=False):
     src = os.path.join(REF_SRC, "plugins", "covering", "dct_hc.cu")
     if not os.path.exists(src):
         if os.path.exists(OUT):
-            return OUT                    # prebuilt (the GPU box has no source)
+            return OUT                    # prebuilt; no source here
         raise FileNotFoundError(src)
     if os.path.exists(OUT) and not force and \
             os.path.getmtime(OUT) >= os.path.getmtime(src):

@@ -14,6 +14,13 @@ def gpu_present():
 
 
 def pytest_collection_modifyitems(config, items):
+    # tests of code that has not yet passed on a B200 run after the others
+    # (stable, by rank), so that a run stopping at the first failure has
+    # run everything proven first
+    def rank(item):
+        m = item.get_closest_marker("late")
+        return m.args[0] if m and m.args else (1 if m else 0)
+    items[:] = sorted(items, key=rank)
     if gpu_present():
         return
     skip = pytest.mark.skip(reason="no CUDA device on this machine")

@@ -10,7 +10,7 @@ from coldcore_b200.incidence import (GpuIncidenceBackend,
 from golden_data import incidence_cells, incidence_golden
 from oracle.incidence_oracle import IncidenceOracle, WeightedIncidenceOracle
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late(2)]
 
 
 def open_cell(g, key, inc_mode, cap=16):

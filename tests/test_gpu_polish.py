@@ -8,7 +8,7 @@ import pytest
 from coldcore_b200.gpu import GpuBackend
 from coldcore_b200.search import Searcher
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late(1)]
 
 
 @pytest.mark.parametrize("problem,axes,R,seed", [

@@ -4,8 +4,7 @@ the engine's ordinary transform, bit for bit, on two calls in a row.
 It serves callers that may not allocate device memory themselves — for
 instance a host framework whose caching allocator must own every buffer —
 so the test hands it buffers allocated by torch and checks that the map it
-writes equals the one dct_transform computes.  Collected last (file name),
-so a run stopping at the first failure has run everything else first."""
+writes equals the one dct_transform computes."""
 import ctypes
 
 import numpy as np

@@ -1,16 +1,14 @@
 """Out-of-core transforms on the GPU (dct_b200_ooc_transform): the layer
 planes streamed through small device pieces in pinned host memory give,
 bit for bit, the oracle's map, cnt and layers on small cells cut into many
-slabs and ragged columns, and the in-memory engine's on H2(22,3).
-Collected last (file name), so a run stopping at the first failure has run
-everything else first."""
+slabs and ragged columns, and the in-memory engine's on H2(22,3)."""
 import numpy as np
 import pytest
 
 from coldcore_b200.outofcore import ooc_plan, ooc_transform
 from oracle.dp_oracle import OracleBackend
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late(3)]
 
 torch = pytest.importorskip("torch")
 
