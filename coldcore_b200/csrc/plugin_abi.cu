@@ -998,8 +998,19 @@ int dct_init3(int problem, int n, const int *ax, int R,
 
 int dct_init3w(int problem, int n, const int *ax, int R, const int32_t *tbl,
                int slots, long long len, int extract_cap, long long *bytes) {
+  return dct_b200_init3wm(problem, n, ax, R, tbl, slots, len, extract_cap,
+                          bytes, 0, 0);
+}
+
+int dct_b200_init3wm(int problem, int n, const int *ax, int R,
+                     const int32_t *tbl, int slots, long long len,
+                     int extract_cap, long long *bytes, int layers_mode,
+                     int cnt_mode) {
   if (!tbl || slots < 1 || slots > kMaxSlots) return -1;
-  int rc = init_common(problem, n, ax, R, len, extract_cap, 0, 0, 0);
+  if (layers_mode < 0 || layers_mode > 2 || cnt_mode < 0 || cnt_mode > 2)
+    return -1;
+  int rc = init_common(problem, n, ax, R, len, extract_cap, layers_mode,
+                       cnt_mode, 0);
   if (rc) return rc;
   std::vector<int32_t> soa((size_t)slots * len, 0);
   for (long long t = 0; t < len; t++)

@@ -61,6 +61,8 @@ def _bind(path):
                           I]),
         "dct_init3w": (I, [I, I, ctypes.POINTER(I), I, _I32P, I, _LL, I,
                            _LLP]),
+        "dct_b200_init3wm": (I, [I, I, ctypes.POINTER(I), I, _I32P, I, _LL,
+                                 I, _LLP, I, I]),
         "dct_init2": (I, [I, I, I, P64, _LL, I, _LLP, I, I, I]),
         "dct_init": (I, [I, I, I, P64, _LL, I, _LLP]),
         "dct_free": (I, []),
@@ -238,8 +240,9 @@ class GpuBackend:
     through the device by each transform (cells of two or more axes up to
     16; others fall back to managed memory), 2 = managed memory; cnt_mode:
     0 = HBM, 1 / 2 = managed memory.  None picks both by ``placement``
-    (HBM whenever the cell fits ``COLDCORE_HBM_BUDGET``).  Cells that take
-    the wide table (more than 16 axes, or axes above 16) are always in HBM.
+    (HBM whenever the cell fits ``COLDCORE_HBM_BUDGET``); cells that take
+    the wide table (more than 16 axes, or axes above 16) get theirs through
+    ``dct_b200_init3wm``.
     """
 
     def __init__(self, axes, R, problem="hamming", plugin_path=None,
@@ -281,9 +284,16 @@ class GpuBackend:
         else:
             tbl = wide_table(axes, R, problem)
             self.ball_len = len(tbl)
-            rc = lib.dct_init3w(pid, self.space.n, ax, self.R,
-                                _p(tbl, ctypes.c_int32), tbl.shape[1],
-                                len(tbl), self.extract_cap, ctypes.byref(by))
+            if layers_mode or cnt_mode:
+                rc = lib.dct_b200_init3wm(
+                    pid, self.space.n, ax, self.R, _p(tbl, ctypes.c_int32),
+                    tbl.shape[1], len(tbl), self.extract_cap,
+                    ctypes.byref(by), int(layers_mode), int(cnt_mode))
+            else:
+                rc = lib.dct_init3w(pid, self.space.n, ax, self.R,
+                                    _p(tbl, ctypes.c_int32), tbl.shape[1],
+                                    len(tbl), self.extract_cap,
+                                    ctypes.byref(by))
         _check("init", rc)
         self._closed = False
         _check("set_mu", lib.dct_set_mu(mu))

@@ -139,6 +139,13 @@ CCP_API int  dct_use_fmt(int fmt);
 CCP_API int  dct_init3w(int problem, int n, const int *ax, int R,
                 const int32_t *tbl, int slots, long long len,
                 int extract_cap, long long *bytes);
+/* dct_init3w with dct_init3's placement arguments (layers_mode 1: host
+ * planes streamed by each transform; 2: managed; cnt_mode 1/2: managed),
+ * so that wide-table cells can take the out-of-core path too. */
+CCP_API int  dct_b200_init3wm(int problem, int n, const int *ax, int R,
+                              const int32_t *tbl, int slots, long long len,
+                              int extract_cap, long long *bytes,
+                              int layers_mode, int cnt_mode);
 /* the engine's CUDA stream (cudaStream_t as an integer), for host timing */
 CCP_API long long dct_b200_stream(void);
 /* describe the launches of one dct_transform(init_mode, out_mode) without

@@ -122,9 +122,11 @@ def _session(axes, R, problem, layers_mode, code):
 
 
 # (family, axes, R, device KB): every transform of the session in at least
-# two pieces (14-36 slabs, 12-41 columns on the layered cells)
+# two pieces (14-36 slabs, 12-41 columns on the layered cells); H2(18,2)
+# takes the wide support table (dct_b200_init3wm)
 HOST_CELLS = [("hamming", [3] * 9, 2, 48), ("lee", [6] * 6, 3, 72),
-              ("torus_linf", [7, 9, 11], 2, 8), ("grid_linf", [8, 8, 8], 2, 4)]
+              ("torus_linf", [7, 9, 11], 2, 8), ("grid_linf", [8, 8, 8], 2, 4),
+              ("hamming", [2] * 18, 2, 1024)]
 
 
 @pytest.mark.parametrize("problem,axes,R,kb", HOST_CELLS,
