@@ -64,6 +64,7 @@ struct Cell {
   int64_t *xidx = nullptr;
   int32_t *xval = nullptr;
   int xcap = 0;
+  uint32_t *bits = nullptr;        // role bit per universe element
   long long *words = nullptr;      // staged candidate lists
   int32_t *out = nullptr;          // staged per-candidate outputs
   long long wcap = 0;
@@ -147,6 +148,58 @@ __global__ void k_rows_dense(const int32_t *__restrict__ inc, int d,
       const int32_t *row = inc + r * d;
 #pragma unroll 4
       for (int j = sl; j < d; j += L) s += role(cnt[row[j]], target, mu);
+    }
+    for (int o = L >> 1; o > 0; o >>= 1)
+      s += __shfl_down_sync(0xffffffffu, s, o, L);
+    if (sl == 0 && i < m) out[i] = s;
+  }
+}
+
+// One bit per universe element: bit u of bits[u / 32] = role(cnt[u]).  The
+// loop bound is uniform across a warp, so every lane reaches the ballot.
+__global__ void k_role_bits(const int32_t *__restrict__ cnt, long long nuniv,
+                            int target, int mu, uint32_t *__restrict__ bits) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long start = (long long)blockIdx.x * blockDim.x +
+                          (threadIdx.x & ~31);
+  const int lane = threadIdx.x & 31;
+  for (long long base = start; base < nuniv; base += stride) {
+    const long long u = base + lane;
+    const bool p = u < nuniv && role(cnt[u], target, mu);
+    const unsigned b = __ballot_sync(0xffffffffu, p);
+    if (lane == 0) bits[base >> 5] = b;
+  }
+}
+
+// k_rows_dense over the role bits instead of cnt: each CTA copies the
+// nwords bit words into shared memory, then a row entry costs one shared
+// bit test instead of a counter gather through L1/L2.
+template <int L>
+__global__ void k_rows_dense_bits(const int32_t *__restrict__ inc, int d,
+                                  const uint32_t *__restrict__ bits,
+                                  int nwords,
+                                  const long long *__restrict__ words,
+                                  long long m, int32_t *__restrict__ out) {
+  extern __shared__ uint32_t sbits[];
+  for (int t = threadIdx.x; t < nwords; t += blockDim.x) sbits[t] = bits[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, seg = lane / L, sl = lane % L;
+  const int P = 32 / L;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x)
+                         >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long ngroups = (m + P - 1) / P;
+  for (long long g = warp; g < ngroups; g += nwarps) {
+    const long long i = g * P + seg;
+    int s = 0;
+    if (i < m) {
+      const long long r = words ? words[i] : i;
+      const int32_t *row = inc + r * d;
+#pragma unroll 4
+      for (int j = sl; j < d; j += L) {
+        const int u = row[j];
+        s += (sbits[u >> 5] >> (u & 31)) & 1;
+      }
     }
     for (int o = L >> 1; o > 0; o >>= 1)
       s += __shfl_down_sync(0xffffffffu, s, o, L);
@@ -357,7 +410,7 @@ int alloc_fields(int extract_cap) {
 void free_all() {
   auto F = [](void *p) { if (p) cudaFree(p); };
   F(C.inc); F(C.indptr); F(C.w); F(C.uw); F(C.cnt); F(C.map); F(C.acc);
-  F(C.hist); F(C.xidx); F(C.xval); F(C.words); F(C.out);
+  F(C.hist); F(C.xidx); F(C.xval); F(C.words); F(C.out); F(C.bits);
   C = Cell();
 }
 
@@ -405,9 +458,47 @@ int stage_words(const long long *idx, long long m) {
   return 0;
 }
 
+// The role-bit form of a dense field or gather (CC_SPARSE_BITS=1): the
+// bits of the whole universe in at most 48 KB of shared memory a CTA.
+constexpr long long kBitsMaxWords = 48 * 1024 / 4;
+
+bool use_bits() {
+  const char *e = getenv("CC_SPARSE_BITS");
+  return e && atoi(e) == 1 && !C.csr &&
+         (C.nuniv + 31) / 32 <= kBitsMaxWords;
+}
+
+int launch_rows_bits(const long long *words, long long m, int target,
+                     int32_t *out) {
+  const int nwords = (int)((C.nuniv + 31) / 32);
+  int rc;
+  if (!C.bits && (rc = alloc_dev((void **)&C.bits, (size_t)nwords * 4)))
+    return rc;
+  k_role_bits<<<grid_for((long long)nwords * 32), kThreads, 0, g_s>>>(
+      C.cnt, C.nuniv, target, g_mu, C.bits);
+  SK(cudaGetLastError());
+  const int L = C.lanes, P = 32 / L;
+  const int grid = grid_for((m + P - 1) / P * 32);
+  const size_t smem = (size_t)nwords * 4;
+#define CC_BITS(LL)                                                         \
+  case LL:                                                                  \
+    k_rows_dense_bits<LL><<<grid, kThreads, smem, g_s>>>(                   \
+        C.inc, C.d, C.bits, nwords, words, m, out);                         \
+    break;
+  switch (L) {
+    CC_BITS(1) CC_BITS(2) CC_BITS(4) CC_BITS(8) CC_BITS(16) CC_BITS(32)
+    default:
+      return -2;
+  }
+#undef CC_BITS
+  SK(cudaGetLastError());
+  return 0;
+}
+
 // per-candidate row sums: the field (words null, into map) or a gather
 int launch_rows(const long long *words, long long m, int target,
                 int32_t *out) {
+  if (use_bits()) return launch_rows_bits(words, m, target, out);
   const int L = C.lanes, P = 32 / L;
   const int grid = grid_for((m + P - 1) / P * 32);
 #define CC_ROWS(LL)                                                         \

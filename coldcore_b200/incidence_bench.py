@@ -10,7 +10,11 @@ reference's own ``src/plugins/sparse/sparse.cu`` built for sm_100a), its
 kernels are timed in alternation on the same incidence.
 
     python -m coldcore_b200.incidence_bench [--v 30 --k 8 --t 4 --reps 20]
-                                            [--ref PATH]
+                                            [--ref PATH] [--bits]
+
+``--bits`` also times the role-bit form (``CC_SPARSE_BITS=1``: the role of
+every universe element as one bit in shared memory) and checks its gain
+field against the default form's.
 """
 import argparse
 import json
@@ -19,7 +23,6 @@ import statistics
 import time
 
 import numpy as np
-
 
 
 def _warm(b, seconds=0.3):
@@ -46,7 +49,7 @@ def _time_fields(b, stream, reps):
 
 
 def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
-            cpu_field=None):
+            cpu_field=None, bits=False):
     """Both cells stay resident and are timed in alternation, `rounds`
     times each after a warm-up; the medians are reported.  ``cpu_field``
     (optional, the caller's CPU baseline): ``cpu_field(rows, cnt, out)``
@@ -89,6 +92,18 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
             b.gain_map()
             sample = np.arange(0, n_cand, 997)
             gain = b.map_read_at(sample)
+            bit_rounds = bits_same = None
+            if bits:
+                os.environ["CC_SPARSE_BITS"] = "1"
+                try:
+                    _warm(b, 0.1)
+                    bit_rounds = [_time_fields(b, stream, reps)
+                                  for _ in range(rounds)]
+                    b.gain_map()
+                    bits_same = bool(np.array_equal(b.map_read_at(sample),
+                                                    gain))
+                finally:
+                    os.environ.pop("CC_SPARSE_BITS", None)
             same = None
             if ref is not None:
                 ref.gain_map()
@@ -114,6 +129,12 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
                 "ms_rounds_8_ctas_per_sm": [round(x, 4) for x in one_wave],
                 "GBps": round(by / (ms * 1e-3) / 1e9, 1),
                 "algorithmic_bytes_per_field": by})
+    if bit_rounds is not None:
+        bms = statistics.median(bit_rounds)
+        out["role_bits"] = {"ms_per_field": round(bms, 4),
+                            "ms_rounds": [round(x, 4) for x in bit_rounds],
+                            "GBps": round(by / (bms * 1e-3) / 1e9, 1),
+                            "same_gain_sample": bits_same}
     if cpu_ms is not None:
         out["cpu_baseline"] = {
             "value": round(by / (cpu_ms * 1e-3) / 1e9, 2), "unit": "GB/s",
@@ -141,8 +162,11 @@ def main():
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--ref", default=None,
                     help="another ABI-2 library to time beside the engine")
+    ap.add_argument("--bits", action="store_true",
+                    help="also time the role-bit form (CC_SPARSE_BITS=1)")
     a = ap.parse_args()
-    print(json.dumps(measure(a.v, a.k, a.t, a.reps, ref_path=a.ref)))
+    print(json.dumps(measure(a.v, a.k, a.t, a.reps, ref_path=a.ref,
+                             bits=a.bits)))
 
 
 if __name__ == "__main__":

@@ -291,3 +291,30 @@ def test_orbit_search_on_the_engine():
                                 notch_budget_s=5, reserve_s=0.0)
     assert len(blocks) == 21
     assert DesignOracle(21, 5, 2).verify(blocks)
+
+
+@pytest.mark.late(4)
+@pytest.mark.parametrize("d,n_univ", [(1, 31), (3, 32), (6, 33), (17, 150),
+                                      (33, 1000), (70, 27405)])
+def test_role_bit_form_against_the_oracle(d, n_univ, monkeypatch):
+    """CC_SPARSE_BITS=1: dense fields and gathers through the role bits in
+    shared memory (universes of 31 to 27,405 elements, whole and partial
+    bit words) equal the oracle's, before and after updates."""
+    monkeypatch.setenv("CC_SPARSE_BITS", "1")
+    rng = np.random.default_rng(d + n_univ)
+    n_cand = 777
+    inc = np.stack([rng.choice(n_univ, d, replace=False)
+                    for _ in range(n_cand)])
+    o = IncidenceOracle(inc, n_univ, mu=2)
+    with GpuIncidenceBackend(inc, n_univ, mu=2) as b:
+        for step in range(2):
+            sol = rng.choice(n_cand, 60 + 40 * step, replace=False)
+            b.recount(sol)
+            o.recount(sol)
+            for t in (0, 1, 2, 3):
+                o.field(t)
+                assert b._lib.sparse_field(t) == 0
+                assert np.array_equal(b.map_all(), o.map), (step, t)
+                probe = rng.choice(n_cand, 53)
+                assert np.array_equal(b.ball_gather(probe, t),
+                                      o.ball_gather(probe, t)), (step, t)
