@@ -177,10 +177,19 @@ def plan_probe(problem, axes, R, init_mode, out_mode, budget_kb=100, pipe=1,
             for i in range(n)]
 
 
+def ball_order():
+    """True unless ``COLDCORE_BALL_ORDER=native`` asks for the builder's
+    table order (coldcore ``gpu.py:119``, an A/B switch: the walks are
+    order-free, so only the memory traffic changes)."""
+    return os.environ.get("COLDCORE_BALL_ORDER", "locality") != "native"
+
+
 def locality_order(pats, axes):
     """Sort a v1 table by unwrapped offset so that neighbouring walk threads
     touch neighbouring words (coldcore ``gpu.py:106-129``); order-free walks
     make this a pure traffic optimisation.  Entry 0 stays the centre."""
+    if not ball_order():
+        return pats
     pats = np.ascontiguousarray(pats, dtype=np.uint64)
     n = len(axes)
     pos = np.zeros((len(pats), 8), dtype=np.int64)
@@ -274,7 +283,7 @@ class GpuBackend:
         pid = PROBLEM_IDS[problem]
         if max(axes) <= 16 and self.space.n <= 16 and (
                 problem in ("hamming", "lee") or self.space.n <= 8):
-            pats = v1_table(axes, R, problem)
+            pats = v1_table(axes, R, problem, order=ball_order())
             self.ball_len = len(pats)
             rc = lib.dct_init3(pid, self.space.n, ax, self.R,
                                _p(pats, ctypes.c_uint64), len(pats),
@@ -282,7 +291,7 @@ class GpuBackend:
                                layers_mode or 0, cnt_mode or 0,
                                1 if use_owner else 0)
         else:
-            tbl = wide_table(axes, R, problem)
+            tbl = wide_table(axes, R, problem, order=ball_order())
             self.ball_len = len(tbl)
             if layers_mode or cnt_mode:
                 rc = lib.dct_b200_init3wm(

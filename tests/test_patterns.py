@@ -51,3 +51,19 @@ def test_ball_sizes():
     assert ball_size([7] * 8, 4, "lee") == 3633
     assert ball_size([2048, 2048], 1, "torus_linf") == 9
     assert ball_size([3] * 8, 2, "hamming") == 129
+
+
+def test_ball_order_switch(monkeypatch):
+    """COLDCORE_BALL_ORDER=native keeps the builder's order (coldcore
+    gpu.py:119); either order holds the same patterns, centre first."""
+    from coldcore_b200.gpu import ball_order, locality_order
+    from coldcore_b200.patterns import v1_table
+    axes, R = [3, 4, 5, 3], 2
+    native = v1_table(axes, R, "hamming", order=False)
+    assert ball_order()
+    sorted_ = locality_order(native, axes)
+    monkeypatch.setenv("COLDCORE_BALL_ORDER", "native")
+    assert not ball_order()
+    assert locality_order(native, axes) is native
+    assert sorted_[0] == native[0] == 0
+    assert sorted(sorted_.tolist()) == sorted(native.tolist())
