@@ -428,3 +428,22 @@ def test_engine_schedule_fuzz(lib):
                                            out_mode, mu, cap, mw)
         ran += 1
     assert ran >= 30
+
+
+def test_pitch_limit_bounds_the_split(lib):
+    """K_10(10,5), 10^10 words, on a 100 GB piece budget: P_low = 10^9
+    would need a 4 GB row pitch (2-D copies take < 2^31 bytes), so the
+    split stops at P_low = 10^8: 5 slabs of 20 rows, then 5 column blocks
+    whose rows are 41 MB of 16-bit words."""
+    axes, R = [10] * 10, 5
+    info = ooc.ooc_plan("hamming", axes, R, 0, 2, 100 << 30, M=60000,
+                        maxmult=1)
+    assert info["p_low"] == 10 ** 8 and info["split"] == 8
+    assert info["p_low"] * 4 <= ooc.MAX_PITCH
+    assert info["half"] == 1 and info["live_mid"] == 6
+    assert info["link_bytes"] == 2 * 10 ** 10 * 2 * 6
+    assert info["device_bytes"] <= 100 << 30
+    want = plan_pieces(axes, info["cap"])
+    assert {k: info[k] for k in want} == want
+    assert info["n_slabs"] == 5 and info["n_cols"] == 5
+    assert info["col_width"] * 2 >= 32 << 20            # rows of >= 32 MB
