@@ -1537,8 +1537,9 @@ long long dct_b200_stream(void) {
 }
 
 int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
-  if (!S.live || init_mode < 0 || init_mode > 2 || out_mode < 1 ||
-      out_mode > 3)
+  // a streamed cell runs the out-of-core schedule (dct_b200_ooc_plan)
+  if (!S.live || S.streamed || init_mode < 0 || init_mode > 2 ||
+      out_mode < 1 || out_mode > 3)
     return -1;
   Plan &P = plan_for(init_mode, out_mode);
   const long long X = S.g.space;
@@ -1632,7 +1633,7 @@ int dct_b200_plan_probe(int problem, int n, const int *ax, int R,
 }
 
 int dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap) {
-  if (!S.live || init_mode < 0 || init_mode > 2 || out_mode < 1 ||
+  if (!S.live || S.streamed || init_mode < 0 || init_mode > 2 || out_mode < 1 ||
       out_mode > 3 || cap < 0)
     return -1;
   Plan &P = plan_for(init_mode, out_mode);

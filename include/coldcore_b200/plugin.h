@@ -151,7 +151,8 @@ CCP_API long long dct_b200_stream(void);
 /* describe the launches of one dct_transform(init_mode, out_mode) without
  * running it: per launch 4 values (first axis, axes in the launch,
  * algorithmic HBM bytes read + written, kernel id); returns the number of
- * launches (at most cap/4 described) or a negative error. */
+ * launches (at most cap/4 described) or a negative error (-1 for a cell
+ * whose layers stream from host memory: dct_b200_ooc_plan describes it). */
 CCP_API int  dct_b200_plan(int init_mode, int out_mode, long long *info, int cap);
 /* schedule form of each group launch of one transform (no counterpart in
  * the reference): bit 1 prefetching (cp.async) kernel, 2 packed word pairs,
