@@ -470,42 +470,6 @@ def candidates_covering(v, k, t, univ_idx):
     return np.sort(subset_ranks(np.sort(rows, axis=1)))
 
 
-def read_cover(path, v, k):
-    """A cover file in the La Jolla repository's format -> candidate
-    indices (colex ranks): one block per line, k distinct elements in
-    1..v, space separated; blank lines and ``#`` comments skipped
-    (coldcore ``problems/covering_design.py:138-160``)."""
-    rows = []
-    with open(path) as fh:
-        for ln, line in enumerate(fh, 1):
-            line = line.strip()
-            if not line or line.startswith("#"):
-                continue
-            vals = [int(x) for x in line.split()]
-            if len(vals) != k:
-                raise ValueError(f"{path}:{ln}: {len(vals)} elements, "
-                                 f"want k={k}")
-            if min(vals) < 1 or max(vals) > v:
-                raise ValueError(f"{path}:{ln}: element out of 1..{v}")
-            if len(set(vals)) != k:
-                raise ValueError(f"{path}:{ln}: repeated element")
-            rows.append(sorted(vals))
-    if not rows:
-        return np.zeros(0, dtype=np.int64)
-    return subset_ranks(np.asarray(rows, dtype=np.int64) - 1)
-
-
-def write_cover(path, blocks):
-    """(M, k) 0-based blocks -> the same format (1-based, sorted, one
-    block per line), written to a temporary file and renamed into place
-    (covering_design.py:163-170)."""
-    tmp = path + ".tmp"
-    with open(tmp, "w") as fh:
-        for row in np.asarray(blocks):
-            fh.write(" ".join(str(int(x) + 1) for x in sorted(row)) + "\n")
-    os.replace(tmp, path)
-
-
 class GpuCoveringDesignBackend(GpuIncidenceBackend):
     """A covering design C(v,k,t) (mu-fold) whose incidence is built on the
     B200 (``sparse_b200_init_design``), in the layout of coldcore's
@@ -572,16 +536,6 @@ class GpuCoveringDesignBackend(GpuIncidenceBackend):
 
     def candidates_covering(self, univ_idx):
         return candidates_covering(self.v, self.k, self.t, univ_idx)
-
-    def read_cover(self, path):
-        return read_cover(path, self.v, self.k)
-
-    def write_cover(self, path, idx):
-        write_cover(path, self.rank_block(idx))
-
-    # the names a campaign driver's solution-file hooks look for
-    read_solution_file = read_cover
-    write_solution_file = write_cover
 
     def rows(self, c0=0, n=None):
         """Incidence rows [c0, c0 + n) as an (n, d) int32 array."""

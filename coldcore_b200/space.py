@@ -1,29 +1,37 @@
-"""Finite product space X = prod_j Z_{a_j}, little-endian mixed radix.
+"""The mixed-radix product space X = Z_{a_0} x ... x Z_{a_(n-1)}.
 
-Index <-> digit conversions as in coldcore ``src/coldcore/space.py:10-45``
-(x = sum_j d_j * prod_{i<j} a_i), with int64 digits so that axes wider than
-255 convert correctly (the reference's ``index_word`` returns uint8).
+A word (d_0, ..., d_(n-1)) has the index x = sum_j d_j * s_j with the
+little-endian strides s_j = a_0 * ... * a_(j-1); that numbering is the one
+coldcore's cells, codes and cover files use (``src/coldcore/space.py:10-45``
+defines the same numbering).  Digits here are int64 throughout, so axes
+wider than 255 round-trip (coldcore's ``index_word`` returns uint8 digits).
+
+The conversions are single vectorised expressions over the stride vector:
+an index's digit j is ``(x // s_j) mod a_j``.
 """
 import numpy as np
 
 
 class ProductSpace:
+    """``ProductSpace(q, n)`` for the homogeneous space Z_q^n, or
+    ``ProductSpace(axes)`` for a mixed radix; exposes ``axes``, ``n``,
+    ``q`` (None when mixed), ``size`` and the strides ``pow_q``."""
 
     def __init__(self, q_or_axes, n=None):
-        if n is not None:
-            axes = [int(q_or_axes)] * int(n)
-        else:
-            axes = [int(a) for a in q_or_axes]
-        self.axes = axes
-        self.n = len(axes)
-        self.q = axes[0] if len(set(axes)) == 1 else None
-        self.size = 1
-        pows = []
-        for a in axes:
-            pows.append(self.size)
-            self.size *= a
-        self.pow_q = np.array(pows, dtype=np.int64)
-        self._ax = np.array(axes, dtype=np.int64)
+        radix = (np.full(int(n), int(q_or_axes), dtype=np.int64)
+                 if n is not None else
+                 np.array([int(a) for a in q_or_axes], dtype=np.int64))
+        if radix.ndim != 1 or np.any(radix < 1):
+            raise ValueError(f"bad axes {q_or_axes!r}")
+        stride = np.ones(len(radix), dtype=np.int64)
+        np.cumprod(radix[:-1], out=stride[1:])
+        self._radix = radix
+        self.pow_q = stride
+        self.axes = radix.tolist()
+        self.n = len(radix)
+        self.size = int(np.prod(radix, dtype=np.int64))
+        self.q = int(radix[0]) if self.n and np.all(radix == radix[0]) \
+            else None
 
     def word_index(self, words):
         """(k, n) digit array -> int64 indices."""
@@ -31,13 +39,8 @@ class ProductSpace:
 
     def index_word(self, idx):
         """int64 indices -> (k, n) int64 digit array."""
-        idx = np.asarray(idx, dtype=np.int64).ravel()
-        out = np.empty((len(idx), self.n), dtype=np.int64)
-        x = idx.copy()
-        for i in range(self.n):
-            out[:, i] = x % self._ax[i]
-            x //= self._ax[i]
-        return out
+        x = np.asarray(idx, dtype=np.int64).reshape(-1, 1)
+        return (x // self.pow_q) % self._radix
 
     def all_words(self):
         return self.index_word(np.arange(self.size, dtype=np.int64))

@@ -281,18 +281,6 @@ def test_every_csr_row_width_against_the_oracle(mean_len):
         assert np.array_equal(b.map_all(), o.ball_gather(np.arange(n_cand), 1))
 
 
-def test_orbit_search_on_the_engine():
-    """The quotient of C(21,5,2) by Z_21 as a weighted cell on the engine:
-    the orbit search reaches 21 blocks (the reference's own GPU case,
-    tests/test_design_orbits.py:243-249)."""
-    from coldcore_b200.design_orbits import orbit_search
-    from oracle.incidence_oracle import DesignOracle
-    blocks, s, q = orbit_search(21, 5, 2, "cyclic", budget_s=20, seed=1,
-                                notch_budget_s=5, reserve_s=0.0)
-    assert len(blocks) == 21
-    assert DesignOracle(21, 5, 2).verify(blocks)
-
-
 @pytest.mark.late(4)
 @pytest.mark.parametrize("d,n_univ", [(1, 31), (3, 32), (6, 33), (17, 150),
                                       (33, 1000), (70, 27405)])

@@ -120,42 +120,6 @@ def test_deficit_ruin_on_a_design():
     assert s.stats.get("deficit_ruins", 0) > 0
 
 
-def test_cover_file_round_trip(tmp_path):
-    from coldcore_b200.incidence import (design_blocks, read_cover,
-                                         write_cover)
-    v, k = 9, 3
-    rng = np.random.default_rng(5)
-    idx = np.sort(rng.choice(84, 12, replace=False))
-    p = str(tmp_path / "c.txt")
-    write_cover(p, design_blocks(v, k, idx))
-    lines = open(p).read().splitlines()
-    assert len(lines) == 12
-    for ln in lines:
-        vals = [int(x) for x in ln.split()]
-        assert len(vals) == 3 and vals == sorted(vals)
-        assert 1 <= min(vals) and max(vals) <= 9
-    assert np.array_equal(read_cover(p, v, k), idx)
-    with open(p, "a") as fh:
-        fh.write("\n# trailing comment\n")
-    assert np.array_equal(read_cover(p, v, k), idx)
-    with pytest.raises(ValueError):
-        read_cover(p, 9, 4)
-    bad = str(tmp_path / "bad.txt")
-    open(bad, "w").write("1 2 10\n")
-    with pytest.raises(ValueError):
-        read_cover(bad, 9, 3)
-    open(bad, "w").write("1 2 2\n")
-    with pytest.raises(ValueError):
-        read_cover(bad, 9, 3)
-    open(bad, "w").write("# nothing\n\n")
-    assert read_cover(bad, 9, 3).shape == (0,)
-    # the known-optimal Fano-plane cover of C(7,3,2), 1-based
-    fano = str(tmp_path / "fano.txt")
-    open(fano, "w").write("1 2 3\n1 4 5\n1 6 7\n2 4 6\n2 5 7\n3 4 7\n3 5 6\n")
-    from oracle.incidence_oracle import DesignOracle
-    assert DesignOracle(7, 3, 2).verify(read_cover(fano, 7, 3))
-
-
 def test_block_neighbourhoods_and_coverers():
     """The remaining locality hooks of the design layer
     (covering_design.py:231-269), against the design oracle."""
