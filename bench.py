@@ -487,10 +487,10 @@ def measure_lns(args):
     on them; then, from one greedy start, a plain descent (record mix) and
     a learned-ruin descent run for the same wall-time budget.  The ratio is
     the learned run's time to the plain run's best size over the plain
-    run's time to it (coldcore_b200.lns_study runs the multi-seed form)."""
+    run's time to it (harness.lns_study runs the multi-seed form)."""
     from coldcore_b200.gpu import GpuBackend
     from coldcore_b200.learned import RuinFeatures, train_scorer
-    from coldcore_b200.lns_study import evaluate, log_moves
+    from harness.lns_study import evaluate, log_moves
     t0 = time.perf_counter()
     with GpuBackend([3] * 14, 3) as b:
         feats = RuinFeatures(b)
@@ -606,7 +606,7 @@ def run_b200(args, dist):
     if not args.no_incidence and dist.world == 1:
         # the explicit-incidence engine (plugin ABI 2) on a covering design
         def incidence():
-            from coldcore_b200.incidence_bench import measure as inc_measure
+            from harness.incidence_bench import measure as inc_measure
             cpu_field = None
             if not args.no_cpu:
                 from oracle.cport import inc_field

@@ -202,32 +202,48 @@ def locality_order(pats, axes):
         pats[np.argsort(locality_key(pos, dlt, axes), kind="stable")])
 
 
+def _swap_inputs(drops, cands):
+    """Normalise swap_eval's arguments: (drops int64[k], one candidate
+    array per drop, the length of the array every drop shares, or None
+    when each drop has its own)."""
+    drops = np.ascontiguousarray(np.atleast_1d(drops), dtype=np.int64)
+    if isinstance(cands, (list, tuple)):
+        if len(cands) != len(drops):
+            raise ValueError("need one candidate array per drop")
+        return drops, [np.ascontiguousarray(np.atleast_1d(c), dtype=np.int64)
+                       for c in cands], None
+    one = np.ascontiguousarray(np.atleast_1d(cands), dtype=np.int64)
+    return drops, [one] * len(drops), len(one)
+
+
+def _swap_output(loss, gains, shared):
+    """Shared candidates come back as a (k, shared) array, else a list."""
+    if shared is None:
+        return loss, gains
+    return loss, (np.stack(gains) if gains
+                  else np.zeros((0, shared), dtype=np.int32))
+
+
 def swap_eval_generic(backend, drops, cands):
-    """Reference form of ``swap_eval`` for any backend (coldcore
-    ``gpu.py:132-164``): gather role 1 of each drop, then with that drop
-    removed the role-0 gathers of its candidates; cnt is restored."""
-    drops = np.atleast_1d(np.asarray(drops, dtype=np.int64))
-    shared = not isinstance(cands, (list, tuple))
-    parts = ([np.atleast_1d(np.asarray(cands, dtype=np.int64))] * len(drops)
-             if shared else
-             [np.atleast_1d(np.asarray(c, dtype=np.int64)) for c in cands])
-    loss = np.empty(len(drops), dtype=np.int32)
+    """``swap_eval`` composed from the protocol for any backend (the form
+    of coldcore ``gpu.py:132-164``): per drop word its role-1 gather, then,
+    with the word taken out, the role-0 gathers of its candidates; the
+    word is put back, so cnt ends as it started."""
+    drops, parts, shared = _swap_inputs(drops, cands)
+    loss = np.zeros(len(drops), dtype=np.int32)
     gains = []
-    for i, w in enumerate(drops.tolist()):
-        wa = np.array([w], dtype=np.int64)
-        loss[i] = int(backend.ball_gather(wa, 1)[0])
-        if len(parts[i]):
-            backend.ball_update(wa, -1)
-            gains.append(np.asarray(backend.ball_gather(parts[i], 0),
-                                    dtype=np.int32))
-            backend.ball_update(wa, +1)
-        else:
-            gains.append(np.zeros(0, dtype=np.int32))
-    if shared:
-        return loss, (np.stack(gains) if len(gains) else
-                      np.zeros((0, len(parts[0]) if parts else 0),
-                               dtype=np.int32))
-    return loss, gains
+    for i, (w, cand) in enumerate(zip(drops.tolist(), parts)):
+        one = np.array([w], dtype=np.int64)
+        loss[i] = int(backend.ball_gather(one, 1)[0])
+        g = np.zeros(0, dtype=np.int32)
+        if cand.size:
+            backend.ball_update(one, -1)
+            try:
+                g = np.asarray(backend.ball_gather(cand, 0), dtype=np.int32)
+            finally:
+                backend.ball_update(one, +1)
+        gains.append(g)
+    return _swap_output(loss, gains, shared)
 
 
 def ball_update_delta_generic(backend, idx, delta):
@@ -454,49 +470,39 @@ class GpuBackend:
             _p(idx), len(idx), int(delta), ctypes.byref(dd)))
         return int(dd.value)
 
+    #: most drops, and most candidates, one dct_swap_eval call takes (the
+    #: ABI's 65,535-occurrence word check applies to both)
+    SWAP_CAP = (1 << 16) - 1
+
     def swap_eval(self, drops, cands):
         """Exact costs of many swaps without changing state (coldcore
-        ``gpu.py:368-440``): ``(loss, gains)``."""
-        drops = np.ascontiguousarray(np.atleast_1d(drops), dtype=np.int64)
-        k = len(drops)
-        shared = not isinstance(cands, (list, tuple))
-        cap = (1 << 16) - 1
-        if shared:
-            c1 = np.ascontiguousarray(np.atleast_1d(cands), dtype=np.int64)
-            parts = [c1] * k
-        else:
-            if len(cands) != k:
-                raise ValueError("need one candidate array per drop")
-            parts = [np.ascontiguousarray(np.atleast_1d(c), dtype=np.int64)
-                     for c in cands]
-        loss = np.empty(k, dtype=np.int32)
-        gains = [None] * k
-        i = 0
-        while i < k:
-            j, tot = i, 0
-            while j < k and j - i < cap and tot + len(parts[j]) <= cap:
-                tot += len(parts[j])
-                j += 1
-            if j == i:
+        ``gpu.py:368-440``): ``(loss, gains)``.  Drops are sent in runs
+        that stay within ``SWAP_CAP`` drops and ``SWAP_CAP`` candidates."""
+        drops, parts, shared = _swap_inputs(drops, cands)
+        k, cap = len(drops), self.SWAP_CAP
+        ends = np.zeros(k + 1, dtype=np.int64)
+        np.cumsum([len(p) for p in parts], out=ends[1:])
+        loss = np.zeros(k, dtype=np.int32)
+        gains = []
+        lo = 0
+        while lo < k:
+            # the longest run [lo, hi) within both caps
+            hi = min(k, lo + cap,
+                     int(np.searchsorted(ends, ends[lo] + cap, "right")) - 1)
+            if hi <= lo:
                 raise ValueError(f"over {cap} candidates for one drop")
-            cat = (np.concatenate(parts[i:j]) if tot
-                   else np.zeros(1, dtype=np.int64))
-            off = np.zeros(j - i + 1, dtype=np.int64)
-            off[1:] = np.cumsum([len(p) for p in parts[i:j]])
-            g = np.empty(max(tot, 1), dtype=np.int32)
-            lo = np.empty(j - i, dtype=np.int32)
-            sub = np.ascontiguousarray(drops[i:j])
+            base = ends[lo:hi + 1] - ends[lo]
+            flat = (np.concatenate(parts[lo:hi]) if base[-1]
+                    else np.zeros(1, dtype=np.int64))
+            g = np.zeros(max(int(base[-1]), 1), dtype=np.int32)
+            run = np.ascontiguousarray(drops[lo:hi])
             _check("swap_eval", self._lib.dct_swap_eval(
-                _p(sub), j - i, _p(cat), _p(off), _p(g, ctypes.c_int32),
-                _p(lo, ctypes.c_int32)))
-            loss[i:j] = lo
-            for t in range(j - i):
-                gains[i + t] = g[off[t]:off[t + 1]].copy()
-            i = j
-        if shared:
-            return loss, (np.stack(gains) if k
-                          else np.zeros((0, len(c1)), dtype=np.int32))
-        return loss, gains
+                _p(run), hi - lo, _p(flat), _p(np.ascontiguousarray(base)),
+                _p(g, ctypes.c_int32), _p(loss[lo:hi], ctypes.c_int32)))
+            gains.extend(g[base[t]:base[t + 1]].copy()
+                         for t in range(hi - lo))
+            lo = hi
+        return _swap_output(loss, gains, shared)
 
     def loss_owner(self, idx):
         idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)

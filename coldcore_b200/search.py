@@ -9,10 +9,11 @@ This module restates the part of coldcore's search core
 * ``peel``: zero-loss removal in independent batches (search.py:621-670);
 * ``lns``: fixed-M LNS with ``select="fixed"`` (the record mix) or
   ``"adaptive"`` (:class:`OperatorBandit`), search.py:672-784;
-* ``descend``: the notch ladder, v0.2 schedule (search.py:1757-1918);
-* ``anneal``: the swap-neighbourhood polish at fixed M (LAHC or
-  Metropolis), over the "pool" or the local "shell" neighbourhood,
-  costed exactly by the backend's ``swap_eval`` (search.py:787-1360).
+* ``descend``: the notch ladder, v0.2 schedule (search.py:1757-1918).
+
+The swap polish (``anneal``, ``two_swap``) is not restated: it is a caller
+of the engine's ``swap_eval`` / ``ball_update_delta`` fast paths, and
+coldcore's own ``Searcher`` drives those unchanged.
 
 The random draws happen in the reference's order, so with a backend whose
 ``map_extract`` returns ascending indices (the CPU backends) a seeded run
@@ -56,53 +57,49 @@ FIXED_DRAW_DEFICIT = FIXED_DRAW + ("deficit", "deficit")
 #: scan of cnt (search.py:80-81)
 DEFICIT_WORDS = 4
 SCAN_CHUNK = 1 << 24
-#: shell-polish defaults (search.py:70-90): sampled distance-2 words,
-#: top-of-gain draws and uniform draws per move, the cheapest incumbents
-#: a move drops from, the top-gain pool cap and the pool-neighbourhood cap
-SHELL2, SHELL_TOP, SHELL_RAND, SHELL_TOPK = 128, 48, 8, 24
-SHELL_POOL_CAP = 4096
-POOL_CAP = 1 << 14
-
-
 def _rng_for(seed):
     return np.random.default_rng(seed * 1000003 + 12345)
 
 
 class OperatorBandit:
-    """Roulette-wheel ruin-operator choice with a uniform floor
-    (search.py:96-167).
+    """Adaptive ruin-operator choice (coldcore ``search.py:96-167``).
 
-    Each operator's score is an exponential moving average of the reward
-    of its rounds.  The draw is ``floor / k + (1 - floor) * score / sum``.
-    Scores start at the prior mix, scaled to mean 1."""
+    State per operator: ``score``, an exponential moving average of the
+    rewards its rounds earned (weight ``1 - decay`` on the newest), which
+    starts at the prior mix rescaled to mean 1.  A draw mixes the score
+    shares with a uniform ``floor``: P(op) = floor / n + (1 - floor) *
+    score / total.  A hint ``{op: factor}`` multiplies one operator's score,
+    first raised to at least the floor, for that draw only.  Rewards are
+    tiered: a new global best 3, better than the round's start 1, equal
+    0.3, worse 0."""
 
     REWARD_BEST, REWARD_BETTER, REWARD_EQUAL, REWARD_WORSE = 3.0, 1.0, 0.3, 0.0
 
     def __init__(self, rng, ops=RUIN_OPS, floor=0.15, decay=0.9,
                  prior=RUIN_PRIOR):
-        self.ops = list(ops)
         self.rng = rng
-        self.floor, self.decay = float(floor), float(decay)
-        w = np.array([float(prior.get(o, 1.0)) for o in self.ops])
-        self.score = w * (len(w) / w.sum())
-        self.uses = np.zeros(len(self.ops), dtype=np.int64)
-        self.reward = np.zeros(len(self.ops))
+        self.ops = list(ops)
+        self._slot = {op: i for i, op in enumerate(self.ops)}
+        self.floor = float(floor)
+        self.decay = float(decay)
+        n = len(self.ops)
+        start = np.fromiter((float(prior.get(op, 1.0)) for op in self.ops),
+                            dtype=np.float64, count=n)
+        self.score = start * (n / start.sum())
+        self.uses = np.zeros(n, dtype=np.int64)
+        self.reward = np.zeros(n, dtype=np.float64)
 
     def probabilities(self, boost=None):
-        """``boost``: optional {op: factor} hint applied to the scores
-        (lifted to the floor first, so a crushed score can come back)
-        before normalising (search.py:131-149)."""
-        w = np.maximum(self.score, 0.0)
-        k = len(self.ops)
-        if boost:
-            w = w.copy()
-            for op, f in boost.items():
-                if op in self.ops:
-                    i = self.ops.index(op)
-                    w[i] = max(w[i], self.floor) * float(f)
-        if w.sum() <= 0:
-            return np.full(k, 1.0 / k)
-        return self.floor / k + (1.0 - self.floor) * w / w.sum()
+        n = len(self.ops)
+        w = np.clip(self.score, 0.0, None)
+        for op, factor in (boost or {}).items():
+            i = self._slot.get(op)
+            if i is not None:
+                w[i] = max(w[i], self.floor) * float(factor)
+        total = w.sum()
+        if not total > 0:
+            return np.full(n, 1.0 / n)
+        return self.floor / n + (1.0 - self.floor) * w / total
 
     def select(self, boost=None):
         i = int(self.rng.choice(len(self.ops), p=self.probabilities(boost)))
@@ -110,24 +107,25 @@ class OperatorBandit:
         return self.ops[i]
 
     def update(self, op, reward):
-        i = self.ops.index(op)
+        i = self._slot[op]
         self.reward[i] += reward
-        self.score[i] = self.decay * self.score[i] + (1 - self.decay) * reward
+        keep = self.decay
+        self.score[i] = keep * self.score[i] + (1.0 - keep) * reward
 
     @classmethod
     def tier(cls, new_best, pre, post):
-        """Reward of a round: new global best > better > sideways > worse."""
+        """Reward of one round from its outcome."""
         if new_best:
             return cls.REWARD_BEST
-        if post < pre:
-            return cls.REWARD_BETTER
-        return cls.REWARD_EQUAL if post == pre else cls.REWARD_WORSE
+        if post != pre:
+            return cls.REWARD_BETTER if post < pre else cls.REWARD_WORSE
+        return cls.REWARD_EQUAL
 
     def summary(self):
         p = self.probabilities()
-        return {o: {"uses": int(self.uses[i]),
-                    "reward": float(self.reward[i] / max(1, self.uses[i])),
-                    "p": float(p[i])} for i, o in enumerate(self.ops)}
+        mean = self.reward / np.maximum(self.uses, 1)
+        return {op: {"uses": int(self.uses[i]), "reward": float(mean[i]),
+                     "p": float(p[i])} for op, i in self._slot.items()}
 
 
 class Searcher:
@@ -168,8 +166,6 @@ class Searcher:
                       "learned_rounds": 0, "fallback_rounds": 0}
         self._scan_off = 0                 # rotating start of the cnt scan
         self._deficit_cache = (None, None)
-        self._sh1 = None                   # per-axis shell displacements
-        self.stats.update({"moves": 0})
 
     # ------------------------------------------------ state
     def time_left(self):
@@ -340,44 +336,46 @@ class Searcher:
 
     def uncovered_words(self, limit=DEFICIT_WORDS, chunk=SCAN_CHUNK,
                         scan_cap=None):
-        """Up to ``limit`` currently deficient words (search.py:480-528):
-        the backend's own ``deficient_universe`` when it has one, else a
-        chunked scan of cnt from a rotating offset, cached against the
-        solution that produced it.  Empty means none found within the cap,
-        never that nothing is uncovered."""
-        if not self.supports_deficit() or self.uncov == 0:
+        """Up to ``limit`` currently deficient words (coldcore
+        ``search.py:480-528``), ascending.  A backend with its own
+        ``deficient_universe`` answers directly; otherwise cnt is read in
+        chunks from a rotating cursor (so repeated calls at one state see
+        different deficient words), the cursor moving past the last hit and
+        back to 0 after a scan that came up short.  A non-empty answer is
+        memoised for the solution that produced it.  Empty means none was
+        found within ``scan_cap`` words, not that nothing is uncovered."""
+        if self.uncov == 0 or not self.supports_deficit():
             return np.zeros(0, dtype=np.int64)
-        exact = getattr(self.b, "deficient_universe", None)
-        if exact is not None:
-            return np.asarray(exact(limit, self.rng), dtype=np.int64)
-        key = (len(self.code), self.uncov,
-               hash(np.ascontiguousarray(self.code).tobytes()))
-        ckey, cval = self._deficit_cache
-        if ckey == key and cval is not None and len(cval) >= min(
-                limit, self.uncov):
-            return cval[:limit]
-        size = self.b.space.size
+        direct = getattr(self.b, "deficient_universe", None)
+        if direct is not None:
+            return np.asarray(direct(limit, self.rng), dtype=np.int64)
+        state = (len(self.code), self.uncov,
+                 hash(np.ascontiguousarray(self.code).tobytes()))
+        memo_state, memo = self._deficit_cache
+        if (memo_state == state and memo is not None
+                and len(memo) >= min(limit, self.uncov)):
+            return memo[:limit]
+        n = self.b.space.size
         mu = getattr(self.b, "mu", 1)
-        chunk = max(1, int(chunk))
-        budget = size if scan_cap is None else min(size, int(scan_cap))
-        found = []
-        off = int(self._scan_off) % size
-        read = 0
-        while read < budget and len(found) < limit:
-            take = min(chunk, size - off, budget - read)
-            hit = np.flatnonzero(np.asarray(self.b.read_cnt(off, take)) < mu)
-            if len(hit):
-                got = hit[:limit - len(found)] + off
-                found.extend(int(v) for v in got)
-                self._scan_off = (int(got[-1]) + 1) % size
-            read += take
-            off = (off + take) % size
-        if len(found) < limit:
-            self._scan_off = 0                 # exhausted: restart the sweep
-        out = np.array(sorted(found), dtype=np.int64)
-        if len(out):
-            self._deficit_cache = (key, out)
-        return out
+        step = max(1, int(chunk))
+        left = n if scan_cap is None else min(n, int(scan_cap))
+        cursor = int(self._scan_off) % n
+        hits = np.zeros(0, dtype=np.int64)
+        while left > 0 and len(hits) < limit:
+            span = min(step, n - cursor, left)
+            low = np.flatnonzero(np.asarray(self.b.read_cnt(cursor, span))
+                                 < mu)[:limit - len(hits)]
+            if len(low):
+                hits = np.concatenate([hits, low.astype(np.int64) + cursor])
+                self._scan_off = (int(hits[-1]) + 1) % n
+            left -= span
+            cursor = (cursor + span) % n
+        if len(hits) < limit:
+            self._scan_off = 0
+        hits = np.sort(hits)
+        if len(hits):
+            self._deficit_cache = (state, hits)
+        return hits
 
     def _pick(self, k, mode, deficit_pool=3):
         """Positions (into ``self.code``) that ``mode`` removes."""
@@ -642,370 +640,3 @@ class Searcher:
                 step = max(1, step // 2)
                 self.load(solved)
         return M
-
-    # ------------------------------------------------ polish at fixed M
-    def _rng_pass(self, seed):
-        """The stream a pass draws from: the searcher's own, or a fresh
-        one for an explicit seed (search.py:214-229)."""
-        return self.rng if seed is None else _rng_for(seed)
-
-    def _gain_pool(self):
-        """Every word of positive exact gain, up to the pool cap
-        (search.py:787-799)."""
-        self.b.gain_map()
-        self.stats["transforms"] += 1
-        if self.b.map_max() <= 0:
-            return np.zeros(0, dtype=np.int64)
-        cap = min(POOL_CAP, self.b.extract_cap)
-        idx, _v, _f = self.b.map_extract(1, cap=cap)
-        return np.asarray(idx, dtype=np.int64)
-
-    def _top_gain_pool(self, work, cap=SHELL_POOL_CAP):
-        """The top of the gain map, at the histogram threshold that keeps
-        about ``cap`` words, minus the incumbents (search.py:871-902)."""
-        b = self.b
-        b.gain_map()
-        self.stats["transforms"] += 1
-        mx = b.map_max()
-        if mx <= 0:
-            return np.zeros(0, dtype=np.int64)
-        thr = 1
-        if mx > 1 and getattr(b, "supports_hist", True):
-            hist = b.map_hist(1024, mx)
-            csum = np.cumsum(hist[::-1])[::-1]
-            good = np.flatnonzero(csum <= cap)
-            if len(good):
-                thr = max(1, int(good[0]) * mx // 1024 + 1)
-        idx, _v, _f = b.map_extract(thr, cap=min(cap, b.extract_cap))
-        idx = np.asarray(idx, dtype=np.int64)
-        return idx[~np.isin(idx, work)] if len(idx) else idx
-
-    def _shell1(self, idx):
-        """Every word at digit distance 1 from ``idx`` (one coordinate to
-        every other value), or the backend's own radius-1 neighbours
-        (search.py:818-852)."""
-        nb = getattr(self.b, "neighbours", None)
-        if nb is not None:
-            return np.asarray(nb(int(idx), 1), dtype=np.int64)
-        sp = self.b.space
-        if self._sh1 is None:
-            self._sh1 = []
-            for p in range(sp.n):
-                a, pw = int(sp.axes[p]), int(sp.pow_q[p])
-                v = np.arange(a, dtype=np.int64)
-                self._sh1.append(np.stack([(v[v != d] - d) * pw
-                                           for d in range(a)]))
-        d = (idx // np.asarray(sp.pow_q)) % np.asarray(sp.axes, dtype=np.int64)
-        out = [idx + self._sh1[p][d[p]] for p in range(sp.n)]
-        return np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
-
-    def _shell_k(self, idx, k, m, rng):
-        """``m`` sampled words at digit distance <= k (search.py:854-869)."""
-        nb = getattr(self.b, "neighbours", None)
-        if nb is not None:
-            return np.asarray(nb(int(idx), k, m, rng), dtype=np.int64)
-        sp = self.b.space
-        if m <= 0 or k <= 0 or k > sp.n:
-            return np.zeros(0, dtype=np.int64)
-        ax = np.asarray(sp.axes, dtype=np.int64)
-        pw = np.asarray(sp.pow_q, dtype=np.int64)
-        movable = np.flatnonzero(ax > 1)
-        if not len(movable):
-            return np.zeros(0, dtype=np.int64)
-        out = np.full(m, idx, dtype=np.int64)
-        for _ in range(k):
-            p = movable[rng.integers(0, len(movable), size=m)]
-            a = ax[p]
-            v = rng.integers(0, a - 1)
-            cur = (out // pw[p]) % a
-            v = v + (v >= cur)                   # skip the current digit
-            out = out + (v - cur) * pw[p]
-        return out
-
-    def _polish_start(self, M):
-        """Trim or fill to M words and reset the best snapshot."""
-        if len(self.code) > M:
-            self.ruin(len(self.code) - M, "low")
-        if len(self.code) < M and self.uncov > 0:
-            self.greedy_fill(M)
-        self.best_uncov = self.best_code = None
-        self._snapshot()
-
-    def anneal(self, M, budget_s, mode="lahc", t0=1.0, t_end=0.05,
-               lahc_len=50, pool_refresh=64, sample=8, seed=None,
-               log_every=0, neighbourhood="pool", n_shell2=SHELL2,
-               n_top=SHELL_TOP, n_rand=SHELL_RAND, w_topk=SHELL_TOPK,
-               w_random_p=0.25, greedy_p=0.5, loss_refresh=48,
-               restart_stale=15000, verify_every=1):
-        """Swap-neighbourhood polish at fixed M that accepts regressions
-        (search.py:1091-1235).  A move drops one incumbent and adds one
-        candidate, costed exactly: uncov + loss(w) - gain(v | w removed).
-        ``mode`` "lahc" (late acceptance over ``lahc_len`` moves) or
-        "anneal" (Metropolis, geometric cooling ``t0`` -> ``t_end`` over
-        the budget).  ``neighbourhood`` "pool": the cheapest of ``sample``
-        random incumbents against the best of ``sample`` draws from the
-        positive-gain pool; "shell": one of the ``w_topk`` cheapest
-        incumbents against its whole distance-1 shell, sampled distance-2
-        words, top-of-gain and uniform draws, all costed in one
-        ``swap_eval``.  Returns the final uncovered count."""
-        if mode not in ("anneal", "lahc"):
-            raise ValueError(f"unknown polish mode: {mode!r}")
-        if neighbourhood not in ("pool", "shell"):
-            raise ValueError(f"unknown neighbourhood: {neighbourhood!r}")
-        if int(pool_refresh) < 1:
-            raise ValueError("pool_refresh must be >= 1")
-        saved = self.rng
-        self.rng = rng = self._rng_pass(seed)
-        try:
-            self.stats["polish_neighbourhood"] = neighbourhood
-            if neighbourhood == "shell":
-                return self._shift_anneal(
-                    M, budget_s, mode, t0, t_end, lahc_len,
-                    int(pool_refresh), log_every, rng, n_shell2, n_top,
-                    n_rand, w_topk, w_random_p, greedy_p, loss_refresh,
-                    restart_stale, verify_every)
-            return self._pool_anneal(M, budget_s, mode, t0, t_end, lahc_len,
-                                     int(pool_refresh), sample, log_every,
-                                     rng)
-        finally:
-            self.rng = saved
-
-    def _accept_many(self, costs, uncov, bound, mode, t0, t_end, elapsed,
-                     budget_s, rng):
-        if mode == "lahc":
-            return np.flatnonzero(costs <= max(bound, uncov))
-        temp = t0 * (t_end / t0) ** min(1.0, elapsed / max(budget_s, 1e-9))
-        dl = (costs - uncov).astype(np.float64)
-        return np.flatnonzero((dl <= 0) | (rng.random(len(dl)) < np.exp(
-            -np.maximum(dl, 0.0) / max(temp, 1e-9))))
-
-    def _pool_anneal(self, M, budget_s, mode, t0, t_end, lahc_len, period,
-                     sample, log_every, rng):
-        """The "pool" neighbourhood (search.py:1237-1360)."""
-        b = self.b
-        self._polish_start(M)
-        if self.uncov == 0 or not len(self.code):
-            return self.uncov
-        work = np.asarray(self.code, dtype=np.int64).copy()
-        codeset = set(work.tolist())
-        pool = np.zeros(0, dtype=np.int64)
-        since_refresh, starved = period, 0
-        hist = [float(self.uncov)] * max(1, int(lahc_len))
-        t_start = time.time()
-        i = moves = accepts = 0
-        while self.uncov > 0:
-            elapsed = time.time() - t_start
-            if elapsed > budget_s or self.time_left() < self.loop_reserve_s:
-                break
-            if since_refresh >= period or not len(pool):
-                self.code = work
-                pool = self._gain_pool()
-                exact = b.uncovered()
-                if exact != self.uncov:
-                    self.on_log(f"WARNING drift: incremental {self.uncov} "
-                                f"!= field {exact}; adopting field")
-                    self.uncov = exact
-                since_refresh = 0
-                if not len(pool):
-                    break
-            # drop: the cheapest of `sample` random incumbents
-            ns = min(sample, len(work))
-            ridx = rng.choice(len(work), size=ns, replace=False)
-            loss = b.ball_gather(work[ridx], 1).astype(np.float64)
-            j = int(np.argmin(loss + rng.random(ns)))
-            slot = int(ridx[j])
-            w = int(work[slot])
-            wa = np.array([w], dtype=np.int64)
-            b.ball_update(wa, -1)
-            codeset.discard(w)
-            # add: the best of `sample` pool draws, exact gains
-            ns = min(sample, len(pool))
-            draw = pool[rng.integers(0, len(pool), size=ns)]
-            cand = np.array([c for c in draw.tolist()
-                             if c != w and c not in codeset], dtype=np.int64)
-            if not len(cand):                    # stale pool exhausted
-                b.ball_update(wa, +1)
-                codeset.add(w)
-                since_refresh = period
-                pool = np.zeros(0, dtype=np.int64)
-                starved += 1
-                if starved > 2:
-                    break
-                continue
-            starved = 0
-            gain = b.ball_gather(cand, 0).astype(np.float64)
-            g = int(np.argmax(gain + rng.random(len(gain))))
-            v = int(cand[g])
-            b.ball_update(np.array([v], dtype=np.int64), +1)
-            cost = self.uncov + int(loss[j]) - int(gain[g])
-            moves += 1
-            if mode == "lahc":
-                ok = cost <= hist[i % len(hist)] or cost <= self.uncov
-            else:
-                delta = cost - self.uncov
-                temp = t0 * (t_end / t0) ** min(
-                    1.0, elapsed / max(budget_s, 1e-9))
-                ok = delta <= 0 or rng.random() < np.exp(
-                    -delta / max(temp, 1e-9))
-            if ok:
-                work[slot] = v
-                codeset.add(v)
-                self.uncov = cost
-                accepts += 1
-                since_refresh += 1
-                self.code = work
-                self._snapshot()
-            else:
-                b.ball_update(np.array([v], dtype=np.int64), -1)
-                b.ball_update(wa, +1)
-                codeset.add(w)
-            if mode == "lahc":
-                hist[i % len(hist)] = float(self.uncov)
-            i += 1
-            if log_every and i % log_every == 0:
-                self.on_log(f"{mode} M={M} move={i} acc={accepts} "
-                            f"uncov={self.uncov} best={self.best_uncov}")
-        self.stats["moves"] += moves
-        self.stats["accepts"] += accepts
-        return self._polish_end(np.sort(work))
-
-    def _polish_end(self, code):
-        """Adopt the final or the best state, recounted exactly."""
-        self.code = code
-        if self.uncov == 0:
-            self._snapshot()
-        elif self.best_code is not None and self.best_uncov < self.uncov:
-            self.code = np.sort(self.best_code)
-            self.b.recount(self.code)
-            self.stats["transforms"] += 1
-            self.uncov = self.b.uncovered()
-        return self.uncov
-
-    def _shift_anneal(self, M, budget_s, mode, t0, t_end, lahc_len, period,
-                      log_every, rng, n_shell2, n_top, n_rand, w_topk,
-                      w_random_p, greedy_p, loss_refresh, restart_stale,
-                      verify_every):
-        """The "shell" neighbourhood (search.py:904-1089)."""
-        from .gpu import swap_eval_generic
-        b = self.b
-        swap_eval = getattr(b, "swap_eval", None) or (
-            lambda d, c: swap_eval_generic(b, d, c))
-        self._polish_start(M)
-        if self.uncov == 0 or not len(self.code):
-            return self.uncov
-        work = np.sort(np.asarray(self.code, dtype=np.int64)).copy()
-        M = len(work)
-        self.code = work
-        uncov = int(self.uncov)
-        best_u, best_code = uncov, work.copy()
-        losses = self.losses().astype(np.int64)
-        pool = self._top_gain_pool(work)
-        t_start = time.time()
-        since_pool = since_loss = 0
-        hist = [float(uncov)] * max(1, int(lahc_len))
-        i = moves = accepts = drift = stale = 0
-        last_slot = -1
-        while uncov > 0:
-            elapsed = time.time() - t_start
-            if elapsed > budget_s or self.time_left() < self.loop_reserve_s:
-                break
-            # the word to move: one of the cheapest by exact loss, or now
-            # and then a uniform one
-            if rng.random() < w_random_p or len(losses) != M:
-                slot = int(rng.integers(M))
-            else:
-                k = min(int(w_topk), M)
-                cheap = np.argpartition(losses, k - 1)[:k]
-                slot = int(cheap[rng.integers(k)])
-            if slot == last_slot and M > 1:
-                slot = int(rng.integers(M))
-            w = int(work[slot])
-            wa = np.array([w], dtype=np.int64)
-            # candidates that can plug the hole w would leave
-            parts = [self._shell1(w)]
-            if n_shell2:
-                parts.append(self._shell_k(w, 2, int(n_shell2), rng))
-            if n_top and len(pool):
-                parts.append(pool[rng.integers(0, len(pool),
-                                               size=min(int(n_top),
-                                                        len(pool)))])
-            if n_rand:
-                parts.append(rng.integers(0, b.space.size, size=int(n_rand))
-                             .astype(np.int64))
-            cand = np.unique(np.concatenate(parts))
-            cand = cand[(cand != w) & ~np.isin(cand, work)]
-            if not len(cand):
-                i += 1
-                continue
-            # the drop and the whole batch, costed in one read-only call
-            lw_a, g_l = swap_eval(wa, [cand])
-            lw = int(lw_a[0])
-            gains = np.asarray(g_l[0]).astype(np.int64)
-            costs = uncov + lw - gains
-            moves += 1
-            ok = self._accept_many(costs, uncov, hist[i % len(hist)], mode,
-                                   t0, t_end, elapsed, budget_s, rng)
-            if len(ok):
-                if rng.random() < greedy_p:
-                    sub = ok[costs[ok] == costs[ok].min()]
-                    pick = int(sub[rng.integers(len(sub))])
-                else:
-                    pick = int(ok[rng.integers(len(ok))])
-                v = int(cand[pick])
-                b.ball_update(wa, -1)
-                b.ball_update(np.array([v], dtype=np.int64), +1)
-                work[slot] = v
-                uncov = int(costs[pick])
-                accepts += 1
-                since_pool += 1
-                since_loss += 1
-                last_slot = slot
-                if verify_every and accepts % verify_every == 0:
-                    exact = b.uncovered()
-                    if exact != uncov:
-                        drift += 1
-                        uncov = exact
-                if uncov < best_u:
-                    best_u, best_code = uncov, work.copy()
-                    stale = 0
-                    self.code, self.uncov = work, uncov
-                    self._snapshot()
-                    if uncov == 0:
-                        break
-            else:
-                last_slot = -1
-            if mode == "lahc":
-                hist[i % len(hist)] = float(uncov)
-            i += 1
-            stale += 1
-            if restart_stale and stale >= restart_stale:
-                # back to the best state, acceptance history restarted
-                work = best_code.copy()
-                b.recount(work)
-                self.stats["transforms"] += 1
-                uncov = b.uncovered()
-                hist = [float(uncov)] * len(hist)
-                losses = self.losses().astype(np.int64)
-                pool = self._top_gain_pool(work)
-                since_pool = since_loss = stale = 0
-                last_slot = -1
-                continue
-            if since_pool >= period:
-                pool = self._top_gain_pool(work)
-                since_pool = 0
-            if since_loss >= loss_refresh:
-                self.code = work
-                losses = self.losses().astype(np.int64)
-                since_loss = 0
-            if log_every and i % log_every == 0:
-                self.on_log(f"shift M={M} move={i} acc={accepts} "
-                            f"uncov={uncov} best={best_u}")
-        self.stats["moves"] += moves
-        self.stats["accepts"] += accepts
-        self.stats["shift_drift"] = self.stats.get("shift_drift", 0) + drift
-        self.code = np.sort(best_code if best_u < uncov else work)
-        b.recount(self.code)
-        self.stats["transforms"] += 1
-        self.uncov = b.uncovered()
-        self._snapshot()
-        return self.uncov

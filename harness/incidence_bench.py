@@ -9,7 +9,7 @@ cnt read once).  Given another ABI-2 library (``--ref PATH``, e.g. the
 reference's own ``src/plugins/sparse/sparse.cu`` built for sm_100a), its
 kernels are timed in alternation on the same incidence.
 
-    python -m coldcore_b200.incidence_bench [--v 30 --k 8 --t 4 --reps 20]
+    python -m harness.incidence_bench [--v 30 --k 8 --t 4 --reps 20]
                                             [--ref PATH] [--bits]
 
 ``--bits`` also times the role-bit form (``CC_SPARSE_BITS=1``: the role of
@@ -57,7 +57,8 @@ def measure(v=30, k=8, t=4, reps=20, rounds=3, ref_path=None,
     timed over three calls and checked against the engine's field."""
     import torch
 
-    from .incidence import GpuCoveringDesignBackend, GpuIncidenceBackend
+    from coldcore_b200.incidence import (GpuCoveringDesignBackend,
+                                         GpuIncidenceBackend)
     rng = np.random.default_rng(v * 100 + k * 10 + t)
     out = {"design": f"C({v},{k},{t})"}
     with GpuCoveringDesignBackend(v, k, t) as b:

@@ -1,6 +1,6 @@
 """Time-to-size study of the learned ruin proposal against plain LNS.
 
-    python -m coldcore_b200.lns_study --q 3 --n 14 --R 3 --seeds 5 \
+    python -m harness.lns_study --q 3 --n 14 --R 3 --seeds 5 \
         --budget 120 --moves 100000 --out study.json
 
 Steps, all on the GPU engine:
@@ -26,8 +26,9 @@ import time
 
 import numpy as np
 
-from .learned import LearnedRuin, MoveLog, RuinFeatures, train_scorer
-from .search import Searcher
+from coldcore_b200.learned import (LearnedRuin, MoveLog, RuinFeatures,
+                                   train_scorer)
+from coldcore_b200.search import Searcher
 
 
 def greedy_start(b, seed):
@@ -182,7 +183,7 @@ def summarize(runs):
 
 
 def main(argv=None):
-    from .gpu import GpuBackend
+    from coldcore_b200.gpu import GpuBackend
     ap = argparse.ArgumentParser()
     ap.add_argument("--q", type=int, default=3)
     ap.add_argument("--n", type=int, default=14)

@@ -1,15 +1,15 @@
 """Run one cell's transforms a few times — a small, fixed workload for
 ``ncu`` captures and ``DCT_TIMING=1`` per-launch timings.
 
-    python -m coldcore_b200.profile_cell --cell H2_26_3 --mode gain --reps 2
+    python -m harness.profile_cell --cell H2_26_3 --mode gain --reps 2
 
 Prints the launch plan (first axis, axes, algorithmic bytes, kernel id) and,
 with --timing, each launch's device milliseconds and GB/s.
 """
 import argparse
 
-from .gpu import GpuBackend
-from .workloads import CELLS, code_for
+from coldcore_b200.gpu import GpuBackend
+from coldcore_b200.workloads import CELLS, code_for
 
 MODES = {"recount": (0, 2), "gain": (1, 1), "loss": (2, 1)}
 

@@ -28,11 +28,26 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT = os.path.join(OUT_DIR, "libref_covering.so")
 SPARSE_OUT = os.path.join(OUT_DIR, "libref_sparse.so")
-REF_SRC = os.environ.get("COLDCORE_REF_SRC", "/root/reference/src")
+
+
+def ref_src():
+    """The reference checkout's ``src/`` directory: ``COLDCORE_REF_SRC``.
+    Unset means no source here; a prebuilt library is then used as is."""
+    path = os.environ.get("COLDCORE_REF_SRC")
+    if not path:
+        raise FileNotFoundError(
+            "COLDCORE_REF_SRC is unset: point it at the reference "
+            "checkout's src/ directory to build the reference plugins")
+    return path
 
 
 def build(force=False):
-    src = os.path.join(REF_SRC, "plugins", "covering", "dct_hc.cu")
+    try:
+        src = os.path.join(ref_src(), "plugins", "covering", "dct_hc.cu")
+    except FileNotFoundError:
+        if os.path.exists(OUT):
+            return OUT
+        raise
     if not os.path.exists(src):
         if os.path.exists(OUT):
             return OUT                    # prebuilt; no source here
@@ -44,7 +59,7 @@ def build(force=False):
     cmd = ["nvcc", "-O3", "-std=c++17",
            "-gencode", "arch=compute_100a,code=sm_100a",
            "-shared", "-Xcompiler", "-fPIC",
-           "-I", os.path.join(REF_SRC, "include"),
+           "-I", os.path.join(ref_src(), "include"),
            src, "-o", OUT + ".tmp"]
     subprocess.run(cmd, check=True)
     os.replace(OUT + ".tmp", OUT)
@@ -52,7 +67,12 @@ def build(force=False):
 
 
 def build_sparse(force=False):
-    src = os.path.join(REF_SRC, "plugins", "sparse", "sparse.cu")
+    try:
+        src = os.path.join(ref_src(), "plugins", "sparse", "sparse.cu")
+    except FileNotFoundError:
+        if os.path.exists(SPARSE_OUT):
+            return SPARSE_OUT
+        raise
     if not os.path.exists(src):
         if os.path.exists(SPARSE_OUT):
             return SPARSE_OUT

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures from the reference's own CPU backends.
 
-Run in a checkout that has the reference source (default
-``/root/reference/src``, override with ``COLDCORE_REF_SRC``):
+Run in a checkout that has the reference source, with
+``COLDCORE_REF_SRC`` naming its ``src/`` directory:
 
     python tests/golden/make_golden.py            # small fixtures (~1 min)
     python tests/golden/make_golden.py --full     # + full-size checksums
@@ -35,7 +35,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-sys.path.insert(0, os.environ.get("COLDCORE_REF_SRC", "/root/reference/src"))
+REF_SRC = os.environ.get("COLDCORE_REF_SRC")
+if not REF_SRC or not os.path.isdir(os.path.join(REF_SRC, "coldcore")):
+    sys.exit("set COLDCORE_REF_SRC to the reference checkout's src/ "
+             "directory (the one holding the coldcore package)")
+sys.path.insert(0, REF_SRC)
 
 from coldcore.dp import NumpyDPBackend                      # noqa: E402
 from coldcore.gpu import locality_order                      # noqa: E402

@@ -1,8 +1,8 @@
 """Generate ``incidence_golden.npz``: the reference's own explicit-incidence
 backends (coldcore ``src/coldcore/incidence.py``) run on seeded inputs.
 
-Needs the reference source tree on the path (default
-``/root/reference/src``, override with ``COLDCORE_REF_SRC``):
+Needs the reference source tree, with ``COLDCORE_REF_SRC`` naming its
+``src/`` directory:
 
     python tests/golden/make_incidence_golden.py
 
@@ -25,7 +25,11 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, os.environ.get("COLDCORE_REF_SRC", "/root/reference/src"))
+REF_SRC = os.environ.get("COLDCORE_REF_SRC")
+if not REF_SRC or not os.path.isdir(os.path.join(REF_SRC, "coldcore")):
+    sys.exit("set COLDCORE_REF_SRC to the reference checkout's src/ "
+             "directory (the one holding the coldcore package)")
+sys.path.insert(0, REF_SRC)
 
 from coldcore.incidence import (SparseIncidenceBackend,  # noqa: E402
                                 WeightedIncidenceBackend)

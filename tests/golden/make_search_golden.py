@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Golden traces of the reference's search core on its own CPU backend.
 
-Run in a checkout that has the reference source (default
-``/root/reference/src``, override with ``COLDCORE_REF_SRC``):
+Run in a checkout that has the reference source, with
+``COLDCORE_REF_SRC`` naming its ``src/`` directory:
 
     python tests/golden/make_search_golden.py
 
@@ -21,11 +21,6 @@ ascending indices, so a seeded run is deterministic):
 Output: ``search_traces.json`` (committed; nothing at test time reads the
 reference).
 
-With ``--anneal`` it writes ``search_anneal_traces.json``: the
-swap-neighbourhood polish ``anneal(M, ..., mode="lahc")`` over the
-"pool" and "shell" neighbourhoods, one notch below the peeled size (a run
-that does not solve within its budget is marked ``"solved": false``).
-
 With ``--deficit`` it writes ``search_deficit_traces.json`` instead: the
 opt-in deficit-targeted ruin (``ruin(k, "deficit")`` after three ``low``
 removals, so that words are uncovered) and ``lns(..., deficit=True)``
@@ -36,7 +31,11 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.environ.get("COLDCORE_REF_SRC", "/root/reference/src"))
+REF_SRC = os.environ.get("COLDCORE_REF_SRC")
+if not REF_SRC or not os.path.isdir(os.path.join(REF_SRC, "coldcore")):
+    sys.exit("set COLDCORE_REF_SRC to the reference checkout's src/ "
+             "directory (the one holding the coldcore package)")
+sys.path.insert(0, REF_SRC)
 
 from coldcore.dp import NumpyDPBackend                       # noqa: E402
 from coldcore.search import Searcher                          # noqa: E402
@@ -133,34 +132,8 @@ def main_deficit():
         json.dump(out, f)
 
 
-def main_anneal():
-    out = []
-    for problem, axes, R, mu, seed in CELLS:
-        runs = {}
-        for nb in ("pool", "shell"):
-            t = built(problem, axes, R, mu, seed)
-            t.peel()
-            M = len(t.code) - 1
-            t.ruin(1, "low")
-            unc = t.anneal(M, 30.0, mode="lahc", neighbourhood=nb,
-                           log_every=0)
-            runs[nb] = {"M": M, "uncov": int(unc), "solved": unc == 0,
-                        "moves": int(t.stats["moves"]),
-                        "accepts": int(t.stats["accepts"]),
-                        "code": t.code.tolist()}
-        out.append({"problem": problem, "axes": axes, "R": R, "mu": mu,
-                    "seed": seed, "anneal": runs})
-        print(problem, axes, R, mu,
-              {k: (v["uncov"], v["moves"], v["accepts"])
-               for k, v in runs.items()}, flush=True)
-    with open(os.path.join(HERE, "search_anneal_traces.json"), "w") as f:
-        json.dump(out, f)
-
-
 if __name__ == "__main__":
     if "--deficit" in sys.argv:
         main_deficit()
-    elif "--anneal" in sys.argv:
-        main_anneal()
     else:
         main()

@@ -158,7 +158,7 @@ def test_learned_proposal_beats_plain_lns_on_k3_14_3(gpu):
     model is trained here on moves logged from plain runs on other
     seeds."""
     from coldcore_b200.learned import LearnedRuin, RuinFeatures, train_scorer
-    from coldcore_b200.lns_study import (descent, greedy_start, log_moves,
+    from harness.lns_study import (descent, greedy_start, log_moves,
                                          time_to)
     b = gpu.GpuBackend([3] * 14, 3)
     try:

@@ -154,7 +154,7 @@ def test_heldout_rounds_keep_both_labels():
 
 
 def test_time_to_size_target_and_bound():
-    from coldcore_b200.lns_study import summarize, time_to_size
+    from harness.lns_study import summarize, time_to_size
     row = {"start_M": 100,
            "fixed": {"trace": [(0.0, 100)], "best": 100},
            "adaptive": {"trace": [(0.0, 100), (40.0, 99)], "best": 99},

@@ -208,26 +208,3 @@ def test_bandit_boost_hint():
     for _ in range(300):
         b.update("deficit", 0.0)
     assert b.probabilities({"deficit": 4.0})[i] > b.probabilities()[i]
-
-
-with open(os.path.join(HERE, "golden", "search_anneal_traces.json")) as f:
-    ANNEAL_TRACES = json.load(f)
-
-
-@pytest.mark.parametrize("t", ANNEAL_TRACES, ids=_id)
-@pytest.mark.parametrize("nb", ["pool", "shell"])
-def test_anneal_matches_reference(t, nb):
-    """The swap-neighbourhood polish: the same moves, accepts and final
-    code as the reference's own run (LAHC, pool and shell)."""
-    g = t["anneal"][nb]
-    if not g["solved"]:
-        pytest.skip("the reference run hit its time budget (not replayable)")
-    s = _built(t)
-    s.peel()
-    s.ruin(1, "low")
-    unc = s.anneal(g["M"], 120.0, mode="lahc", neighbourhood=nb, log_every=0)
-    assert unc == 0
-    assert s.stats["moves"] == g["moves"]
-    assert s.stats["accepts"] == g["accepts"]
-    assert s.code.tolist() == g["code"]
-    assert s.verify_full() == 0
