@@ -298,6 +298,24 @@ def measure_cell(cell, args, dist, timed=True):
         ms = dist.max(e0.elapsed_time(e1)) / args.steps
         res["clocks"] = clocks.stop() if timed else None
         res["ms"] = ms
+        if timed:
+            # the same steps back to back for at least a second, with its
+            # own clock record: shows the K-step number is the steady one
+            reps = max(args.steps, int(1.2e3 / max(ms, 1e-3)) + 1)
+            sclk = Clocks(dist.local)
+            sclk.start()
+            dist.barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            dist.barrier()
+            sms = dist.max(e0.elapsed_time(e1))
+            res["sustained"] = {"steps": reps, "seconds": round(sms / 1e3, 3),
+                                "ms_per_step": round(sms / reps, 4),
+                                "clocks": sclk.stop()}
         res["value"] = step_model_bytes(cell) * dist.world / (ms * 1e-3) / 1e9
         res["launches_per_step"] = sum(
             len(b.plan(i, o)) for i, o in ((0, 2), (1, 1), (2, 1)))
@@ -535,6 +553,10 @@ def run_b200(args, dist):
     total = sum(r["ms"] for r in rows)
     dom = max(rows, key=lambda r: r["ms"])
     ach = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
+    # the whole step's algorithmic bytes (every launch of the three fused
+    # transforms) over the step time: the achieved DRAM-side rate
+    step_bytes = sum(r["bytes"] for r in rows)
+    step_rate = step_bytes / (res["ms"] * 1e-3) / 1e9
     # keyed by the launch's axes: the capture must be of the same group
     tkey = f"{cell.name}:{dom['transform']}:{dom['axes']}"
     traffic = ncu_traffic(tkey)
@@ -583,6 +605,13 @@ def run_b200(args, dist):
                      "algorithmic_bytes": dom["bytes"],
                      "traffic": traffic},
         "cpu_baseline": cpu,
+        "step_rate": {"algorithmic_bytes": step_bytes,
+                      "GBps": round(step_rate, 1),
+                      "frac": round(step_rate / peak, 4),
+                      "note": "every launch's algorithmic bytes of one step "
+                              "over ms_per_step; value is the one-axis-per-"
+                              "pass model rate"},
+        "sustained": res.get("sustained"),
     }
     if also:
         line["also"] = also
@@ -603,6 +632,12 @@ def run_b200(args, dist):
         leg("lns", lambda: measure_lns(args))
     if not args.no_batch:
         leg("batched_small", lambda: measure_batch_small(args))
+    if not args.no_ops and dist.world == 1:
+        # updates, per-candidate gathers and the Lee / king fields
+        def ops():
+            from harness.ops_bench import measure as ops_measure
+            return ops_measure(cpu=not args.no_cpu)
+        leg("ops", ops)
     if not args.no_incidence and dist.world == 1:
         # the explicit-incidence engine (plugin ABI 2) on a covering design
         def incidence():
@@ -630,6 +665,7 @@ def main():
     ap.add_argument("--no-incidence", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-lns", action="store_true")
+    ap.add_argument("--no-ops", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--lns-budget", type=float, default=60.0)
     ap.add_argument("--lns-moves", type=int, default=30000)

@@ -21,9 +21,19 @@
 //    overlaps on the GPU — two streams, or two host threads — race on it;
 //  * the first call on a device resolves the array's device address with
 //    cudaGetSymbolAddress (the host-side name is only a stand-in), so that
-//    first call should come before any stream capture.
-// No cudaMalloc, cudaFree or other allocating routine is called; the work is
-// queued on the caller's stream and the call returns without waiting.
+//    first call should come before any stream capture;
+//  * with CUDA's default lazy module loading, the array is committed to the
+//    device's memory when this library's kernels are first loaded on that
+//    device, which may be that first call: a caller that reserves the rest
+//    of the device up front should make one small call on every device it
+//    uses before reserving, so that the 64 MiB are already held;
+//  * the looked-up address belongs to the device's current context: after a
+//    cudaDeviceReset of that device, this entry point must not be called
+//    again in the same process.
+// No cudaMalloc, cudaFree or other allocating routine is called; the last
+// group of axes writes the caller's map directly; the work is queued on the
+// caller's stream and the call returns without waiting.
+#include <atomic>
 #include <cstdio>
 
 #include "../../include/coldcore_b200/plugin.h"
@@ -34,23 +44,29 @@ namespace {
 using namespace cc;
 
 constexpr long long kNoAllocWords = 16LL << 20;   // 64 MiB of int32
-constexpr size_t kNoAllocTileBytes = 48 * 1024;   // no opt-in attribute
+// every tile stays within the default 48 KB of dynamic shared memory, so
+// no launch needs the opt-in attribute
+constexpr size_t kNoAllocTileBytes = 48 * 1024;
 constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) int32_t g_noalloc_scratch[kNoAllocWords];
 
-int32_t *g_noalloc_ptr[kMaxDevices];
+// per device: the array's device address, looked up once (host threads may
+// race to look it up; they store the same value)
+std::atomic<int32_t *> g_noalloc_ptr[kMaxDevices];
 
 int noalloc_scratch(int32_t **out) {
   int dev = 0;
   CC_CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return -1;
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    CC_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_ptr[dev] = static_cast<int32_t *>(p);
+  int32_t *p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    void *addr = nullptr;
+    CC_CK(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+    p = static_cast<int32_t *>(addr);
+    g_noalloc_ptr[dev].store(p, std::memory_order_release);
   }
-  *out = g_noalloc_ptr[dev];
+  *out = p;
   return 0;
 }
 
@@ -89,6 +105,9 @@ extern "C" int dct_b200_field_noalloc(int problem, int n, const int *ax,
   const int pmode = mu == 1 ? kPredEq : (role == 0 ? kPredDef : kPredCrit);
   const int ptarget = mu == 1 ? role : 0;
   long long reach = 0;               // distance the processed axes can add
+  // tile words per layer within the shared-memory bound (the runtime-size
+  // kernel keeps R+1 int32 planes of the tile, plus one row of padding)
+  const long long tile_budget = (long long)(kNoAllocTileBytes / 4) / R1 - 32;
   int j = 0;
   while (j < n) {
     GroupArgs a{};
@@ -109,12 +128,17 @@ extern "C" int dct_b200_field_noalloc(int problem, int n, const int *ax,
       const long long outer = space / (a.inner * mid2);
       t.k = a.k + 1;
       t.mid = (int)mid2;
-      t.Bo = a.W >= 32 ? 1 : (int)(outer < 2048 / (a.W * mid2)
-                                        ? outer : 2048 / (a.W * mid2));
+      const long long fit = tile_budget / (a.W * mid2);
+      t.Bo = a.W >= 32 ? 1 : (int)(outer < fit ? outer : fit);
       if (t.Bo < 1) t.Bo = 1;
-      if (a.k > 0 && group_smem_bytes(t, R1) > kNoAllocTileBytes) break;
+      if (group_smem_bytes(t, R1) > kNoAllocTileBytes) break;
       a = t;
       mid = mid2;
+    }
+    if (a.k == 0) {                  // cannot happen for axes <= 16
+      fprintf(stderr, "coldcore_b200: dct_b200_field_noalloc found no "
+              "tile for axis %d\n", j);
+      return -2;
     }
     for (int t = 0; t < a.k; t++) a.qax[t] = ax[j + t];
     a.outer = space / (a.inner * (long long)a.mid);
@@ -127,6 +151,7 @@ extern "C" int dct_b200_field_noalloc(int problem, int n, const int *ax,
     a.lout = (int)(reach2 < R ? reach2 : R) + 1;
     a.src = j == 0 ? kSrcCnt : kSrcLayers;
     a.dst = j + a.k == n ? kDstMap : kDstLayers;
+    a.map = map;                     // the last group writes it directly
     GroupPlan p;
     p.a = a;
     p.kernel = -1;                   // the runtime-size kernel
@@ -140,7 +165,5 @@ extern "C" int dct_b200_field_noalloc(int problem, int n, const int *ax,
     reach = reach2;
     j += a.k;
   }
-  CC_CK(cudaMemcpyAsync(map, scratch, (size_t)space * 4,
-                        cudaMemcpyDeviceToDevice, s));
   return 0;
 }

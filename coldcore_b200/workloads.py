@@ -53,6 +53,9 @@ CELLS = {
     # the learned-LNS cell
     "H3_14_3": Cell("H3_14_3", "hamming", (3,) * 14, 3,
                     cover_size(3 ** 14, _B_H3_14_3, 0.6), 5),
+    # the cell of coldcore's published update / gather latencies (K_8(9,4)
+    # with 940 codewords; |B| = 333,166), here a seeded random code
+    "K8_9_4": Cell("K8_9_4", "hamming", (8,) * 9, 4, 940, 6),
 }
 
 

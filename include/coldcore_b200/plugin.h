@@ -233,7 +233,11 @@ CCP_API int  dct_mlp_free(long long h);
  * `stream` (a cudaStream_t as an integer, 0 = the default stream) without
  * waiting.  Calls share the array: calls that overlap on the GPU race.  The
  * first call on a device looks up the array's address, so make it before
- * any stream capture.  Calls no cudaMalloc / cudaFree. */
+ * any stream capture; under CUDA's lazy module loading the array is also
+ * committed to device memory at the library's first use on that device, so
+ * a caller that reserves the rest of the device should make one small call
+ * first.  After a cudaDeviceReset the entry point must not be used again in
+ * that process.  Calls no cudaMalloc / cudaFree. */
 CCP_API int  dct_b200_field_noalloc(int problem, int n, const int *ax, int R,
                                     int mu, int role, const uint16_t *cnt,
                                     int32_t *map, long long stream);

@@ -3,8 +3,9 @@ the engine's ordinary transform, bit for bit, on two calls in a row.
 
 It serves callers that may not allocate device memory themselves — for
 instance a host framework whose caching allocator must own every buffer —
-so the test hands it buffers allocated by torch and checks that the map it
-writes equals the one dct_transform computes."""
+so the test hands it buffers allocated by torch, checks that the map it
+writes equals the one dct_transform computes, and checks that the device's
+free memory is the same before and after each checked call."""
 import ctypes
 
 import numpy as np
@@ -26,7 +27,9 @@ def _noalloc(lib, problem_id, axes, R, mu, role, cnt_t, map_t, stream):
 
 @pytest.mark.parametrize("problem,pid,axes,R,mu", [
     ("hamming", 0, [3] * 8, 2, 1), ("hamming", 0, [2] * 12, 3, 2),
-    ("lee", 2, [5, 6, 7], 2, 1), ("hamming", 0, [3] * 13, 3, 1)])
+    ("lee", 2, [5, 6, 7], 2, 1), ("hamming", 0, [3] * 13, 3, 1),
+    # a first group of 16-ary axes with seven layers: the tile bound
+    ("hamming", 0, [16] * 4, 6, 1), ("lee", 2, [7] * 6, 4, 2)])
 def test_noalloc_field_matches_transform(problem, pid, axes, R, mu):
     import torch
     lib = load_plugin()
@@ -40,8 +43,12 @@ def test_noalloc_field_matches_transform(problem, pid, axes, R, mu):
             cnt = torch.from_numpy(b.read_cnt().view(np.int16)).cuda()
             out = torch.full((size,), -7, dtype=torch.int32, device="cuda")
             role = call % 2
+            torch.cuda.synchronize()
+            free0, _ = torch.cuda.mem_get_info()
             assert _noalloc(lib, pid, axes, R, mu, role, cnt, out, stream) == 0
             torch.cuda.synchronize()
+            free1, _ = torch.cuda.mem_get_info()
+            assert free1 == free0, "the call changed the device's free memory"
             (b.gain_map if role == 0 else b.loss_map)()
             assert np.array_equal(out.cpu().numpy(), b.map_all())
 
