@@ -62,3 +62,34 @@ def test_bounded_wait_reports_and_recovers():
         o = OracleBackend(list(a), R, problem=p, mu=mu)
         o.recount(code)
         assert np.array_equal(b.cnt(0), o.read_cnt())
+
+
+def test_campaign_of_256_cells_against_golden_digests():
+    """The batched configuration the bench times (256 seeded cells, 292 M
+    words): every cell's cnt, gain and loss maps and scalars, in the
+    persistent graph launch and in one launch per pass, against the digests
+    of tests/golden/batch256_golden.json."""
+    import hashlib
+    import json
+    import os
+
+    def digest(a):
+        return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+    with open(os.path.join(os.path.dirname(__file__), "golden",
+                           "batch256_golden.json")) as f:
+        golden = json.load(f)
+    cells = batch_cells(256, seed=7)
+    with BatchEngine() as b:
+        for p, a, R, code in cells:
+            b.add(p, a, R, code)
+        b.build(0)
+        for mode in (0, 1):
+            b.run(mode)
+            sc = b.scalars()
+            for i, g in enumerate(golden):
+                assert digest(b.cnt(i).astype("<u2")) == g["cnt"], (mode, i)
+                assert digest(b.gain(i).astype("<i4")) == g["gain"], (mode, i)
+                assert digest(b.loss(i).astype("<i4")) == g["loss"], (mode, i)
+                assert tuple(sc[i]) == (g["deficit"], g["gain_max"],
+                                        g["loss_max"]), (mode, i)
