@@ -78,6 +78,22 @@ struct GroupArgs {
   int pair_axis;
   long long *red;         // epilogue reduction target (generic tiles)
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
+  // streamed form (transform_tma.cu): tensor loads into `stages` shared
+  // memory stages, W = 2 x lanes inner words a tile
+  int tma;
+  int stages;
+};
+
+// arguments of a streamed group launch (transform_tma.cu)
+constexpr int kTmaMaxStages = 4;
+struct TmaArgs {
+  uint16_t *layers16;
+  long long plane;
+  int32_t *map;
+  uint16_t *cnt;
+  long long inner, nchunk, ntiles;
+  int lin, lout, stages;
+  int *fault;             // mapped host word, set when a wait runs out
 };
 
 struct GroupPlan {
@@ -129,6 +145,15 @@ int group_kernel_variants(int prob, int q, int R1, int *kids, int *bms,
 // (rounds, skew and grid recomputed; tiles unchanged), the plan itself first
 std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
                                       size_t smem_cap);
+// streamed form of a strided group (transform_tma.cu)
+size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages);
+bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages);
+GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages, int threads);
+int launch_tma_group(const GroupPlan &p, cudaStream_t s);
+int tma_prepare(const GroupPlan &p);
+int tma_blocks_per_sm(const GroupPlan &p);
+int tma_fault_pending();
+void tma_fault_clear();
 int launch_code_bounds(const long long *code, long long ncode,
                        long long tile_words, long long ntiles,
                        long long *bounds, cudaStream_t s);

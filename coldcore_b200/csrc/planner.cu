@@ -232,6 +232,19 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   std::vector<int> rows{p.a.W};
   if (p.a.W == 32 && p.a.Bo == 1 && p.a.inner >= 32 && !p.a.pair_axis)
     rows.push_back(16);
+  // the streamed form (tensor loads into shared-memory stages) where the
+  // group qualifies: 32 or 64-word rows, 2 or 3 stages, 256 or 512 threads
+  const char *tma_env = getenv("CC_TMA");
+  const bool tma_off = tma_env && atoi(tma_env) == 0;
+  for (int lanes : {16, 32})
+    for (int stages : {2, 3})
+      if (!tma_off && tma_group_ok(tma_variant(p, lanes, stages, 256).a, q, R1, lanes,
+                       stages))
+        for (int th : {256, 512}) {
+          GroupPlan v = tma_variant(p, lanes, stages, th);
+          v.grid = occupancy_grid(v);
+          out.push_back(v);
+        }
   for (int W : rows)
   for (int i = 0; i < nk; i++)
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {

@@ -346,6 +346,25 @@ Plan build_group_plan(int src, int dst, Knobs kn) {
   Geometry g = S.g;
   g.mu = g_mu;
   P.groups = plan_groups(g, S.R1, ptr, src, dst, kn);
+  // CC_TMA=1: every group the streamed form serves takes it (64-word rows
+  // first, three stages where they fit); the autotuner otherwise times it
+  // beside the other forms
+  const char *te = getenv("CC_TMA");
+  if (te && atoi(te) == 1) {
+    for (auto &p : P.groups) {
+      if (p.kernel < 0 || p.a.nrounds <= 0) continue;
+      bool done = false;
+      for (int lanes : {32, 16})
+        for (int stages : {3, 2}) {
+          if (done) break;
+          GroupPlan v = tma_variant(p, lanes, stages, 256);
+          if (tma_group_ok(v.a, p.a.rq[0], S.R1, lanes, stages)) {
+            p = v;
+            done = true;
+          }
+        }
+    }
+  }
   return P;
 }
 
@@ -453,6 +472,13 @@ int run_streamed(int init_mode, int out_mode) {
 }
 
 int run_transform(int init_mode, int out_mode) {
+  if (tma_fault_pending()) {
+    // an earlier streamed launch gave up waiting for its tile loads
+    tma_fault_clear();
+    fprintf(stderr, "coldcore_b200: a streamed group launch timed out "
+            "waiting for its tensor loads\n");
+    return -8;
+  }
   if (S.streamed) return run_streamed(init_mode, out_mode);
   Plan &P = plan_for(init_mode, out_mode);
   int pm, pt;
@@ -550,7 +576,9 @@ int tune_launches(Plan &P, int init_mode, int out_mode, cudaEvent_t e0,
       p.a.ncode = S.codeM;
       p.a.code_bounds = S.d_bounds;
       if ((rc = prepare_group(p))) return rc;
-      if ((rc = launch_group(p, g_stream))) return rc;
+      rc = launch_group(p, g_stream);
+      if (rc == -9) { rc = 0; continue; }     // a form the launcher refused
+      if (rc) return rc;
       CC_CK(cudaEventRecord(e0, g_stream));
       for (int r = 0; r < 3; r++)
         if ((rc = launch_group(p, g_stream))) return rc;
@@ -1643,7 +1671,7 @@ int dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap) {
     if (forms && n < cap)
       forms[n] = (p.a.pipe ? 1 : 0) | (p.a.pack ? 2 : 0) |
                  (p.a.in16 ? 4 : 0) | (p.a.out16 ? 8 : 0) |
-                 (p.a.pair_axis ? 16 : 0);
+                 (p.a.pair_axis ? 16 : 0) | (p.a.tma ? 32 : 0);
     n++;
   }
   return n;

@@ -1043,6 +1043,7 @@ static GroupFn group_fn(const GroupPlan &p) {
 // per-block limit counts the kernel's static shared memory too).  The
 // opt-in only ever grows, so one launch never lowers another's.
 int ensure_group_smem(const GroupPlan &p) {
+  if (p.a.tma) return tma_prepare(p);
   static size_t attr_set[2 * 64 + 1];
   const int slot = p.kernel < 0 ? 128 : p.kernel + (p.a.pipe ? 64 : 0);
   if (p.smem > 48 * 1024 && p.smem > attr_set[slot]) {
@@ -1068,6 +1069,7 @@ int group_blocks_per_sm(const GroupPlan &p) {
     cudaGetLastError();
   }
   if (!have_device) return 0;
+  if (p.a.tma) return tma_blocks_per_sm(p);
   if (ensure_group_smem(p)) return 0;
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -1088,6 +1090,7 @@ bool pipe_pairs_ok(const GroupArgs &a) {
 }
 
 int launch_group(const GroupPlan &p, cudaStream_t s) {
+  if (p.a.tma) return launch_tma_group(p, s);
   // packed pairs need 4-byte aligned pair accesses: an even inner stride
   // and row width, 16-bit planes in, a register kernel with a packed form
   // (Hamming q <= 3, Lee), and prefetching only in its 16-byte form

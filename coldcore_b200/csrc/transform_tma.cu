@@ -1,0 +1,532 @@
+// transform_tma.cu — strided axis groups of the distance-layer families,
+// streamed through shared memory by the Tensor Memory Accelerator.
+//
+// The group kernels of transform_group.cu load each tile into registers
+// with ordinary loads, so the bytes a CTA keeps in flight are bounded by
+// its register blocks: the large launches of H2(26,3) ran latency-bound at
+// about half of the HBM bandwidth.  Here a group over 16-bit layer planes
+// (two inner words per 32-bit lane) is split into a producer and the
+// compute rounds:
+//
+//   * one thread issues, per tile, ONE tiled bulk tensor load (TMA) of the
+//     tile's live layers — W inner words x mid x lin planes — into one of
+//     S shared-memory stages, completing on that stage's mbarrier; the
+//     loads of the next S-1 tiles are in flight while a tile computes;
+//   * the rounds run in place on the stage (register blocks of Q^b words
+//     per lane, every shared-memory offset a compile-time constant); the
+//     last round writes HBM directly: the u16 layers, the int32 map or the
+//     u16 cnt, 32 lanes x 4 bytes (or 8) per warp store;
+//   * a stage is refilled once every thread has passed the barrier that
+//     ends its last round.
+//
+// Every wait is bounded: a tile whose bytes have not landed within about
+// two seconds (the GPU's global timer) stops the CTA, records a fault that
+// the host sees in mapped host memory, and drains its own outstanding
+// loads (again bounded) before returning.  No cluster multicast is used;
+// the tensor maps cover this GPU's own layer planes only.
+//
+// Recurrence (coldcore src/plugins/covering/dctcore_hamming.cuh:4-8):
+// newA_d[a] = A_d[a] + sum of the fibre's other entries of layer d-1.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "engine.h"
+
+namespace cc {
+namespace {
+
+constexpr size_t kTmaSmemMax = 227 * 1024;
+constexpr unsigned long long kTmaWaitNs = 2000000000ULL;   // 2 s
+constexpr unsigned long long kTmaDrainNs = 200000000ULL;   // 0.2 s
+
+template <int Q, int E>
+struct P { static constexpr int v = Q * P<Q, E - 1>::v; };
+template <int Q>
+struct P<Q, 0> { static constexpr int v = 1; };
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t saddr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(saddr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+          saddr(bar)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// true once the phase of `parity` has completed; false after `limit` ns
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          unsigned long long limit) {
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  for (unsigned it = 1;; it++) {
+    if (mbar_test(bar, parity)) return true;
+    if ((it & 255) == 0 && now_ns() - t0 > limit) return false;
+  }
+}
+__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *map,
+                                          uint64_t *bar, int c0, int c1,
+                                          int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::"
+      "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
+          saddr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2),
+      "r"(c3), "r"(saddr(bar))
+      : "memory");
+}
+
+// ------------------------------------------------------------ axis math
+// One Hamming axis over a register block: the fibres are the Q entries at
+// element stride ST; layers descend so layer d-1 is read before it changes.
+template <int Q, int R1, int QB, int ST>
+__device__ __forceinline__ void ham_axis(uint32_t (&v)[R1][QB]) {
+#pragma unroll
+  for (int e = 0; e < QB; e++) {
+    if ((e / ST) % Q != 0) continue;
+#pragma unroll
+    for (int d = R1 - 1; d >= 1; d--) {
+      if (Q == 2) {
+        const uint32_t a0 = v[d - 1][e], a1 = v[d - 1][e + ST];
+        v[d][e] += a1;
+        v[d][e + ST] += a0;
+      } else {
+        const uint32_t a0 = v[d - 1][e], a1 = v[d - 1][e + ST],
+                       a2 = v[d - 1][e + 2 * ST];
+        v[d][e] += a1 + a2;
+        v[d][e + ST] += a0 + a2;
+        v[d][e + 2 * ST] += a0 + a1;
+      }
+    }
+  }
+}
+
+template <int Q, int R1, int B, int T>
+struct Axes {
+  static __device__ __forceinline__ void run(uint32_t (&v)[R1][P<Q, B>::v]) {
+    ham_axis<Q, R1, P<Q, B>::v, P<Q, T>::v>(v);
+    Axes<Q, R1, B, T + 1>::run(v);
+  }
+};
+template <int Q, int R1, int B>
+struct Axes<Q, R1, B, B> {
+  static __device__ __forceinline__ void run(uint32_t (&)[R1][P<Q, B>::v]) {}
+};
+
+// axes per register round: Q^b x R1 registers at most 64
+template <int Q, int R1>
+struct RoundAxes {
+  static constexpr int v = (P<Q, 4>::v * R1 <= 64) ? 4
+                           : (P<Q, 3>::v * R1 <= 64) ? 3
+                           : (P<Q, 2>::v * R1 <= 64) ? 2 : 1;
+};
+
+// ------------------------------------------------------------ one round
+// Round over axes [A, A + B) of the group on a stage of L lanes x MID mid
+// positions x R1 layers (32-bit packed lanes, layer-major as the tensor
+// load lays it down).  FIRST: layers >= lin start at zero.  LAST: the
+// block goes to HBM (OUT 0 layers, 1 map, 2 cnt) instead of the stage.
+template <int Q, int K, int R1, int L, int OUT, int A, int B, bool FIRST,
+          bool LAST>
+__device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
+                                          long long o, long long i0) {
+  constexpr int MID = P<Q, K>::v;
+  constexpr int QB = P<Q, B>::v;
+  constexpr int QA = P<Q, A>::v;
+  constexpr int NB = L * MID / QB;            // register blocks in the tile
+  for (int blk = threadIdx.x; blk < NB; blk += blockDim.x) {
+    const int l = blk % L;
+    const int rest = blk / L;                 // mid digits outside [A, A+B)
+    const int mb = rest % QA + (rest / QA) * (QA * QB);
+    uint32_t *p = st + mb * L + l;
+    uint32_t v[R1][QB];
+#pragma unroll
+    for (int d = 0; d < R1; d++) {
+      const bool live = !FIRST || d < a.lin;
+#pragma unroll
+      for (int e = 0; e < QB; e++)
+        v[d][e] = live ? p[(d * MID + e * QA) * L] : 0u;
+    }
+    Axes<Q, R1, B, 0>::run(v);
+    if (!LAST) {
+#pragma unroll
+      for (int d = 0; d < R1; d++)
+#pragma unroll
+        for (int e = 0; e < QB; e++) p[(d * MID + e * QA) * L] = v[d][e];
+      continue;
+    }
+    // HBM word of element e: o*(MID*inner) + (mb + e*QA)*inner + i0 + 2l
+    const long long x0 = (o * MID + mb) * a.inner + i0 + 2 * l;
+    const long long step = (long long)QA * a.inner;
+    if (OUT == 0) {
+#pragma unroll
+      for (int d = 0; d < R1; d++) {
+        if (d >= a.lout) break;
+        uint16_t *q = a.layers16 + d * a.plane + x0;
+#pragma unroll
+        for (int e = 0; e < QB; e++)
+          __stcs(reinterpret_cast<unsigned *>(q + e * step), v[d][e]);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int d = 0; d < R1; d++) s += v[d][e];
+        if (OUT == 1)
+          __stcs(reinterpret_cast<int2 *>(a.map + x0 + e * step),
+                 make_int2((int)(s & 0xFFFFu), (int)(s >> 16)));
+        else
+          *reinterpret_cast<unsigned *>(a.cnt + x0 + e * step) = s;
+      }
+    }
+  }
+}
+
+// The rounds of a K-axis group: RoundAxes-sized rounds from axis 0 up, the
+// remainder last.
+template <int Q, int K, int R1, int L, int OUT, int A>
+struct Rounds {
+  static constexpr int BM = RoundAxes<Q, R1>::v;
+  static constexpr int B = (K - A) < BM ? (K - A) : BM;
+  static __device__ __forceinline__ void run(uint32_t *st, const TmaArgs &a,
+                                             long long o, long long i0) {
+    tma_round<Q, K, R1, L, OUT, A, B, A == 0, A + B == K>(st, a, o, i0);
+    if (A + B < K) __syncthreads();
+    Rounds<Q, K, R1, L, OUT, (A + B < K ? A + B : K)>::run(st, a, o, i0);
+  }
+};
+template <int Q, int K, int R1, int L, int OUT>
+struct Rounds<Q, K, R1, L, OUT, K> {
+  static __device__ __forceinline__ void run(uint32_t *, const TmaArgs &,
+                                             long long, long long) {}
+};
+
+// stage stride: the tile's words rounded up to 1 KB (tensor loads land on
+// 128-byte-aligned shared addresses)
+template <int Q, int K, int R1, int L>
+struct Stage {
+  static constexpr int words = (R1 * P<Q, K>::v * L + 255) / 256 * 256;
+};
+
+template <int Q, int K, int R1, int L, int OUT>
+__global__ void __launch_bounds__(512)
+tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
+  extern __shared__ __align__(128) uint8_t dyn[];
+  constexpr int MID = P<Q, K>::v;
+  constexpr int SW = Stage<Q, K, R1, L>::words;
+  const int S = a.stages;
+  // stages on a 1 KB boundary, then the barriers and the stop flag
+  uint8_t *base = dyn + ((1024u - (saddr(dyn) & 1023u)) & 1023u);
+  uint32_t *stage = reinterpret_cast<uint32_t *>(base);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + (size_t)S * SW * 4);
+  volatile int *stop = reinterpret_cast<volatile int *>(bar + kTmaMaxStages);
+  const uint32_t bytes = (uint32_t)(2 * L * 2) * MID * a.lin;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) mbar_init(&bar[s]);
+    *stop = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const long long grid = gridDim.x;
+  auto issue = [&](long long t, int s) {
+    const int i0 = (int)((t % a.nchunk) * (2 * L));
+    const int o = (int)(t / a.nchunk);
+    mbar_expect(&bar[s], bytes);
+    tma_load4(stage + (size_t)s * SW, &map, &bar[s], i0, 0, o, 0);
+  };
+  if (threadIdx.x == 0) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(
+                     reinterpret_cast<uint64_t>(&map))
+                 : "memory");
+    for (int s = 0; s < S; s++) {
+      const long long t = blockIdx.x + s * grid;
+      if (t < a.ntiles) issue(t, s);
+    }
+  }
+  long long it = 0;
+  long long t = blockIdx.x;
+  for (; t < a.ntiles; it++, t += grid) {
+    const int s = (int)(it % S);
+    const uint32_t parity = (uint32_t)((it / S) & 1);
+    if (!mbar_wait(&bar[s], parity, kTmaWaitNs)) *stop = 1;
+    __syncthreads();
+    if (*stop) break;
+    const long long o = t / a.nchunk;
+    const long long i0 = (t % a.nchunk) * (2 * L);
+    Rounds<Q, K, R1, L, OUT, 0>::run(stage + (size_t)s * SW, a, o, i0);
+    __syncthreads();                          // stage s is free again
+    if (threadIdx.x == 0) {
+      const long long nt = t + S * grid;
+      if (nt < a.ntiles) {
+        // the rounds wrote the stage through the generic proxy; order those
+        // writes before the tensor load overwrites it
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        issue(nt, s);
+      }
+    }
+  }
+  if (t < a.ntiles && threadIdx.x == 0) {
+    // a load never completed: report, then wait (bounded) for every load
+    // this CTA still has outstanding before the CTA's memory goes away
+    *a.fault = 1;
+    __threadfence_system();
+    for (long long k = it; k < it + S; k++) {
+      const long long tk = blockIdx.x + k * grid;
+      if (tk >= a.ntiles) break;
+      mbar_wait(&bar[k % S], (uint32_t)((k / S) & 1), kTmaDrainNs);
+    }
+  }
+}
+
+// ------------------------------------------------------------ dispatch
+typedef void (*TmaFn)(const CUtensorMap, const TmaArgs);
+
+struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; };
+
+#define TE(Q, K, R1, L)                                                     \
+  {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0>},                              \
+  {Q, K, R1, L, 1, tma_group<Q, K, R1, L, 1>},                              \
+  {Q, K, R1, L, 2, tma_group<Q, K, R1, L, 2>}
+const TmaEntry kTma[] = {
+    TE(2, 5, 4, 16), TE(2, 6, 4, 16), TE(2, 7, 4, 16), TE(2, 8, 4, 16),
+    TE(2, 5, 4, 32), TE(2, 6, 4, 32), TE(2, 7, 4, 32),
+    TE(3, 3, 5, 16), TE(3, 4, 5, 16), TE(3, 5, 5, 16),
+    TE(3, 3, 5, 32), TE(3, 4, 5, 32),
+    TE(3, 3, 4, 16), TE(3, 4, 4, 16), TE(3, 5, 4, 16),
+    TE(3, 3, 4, 32), TE(3, 4, 4, 32),
+};
+#undef TE
+
+const TmaEntry *find_tma(int q, int k, int r1, int lanes, int out) {
+  for (const auto &e : kTma)
+    if (e.q == q && e.k == k && e.r1 == r1 && e.lanes == lanes &&
+        e.out == out)
+      return &e;
+  return nullptr;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p,
+                                cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// the fault word: mapped pinned host memory the kernels write through
+int *g_fault_host = nullptr;
+int *g_fault_dev = nullptr;
+
+int fault_word(int **dev) {
+  static std::once_flag once;
+  static int rc = 0;
+  std::call_once(once, [] {
+    void *h = nullptr;
+    if (cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped) != cudaSuccess) {
+      cudaGetLastError();
+      rc = -1;
+      return;
+    }
+    g_fault_host = static_cast<int *>(h);
+    *g_fault_host = 0;
+    void *d = nullptr;
+    if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+      cudaGetLastError();
+      rc = -1;
+      return;
+    }
+    g_fault_dev = static_cast<int *>(d);
+  });
+  *dev = g_fault_dev;
+  return rc;
+}
+
+}  // namespace
+
+size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages) {
+  long long mid = 1;
+  for (int i = 0; i < k; i++) mid *= q;
+  const long long words = (r1 * mid * lanes + 255) / 256 * 256;
+  return (size_t)stages * words * 4 + 1024 + kTmaMaxStages * 8 + 16;
+}
+
+// The groups the streamed form serves: binary or ternary Hamming groups
+// over 16-bit planes in packed pairs (16-bit planes, the map or cnt out),
+// one tile per W inner words x the whole group, an instantiated (q, k,
+// layers, lanes) and its stages within 227 KB of shared memory.
+bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
+  if (stages < 2 || stages > kTmaMaxStages || !encode_fn()) return false;
+  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  if (!find_tma(q, a.k, r1, lanes, out)) return false;
+  if (a.prob != kHamming || !a.pack || !a.in16 || a.pair_axis ||
+      a.src != kSrcLayers || a.R + 1 != r1)
+    return false;
+  if (out == 0 && !a.out16) return false;
+  if (a.inner % (2 * lanes) || a.plane % 8 || a.lin < 1 || a.lin > r1)
+    return false;
+  if ((reinterpret_cast<uintptr_t>(a.layers16) & 15) != 0) return false;
+  if (a.outer >= (1LL << 31) || a.inner >= (1LL << 31)) return false;
+  return tma_smem_bytes(q, a.k, r1, lanes, stages) <= kTmaSmemMax;
+}
+
+// The same group as a streamed launch: W = 2 x lanes inner words a tile.
+GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages,
+                      int threads) {
+  GroupPlan v = p;
+  v.a.tma = 1;
+  v.a.stages = stages;
+  v.a.pipe = 0;
+  v.a.W = 2 * lanes;
+  v.a.Bo = 1;
+  v.a.nchunk = (v.a.inner + v.a.W - 1) / v.a.W;
+  v.a.ntiles = v.a.outer * v.a.nchunk;
+  v.threads = threads;
+  v.smem = tma_smem_bytes(v.a.rq[0] ? v.a.rq[0] : v.a.qax[0], v.a.k,
+                          v.a.R + 1, lanes, stages);
+  v.grid = 0;
+  return v;
+}
+
+int tma_fault_pending() {
+  return g_fault_host && *(volatile int *)g_fault_host ? 1 : 0;
+}
+
+void tma_fault_clear() {
+  if (g_fault_host) *(volatile int *)g_fault_host = 0;
+}
+
+namespace {
+
+const TmaEntry *entry_of(const GroupPlan &p) {
+  const GroupArgs &a = p.a;
+  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  return find_tma(a.rq[0] ? a.rq[0] : a.qax[0], a.k, a.R + 1, a.W / 2, out);
+}
+
+// opt every streamed kernel in to the largest dynamic shared memory once
+int opt_in(const TmaEntry *e) {
+  static std::mutex mu;
+  static bool done[sizeof(kTma) / sizeof(kTma[0])];
+  std::lock_guard<std::mutex> g(mu);
+  const size_t idx = (size_t)(e - kTma);
+  if (!done[idx]) {
+    CC_CK(cudaFuncSetAttribute((const void *)e->fn,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTmaSmemMax));
+    done[idx] = true;
+  }
+  return 0;
+}
+
+}  // namespace
+
+int tma_prepare(const GroupPlan &p) {
+  const TmaEntry *e = entry_of(p);
+  if (!e) return -9;
+  return opt_in(e);
+}
+
+int tma_blocks_per_sm(const GroupPlan &p) {
+  const TmaEntry *e = entry_of(p);
+  if (!e || opt_in(e)) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, (const void *)e->fn, p.threads, p.smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
+  const GroupArgs &a = p.a;
+  const int q = a.rq[0] ? a.rq[0] : a.qax[0];
+  const int lanes = a.W / 2;
+  const TmaEntry *e = entry_of(p);
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!e || !enc || a.stages < 2 || a.stages > kTmaMaxStages) return -9;
+  int *fault = nullptr;
+  if (fault_word(&fault)) return -9;
+  int rc = opt_in(e);
+  if (rc) return rc;
+  long long mid = 1;
+  for (int i = 0; i < a.k; i++) mid *= q;
+  // the live layers as a 4-D u16 tensor: inner word, mid, outer, layer
+  CUtensorMap map;
+  const cuuint64_t dims[4] = {(cuuint64_t)a.inner, (cuuint64_t)mid,
+                              (cuuint64_t)a.outer, (cuuint64_t)a.lin};
+  const cuuint64_t strides[3] = {(cuuint64_t)a.inner * 2,
+                                 (cuuint64_t)(a.inner * mid) * 2,
+                                 (cuuint64_t)a.plane * 2};
+  const cuuint32_t box[4] = {(cuuint32_t)(2 * lanes), (cuuint32_t)mid, 1,
+                             (cuuint32_t)a.lin};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+                          a.layers16, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) {
+    fprintf(stderr, "coldcore_b200: tensor map encode failed (%d)\n",
+            (int)cr);
+    return -9;
+  }
+  TmaArgs t{};
+  t.layers16 = a.layers16;
+  t.plane = a.plane;
+  t.map = a.map ? a.map : a.layers;
+  t.cnt = a.cnt;
+  t.inner = a.inner;
+  t.nchunk = a.nchunk;
+  t.ntiles = a.ntiles;
+  t.lin = a.lin;
+  t.lout = a.lout;
+  t.stages = a.stages;
+  t.fault = fault;
+  const size_t smem = tma_smem_bytes(q, a.k, a.R + 1, lanes, a.stages);
+  int grid = p.grid;
+  if (grid < 1) {
+    const int per_sm = tma_blocks_per_sm(p);
+    long long gr = (long long)sm_count() * (per_sm < 1 ? 1 : per_sm);
+    if (gr > a.ntiles) gr = a.ntiles;
+    grid = (int)(gr < 1 ? 1 : gr);
+  }
+  e->fn<<<grid, p.threads, smem, s>>>(map, t);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace cc

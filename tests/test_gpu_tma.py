@@ -1,0 +1,43 @@
+"""The streamed form of the strided groups (tensor loads into shared-memory
+stages, transform_tma.cu) against the oracle: with CC_TMA=1 every group it
+serves takes it; recount, gain and loss fields must equal the oracle's,
+bit for bit, for binary and ternary Hamming cells, mu = 1 and 2."""
+import numpy as np
+import pytest
+
+from coldcore_b200.gpu import GpuBackend
+from oracle.dp_oracle import OracleBackend
+
+pytestmark = pytest.mark.gpu
+
+TMA = 32                                 # GpuBackend.plan_forms bit
+
+
+@pytest.mark.parametrize("axes,R,mu", [
+    ([2] * 20, 3, 1), ([2] * 21, 3, 2), ([2] * 16, 3, 1),
+    ([3] * 13, 4, 1), ([3] * 12, 3, 1), ([3] * 11, 4, 2)])
+def test_streamed_groups_match_the_oracle(monkeypatch, axes, R, mu):
+    monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_TUNE", "0")
+    size = int(np.prod(axes))
+    rng = np.random.default_rng(size % 1000 + R)
+    code = np.sort(rng.choice(size, size=size // 200, replace=False))
+    o = OracleBackend(axes, R, mu=mu)
+    with GpuBackend(axes, R, mu=mu) as b:
+        used = 0
+        for step in range(2):
+            if step:
+                code = np.sort(rng.choice(size, size=size // 150,
+                                          replace=False))
+            b.recount(code)
+            o.recount(code)
+            assert np.array_equal(b.read_cnt(), o.read_cnt()), step
+            b.gain_map()
+            o.gain_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            b.loss_map()
+            o.loss_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            for im, om in ((0, 2), (1, 1), (2, 1)):
+                used += int(np.count_nonzero(b.plan_forms(im, om) & TMA))
+        assert used > 0, "no launch took the streamed form"
