@@ -79,7 +79,8 @@ struct GroupArgs {
   long long *red;         // epilogue reduction target (generic tiles)
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
   // streamed form (transform_tma.cu): tensor loads into `stages` shared
-  // memory stages, W = 2 x lanes inner words a tile
+  // memory stages, W = 2 x lanes inner words a tile (tma 1); the first
+  // group staged from cnt by bulk copies (tma 2)
   int tma;
   int stages;
 };
@@ -94,6 +95,9 @@ struct TmaArgs {
   long long inner, nchunk, ntiles;
   int lin, lout, stages;
   int *fault;             // mapped host word, set when a wait runs out
+  // first group (tma_first): the cnt source and its predicate
+  const uint16_t *cnt_in;
+  int pmode, ptarget, mu;
 };
 
 struct GroupPlan {
@@ -149,6 +153,10 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
 size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages);
 bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages);
 GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages, int threads);
+// the first group read from cnt (axis 0 in the pair), a.tma == 2
+size_t tma_first_smem_bytes(int kk, int r1, int stages);
+bool tma_first_ok(const GroupArgs &a, int r1, int stages);
+GroupPlan tma_first_variant(const GroupPlan &p, int stages, int threads);
 int launch_tma_group(const GroupPlan &p, cudaStream_t s);
 int tma_prepare(const GroupPlan &p);
 int tma_blocks_per_sm(const GroupPlan &p);

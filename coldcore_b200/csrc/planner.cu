@@ -245,6 +245,13 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
           v.grid = occupancy_grid(v);
           out.push_back(v);
         }
+  for (int stages : {2, 3})
+    if (!tma_off && tma_first_ok(p.a, R1, stages))
+      for (int th : {256, 512}) {
+        GroupPlan v = tma_first_variant(p, stages, th);
+        v.grid = occupancy_grid(v);
+        out.push_back(v);
+      }
   for (int W : rows)
   for (int i = 0; i < nk; i++)
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {

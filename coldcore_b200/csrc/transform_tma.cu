@@ -302,6 +302,198 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
   }
 }
 
+// ------------------------------------------------------------ first group
+// The first group of a binary Hamming cell read from cnt: a tile is the
+// contiguous range of 2^(KK+1) words; axis 0 is the word pair inside each
+// 32-bit lane (a 16-bit rotate-and-add), axes 1..KK are bits 0..KK-1 of the
+// lane index p.  One bulk copy stages the tile's cnt (2 bytes a word) per
+// stage; the rounds work on one shared buffer of R1 layers, padded one word
+// per 16 lanes (p + p/16), so that 16-lane register blocks are free of bank
+// conflicts; the first round (lane bits BM..2BM-1) derives layer 0 from the
+// staged cnt, the last round (the highest lane bits) stores to HBM with 32
+// consecutive lanes per warp.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src,
+                                          uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];\n" ::"r"(saddr(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(saddr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ int pad16(int p) { return p + (p >> 4); }
+
+// first-group rounds: BM-bit blocks; round order BM.., 0.., 2BM.., 3BM..
+template <int KK, int BM, int I>
+struct FirstRound {
+  static constexpr int A = I == 0 ? BM : I == 1 ? 0 : I * BM;
+  static constexpr int B = (KK - A) < BM ? (KK - A) : BM;
+  static constexpr int N = (KK + BM - 1) / BM;
+};
+
+template <int KK, int R1, int OUT, int I>
+__device__ __forceinline__ void first_round(uint32_t *work, int WS,
+                                            const uint32_t *cnt32,
+                                            const TmaArgs &a, long long x0,
+                                            uint32_t plo, uint32_t pspan) {
+  constexpr int BM = 4;
+  using FR = FirstRound<KK, BM, I>;
+  constexpr int A = FR::A, B = FR::B;
+  constexpr int QB = 1 << B, QA = 1 << A;
+  constexpr bool FIRST = I == 0, LAST = I == FR::N - 1;
+  constexpr int NB = (1 << KK) / QB;
+  for (int blk = threadIdx.x; blk < NB; blk += blockDim.x) {
+    const int pb = (blk & (QA - 1)) | ((blk >> A) << (A + B));
+    uint32_t v[R1][QB];
+    if (FIRST) {
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        const uint32_t c = cnt32[pb + e * QA];
+        const uint32_t lo = ((c & 0xFFFFu) - plo) <= pspan;
+        const uint32_t hi = ((c >> 16) - plo) <= pspan;
+        v[0][e] = lo | (hi << 16);
+#pragma unroll
+        for (int d = 1; d < R1; d++) v[d][e] = 0;
+        // axis 0, inside the pair: A_1 gains the other half of A_0
+        if (R1 > 1) v[1][e] = __funnelshift_l(v[0][e], v[0][e], 16);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < R1; d++)
+#pragma unroll
+        for (int e = 0; e < QB; e++)
+          v[d][e] = work[d * WS + pad16(pb + e * QA)];
+    }
+    Axes<2, R1, B, 0>::run(v);
+    if (!LAST) {
+#pragma unroll
+      for (int d = 0; d < R1; d++)
+#pragma unroll
+        for (int e = 0; e < QB; e++)
+          work[d * WS + pad16(pb + e * QA)] = v[d][e];
+      continue;
+    }
+    const long long xb = x0 + 2LL * pb;
+    if (OUT == 0) {
+#pragma unroll
+      for (int d = 0; d < R1; d++) {
+        if (d >= a.lout) break;
+        uint16_t *q = a.layers16 + d * a.plane + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++)
+          __stcs(reinterpret_cast<unsigned *>(q + 2 * e * QA), v[d][e]);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int d = 0; d < R1; d++) s += v[d][e];
+        if (OUT == 1)
+          __stcs(reinterpret_cast<int2 *>(a.map + xb + 2 * e * QA),
+                 make_int2((int)(s & 0xFFFFu), (int)(s >> 16)));
+        else
+          *reinterpret_cast<unsigned *>(a.cnt + xb + 2 * e * QA) = s;
+      }
+    }
+  }
+}
+
+template <int KK, int R1, int OUT, int I, int N>
+struct FirstRounds {
+  static __device__ __forceinline__ void run(uint32_t *work, int WS,
+                                             const uint32_t *cnt32,
+                                             const TmaArgs &a, long long x0,
+                                             uint32_t plo, uint32_t pspan,
+                                             uint64_t *refill_bar,
+                                             const void *refill_src,
+                                             void *refill_dst) {
+    first_round<KK, R1, OUT, I>(work, WS, cnt32, a, x0, plo, pspan);
+    __syncthreads();
+    if (I == 0 && threadIdx.x == 0 && refill_src) {
+      // the staged cnt has been read: refill its stage now
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      const uint32_t bytes = (uint32_t)((2LL << KK) * 2);
+      mbar_expect(refill_bar, bytes);
+      bulk_load(refill_dst, refill_src, bytes, refill_bar);
+    }
+    FirstRounds<KK, R1, OUT, I + 1, N>::run(work, WS, cnt32, a, x0, plo,
+                                            pspan, refill_bar, refill_src,
+                                            refill_dst);
+  }
+};
+template <int KK, int R1, int OUT, int N>
+struct FirstRounds<KK, R1, OUT, N, N> {
+  static __device__ __forceinline__ void run(uint32_t *, int,
+                                             const uint32_t *,
+                                             const TmaArgs &, long long,
+                                             uint32_t, uint32_t, uint64_t *,
+                                             const void *, void *) {}
+};
+
+template <int KK, int R1, int OUT>
+__global__ void __launch_bounds__(512)
+tma_first(const TmaArgs a) {
+  extern __shared__ __align__(128) uint8_t dyn[];
+  constexpr int TW = 2 << KK;                 // words per tile
+  constexpr int CW = TW / 2;                  // cnt stage, 32-bit words
+  constexpr int WS = ((1 << KK) + (1 << KK) / 16 + 31) / 32 * 32;
+  constexpr int NR = FirstRound<KK, 4, 0>::N;
+  const int S = a.stages;
+  uint8_t *base = dyn + ((1024u - (saddr(dyn) & 1023u)) & 1023u);
+  uint32_t *cstage = reinterpret_cast<uint32_t *>(base);
+  uint32_t *work = cstage + (size_t)S * CW;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(work + (size_t)R1 * WS);
+  volatile int *stop = reinterpret_cast<volatile int *>(bar + kTmaMaxStages);
+  const uint32_t bytes = (uint32_t)TW * 2;
+  // predicate as a range: plo <= cnt <= plo + pspan
+  const uint32_t plo = a.pmode == kPredDef ? 0u
+                       : a.pmode == kPredCrit ? 1u : (uint32_t)a.ptarget;
+  const uint32_t phi = a.pmode == kPredDef ? (uint32_t)(a.mu - 1)
+                       : a.pmode == kPredCrit ? (uint32_t)a.mu
+                       : (uint32_t)a.ptarget;
+  const uint32_t pspan = phi - plo;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) mbar_init(&bar[s]);
+    *stop = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const long long grid = gridDim.x;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) {
+      const long long t = blockIdx.x + s * grid;
+      if (t < a.ntiles) {
+        mbar_expect(&bar[s], bytes);
+        bulk_load(cstage + (size_t)s * CW, a.cnt_in + t * TW, bytes, &bar[s]);
+      }
+    }
+  }
+  long long it = 0;
+  long long t = blockIdx.x;
+  for (; t < a.ntiles; it++, t += grid) {
+    const int s = (int)(it % S);
+    const uint32_t parity = (uint32_t)((it / S) & 1);
+    if (!mbar_wait(&bar[s], parity, kTmaWaitNs)) *stop = 1;
+    __syncthreads();
+    if (*stop) break;
+    const long long nt = t + S * grid;
+    FirstRounds<KK, R1, OUT, 0, NR>::run(
+        work, WS, cstage + (size_t)s * CW, a, t * TW, plo, pspan, &bar[s],
+        nt < a.ntiles ? (const void *)(a.cnt_in + nt * TW) : nullptr,
+        cstage + (size_t)s * CW);
+  }
+  if (t < a.ntiles && threadIdx.x == 0) {
+    *a.fault = 1;
+    __threadfence_system();
+    for (long long k = it; k < it + S; k++) {
+      const long long tk = blockIdx.x + k * grid;
+      if (tk >= a.ntiles) break;
+      mbar_wait(&bar[k % S], (uint32_t)((k / S) & 1), kTmaDrainNs);
+    }
+  }
+}
+
 // ------------------------------------------------------------ dispatch
 typedef void (*TmaFn)(const CUtensorMap, const TmaArgs);
 
@@ -320,6 +512,19 @@ const TmaEntry kTma[] = {
     TE(3, 3, 4, 32), TE(3, 4, 4, 32),
 };
 #undef TE
+
+typedef void (*FirstFn)(const TmaArgs);
+struct FirstEntry { int kk, r1, out; FirstFn fn; };
+#define FE(KK, R1) {KK, R1, 0, tma_first<KK, R1, 0>}, \
+                   {KK, R1, 1, tma_first<KK, R1, 1>}
+const FirstEntry kFirst[] = {FE(9, 4), FE(10, 4), FE(11, 4), FE(12, 4)};
+#undef FE
+
+const FirstEntry *find_first(int kk, int r1, int out) {
+  for (const auto &e : kFirst)
+    if (e.kk == kk && e.r1 == r1 && e.out == out) return &e;
+  return nullptr;
+}
 
 const TmaEntry *find_tma(int q, int k, int r1, int lanes, int out) {
   for (const auto &e : kTma)
@@ -402,6 +607,17 @@ bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
 }
 
 // The same group as a streamed launch: W = 2 x lanes inner words a tile.
+GroupPlan tma_first_variant(const GroupPlan &p, int stages, int threads) {
+  GroupPlan v = p;
+  v.a.tma = 2;
+  v.a.stages = stages;
+  v.a.pipe = 0;
+  v.threads = threads;
+  v.smem = tma_first_smem_bytes(v.a.k, v.a.R + 1, stages);
+  v.grid = 0;
+  return v;
+}
+
 GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages,
                       int threads) {
   GroupPlan v = p;
@@ -419,6 +635,29 @@ GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages,
   return v;
 }
 
+size_t tma_first_smem_bytes(int kk, int r1, int stages) {
+  const long long lanes = 1LL << kk;
+  const long long ws = (lanes + lanes / 16 + 31) / 32 * 32;
+  return (size_t)stages * (4LL << kk) + (size_t)r1 * ws * 4 + 1024 +
+         kTmaMaxStages * 8 + 16;
+}
+
+// The first group of a binary Hamming cell read from cnt, its axis 0 inside
+// the pair, one contiguous tile of 2^(k+1) words (Bo = 1).
+bool tma_first_ok(const GroupArgs &a, int r1, int stages) {
+  if (stages < 2 || stages > kTmaMaxStages) return false;
+  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  if (out == 2 || !find_first(a.k, r1, out)) return false;
+  if (a.prob != kHamming || !a.pair_axis || !a.pack || a.src != kSrcCnt ||
+      a.W != 2 || a.inner != 2 || a.Bo != 1 || a.R + 1 != r1 ||
+      a.nchunk != 1)
+    return false;
+  if (out == 0 && !a.out16) return false;
+  if (a.plane % 8 || (reinterpret_cast<uintptr_t>(a.cnt) & 15) != 0)
+    return false;
+  return tma_first_smem_bytes(a.k, r1, stages) <= kTmaSmemMax;
+}
+
 int tma_fault_pending() {
   return g_fault_host && *(volatile int *)g_fault_host ? 1 : 0;
 }
@@ -428,6 +667,26 @@ void tma_fault_clear() {
 }
 
 namespace {
+
+const FirstEntry *first_of(const GroupPlan &p) {
+  const GroupArgs &a = p.a;
+  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  return find_first(a.k, a.R + 1, out);
+}
+
+int first_opt_in(const FirstEntry *e) {
+  static std::mutex mu;
+  static bool done[sizeof(kFirst) / sizeof(kFirst[0])];
+  std::lock_guard<std::mutex> g(mu);
+  const size_t idx = (size_t)(e - kFirst);
+  if (!done[idx]) {
+    CC_CK(cudaFuncSetAttribute((const void *)e->fn,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTmaSmemMax));
+    done[idx] = true;
+  }
+  return 0;
+}
 
 const TmaEntry *entry_of(const GroupPlan &p) {
   const GroupArgs &a = p.a;
@@ -453,24 +712,74 @@ int opt_in(const TmaEntry *e) {
 }  // namespace
 
 int tma_prepare(const GroupPlan &p) {
+  if (p.a.tma == 2) {
+    const FirstEntry *f = first_of(p);
+    return f ? first_opt_in(f) : -9;
+  }
   const TmaEntry *e = entry_of(p);
   if (!e) return -9;
   return opt_in(e);
 }
 
 int tma_blocks_per_sm(const GroupPlan &p) {
-  const TmaEntry *e = entry_of(p);
-  if (!e || opt_in(e)) return 0;
+  const void *fn = nullptr;
+  if (p.a.tma == 2) {
+    const FirstEntry *f = first_of(p);
+    if (!f || first_opt_in(f)) return 0;
+    fn = (const void *)f->fn;
+  } else {
+    const TmaEntry *e = entry_of(p);
+    if (!e || opt_in(e)) return 0;
+    fn = (const void *)e->fn;
+  }
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &n, (const void *)e->fn, p.threads, p.smem) != cudaSuccess) {
+          &n, fn, p.threads, p.smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return n;
 }
 
+int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
+  const GroupArgs &a = p.a;
+  const FirstEntry *f = first_of(p);
+  if (!f || a.stages < 2 || a.stages > kTmaMaxStages) return -9;
+  int *fault = nullptr;
+  if (fault_word(&fault)) return -9;
+  int rc = first_opt_in(f);
+  if (rc) return rc;
+  TmaArgs t{};
+  t.layers16 = a.layers16;
+  t.plane = a.plane;
+  t.map = a.map ? a.map : a.layers;
+  t.cnt = a.cnt;
+  t.cnt_in = a.cnt;
+  t.pmode = a.pmode;
+  t.ptarget = a.ptarget;
+  t.mu = a.mu;
+  t.inner = a.inner;
+  t.nchunk = 1;
+  t.ntiles = a.ntiles;
+  t.lin = 1;
+  t.lout = a.lout;
+  t.stages = a.stages;
+  t.fault = fault;
+  const size_t smem = tma_first_smem_bytes(a.k, a.R + 1, a.stages);
+  int grid = p.grid;
+  if (grid < 1) {
+    const int per_sm = tma_blocks_per_sm(p);
+    long long gr = (long long)sm_count() * (per_sm < 1 ? 1 : per_sm);
+    if (gr > a.ntiles) gr = a.ntiles;
+    grid = (int)(gr < 1 ? 1 : gr);
+  }
+  f->fn<<<grid, p.threads, smem, s>>>(t);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
 int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
+  if (p.a.tma == 2) return launch_tma_first(p, s);
   const GroupArgs &a = p.a;
   const int q = a.rq[0] ? a.rq[0] : a.qax[0];
   const int lanes = a.W / 2;
