@@ -98,6 +98,9 @@ struct TmaArgs {
   // first group (tma_first): the cnt source and its predicate
   const uint16_t *cnt_in;
   int pmode, ptarget, mu;
+  // first group of a recount (code_first): the sorted code, per-tile slices
+  const long long *code;
+  const long long *code_bounds;
 };
 
 struct GroupPlan {

@@ -245,7 +245,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
           v.grid = occupancy_grid(v);
           out.push_back(v);
         }
-  for (int stages : {2, 3})
+  for (int stages : {0, 2, 3})
     if (!tma_off && tma_first_ok(p.a, R1, stages))
       for (int th : {256, 512}) {
         GroupPlan v = tma_first_variant(p, stages, th);

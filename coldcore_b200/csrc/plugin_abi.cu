@@ -354,7 +354,7 @@ Plan build_group_plan(int src, int dst, Knobs kn) {
     for (auto &p : P.groups) {
       if (p.kernel < 0 || p.a.nrounds <= 0) continue;
       bool done = false;
-      for (int stages : {3, 2})
+      for (int stages : {3, 2, 0})
         if (!done && tma_first_ok(p.a, S.R1, stages)) {
           p = tma_first_variant(p, stages, 256);
           done = true;

@@ -331,7 +331,7 @@ struct FirstRound {
   static constexpr int N = (KK + BM - 1) / BM;
 };
 
-template <int KK, int R1, int OUT, int I>
+template <int KK, int R1, int OUT, int I, int SRC = 0>
 __device__ __forceinline__ void first_round(uint32_t *work, int WS,
                                             const uint32_t *cnt32,
                                             const TmaArgs &a, long long x0,
@@ -348,10 +348,14 @@ __device__ __forceinline__ void first_round(uint32_t *work, int WS,
     if (FIRST) {
 #pragma unroll
       for (int e = 0; e < QB; e++) {
-        const uint32_t c = cnt32[pb + e * QA];
-        const uint32_t lo = ((c & 0xFFFFu) - plo) <= pspan;
-        const uint32_t hi = ((c >> 16) - plo) <= pspan;
-        v[0][e] = lo | (hi << 16);
+        if (SRC == 0) {                       // the cnt predicate
+          const uint32_t c = cnt32[pb + e * QA];
+          const uint32_t lo = ((c & 0xFFFFu) - plo) <= pspan;
+          const uint32_t hi = ((c >> 16) - plo) <= pspan;
+          v[0][e] = lo | (hi << 16);
+        } else {                              // code counts, staged
+          v[0][e] = work[pad16(pb + e * QA)];
+        }
 #pragma unroll
         for (int d = 1; d < R1; d++) v[d][e] = 0;
         // axis 0, inside the pair: A_1 gains the other half of A_0
@@ -494,6 +498,48 @@ tma_first(const TmaArgs a) {
   }
 }
 
+// The same first group read from the sorted code (a recount): per tile, the
+// code slice [bounds[t], bounds[t+1]) is counted into layer 0 of the shared
+// buffer (16-bit halves of the packed lanes, which the occurrence bound
+// keeps below 2^16), then the rounds run as above.  No HBM reads but the
+// slice; every byte written once.
+template <int KK, int R1, int OUT, int I, int N>
+struct CodeRounds {
+  static __device__ __forceinline__ void run(uint32_t *work, int WS,
+                                             const TmaArgs &a, long long x0) {
+    first_round<KK, R1, OUT, I, 1>(work, WS, nullptr, a, x0, 0u, 0u);
+    __syncthreads();
+    CodeRounds<KK, R1, OUT, I + 1, N>::run(work, WS, a, x0);
+  }
+};
+template <int KK, int R1, int OUT, int N>
+struct CodeRounds<KK, R1, OUT, N, N> {
+  static __device__ __forceinline__ void run(uint32_t *, int,
+                                             const TmaArgs &, long long) {}
+};
+
+template <int KK, int R1, int OUT>
+__global__ void __launch_bounds__(512)
+code_first(const TmaArgs a) {
+  extern __shared__ __align__(128) uint8_t dyn[];
+  constexpr int TW = 2 << KK;
+  constexpr int WS = ((1 << KK) + (1 << KK) / 16 + 31) / 32 * 32;
+  constexpr int NR = FirstRound<KK, 4, 0>::N;
+  uint32_t *work = reinterpret_cast<uint32_t *>(dyn);
+  for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const long long x0 = t * TW;
+    for (int i = threadIdx.x; i < WS; i += blockDim.x) work[i] = 0;
+    __syncthreads();
+    const long long lo = a.code_bounds[t], hi = a.code_bounds[t + 1];
+    for (long long c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+      const int w = (int)(a.code[c] - x0);
+      atomicAdd(&work[pad16(w >> 1)], 1u << (16 * (w & 1)));
+    }
+    __syncthreads();
+    CodeRounds<KK, R1, OUT, 0, NR>::run(work, WS, a, x0);
+  }
+}
+
 // ------------------------------------------------------------ dispatch
 typedef void (*TmaFn)(const CUtensorMap, const TmaArgs);
 
@@ -506,23 +552,23 @@ struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; };
 const TmaEntry kTma[] = {
     TE(2, 5, 4, 16), TE(2, 6, 4, 16), TE(2, 7, 4, 16), TE(2, 8, 4, 16),
     TE(2, 5, 4, 32), TE(2, 6, 4, 32), TE(2, 7, 4, 32),
-    TE(3, 3, 5, 16), TE(3, 4, 5, 16), TE(3, 5, 5, 16),
-    TE(3, 3, 5, 32), TE(3, 4, 5, 32),
-    TE(3, 3, 4, 16), TE(3, 4, 4, 16), TE(3, 5, 4, 16),
-    TE(3, 3, 4, 32), TE(3, 4, 4, 32),
 };
 #undef TE
 
 typedef void (*FirstFn)(const TmaArgs);
-struct FirstEntry { int kk, r1, out; FirstFn fn; };
-#define FE(KK, R1) {KK, R1, 0, tma_first<KK, R1, 0>}, \
-                   {KK, R1, 1, tma_first<KK, R1, 1>}
-const FirstEntry kFirst[] = {FE(9, 4), FE(10, 4), FE(11, 4), FE(12, 4)};
+// src 0: the cnt predicate (tma_first), 1: the sorted code (code_first)
+struct FirstEntry { int src, kk, r1, out; FirstFn fn; };
+#define FE(KK, R1) {0, KK, R1, 0, tma_first<KK, R1, 0>},                 \
+                   {0, KK, R1, 1, tma_first<KK, R1, 1>},                 \
+                   {1, KK, R1, 0, code_first<KK, R1, 0>},                \
+                   {1, KK, R1, 2, code_first<KK, R1, 2>}
+const FirstEntry kFirst[] = {FE(9, 4), FE(10, 4), FE(11, 4), FE(12, 4),
+                             FE(13, 4)};
 #undef FE
 
-const FirstEntry *find_first(int kk, int r1, int out) {
+const FirstEntry *find_first(int src, int kk, int r1, int out) {
   for (const auto &e : kFirst)
-    if (e.kk == kk && e.r1 == r1 && e.out == out) return &e;
+    if (e.src == src && e.kk == kk && e.r1 == r1 && e.out == out) return &e;
   return nullptr;
 }
 
@@ -587,8 +633,8 @@ size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages) {
   return (size_t)stages * words * 4 + 1024 + kTmaMaxStages * 8 + 16;
 }
 
-// The groups the streamed form serves: binary or ternary Hamming groups
-// over 16-bit planes in packed pairs (16-bit planes, the map or cnt out),
+// The groups the streamed form serves: binary Hamming groups over 16-bit
+// planes in packed pairs (an even inner stride) (16-bit planes, the map or cnt out),
 // one tile per W inner words x the whole group, an instantiated (q, k,
 // layers, lanes) and its stages within 227 KB of shared memory.
 bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
@@ -638,19 +684,24 @@ GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages,
 size_t tma_first_smem_bytes(int kk, int r1, int stages) {
   const long long lanes = 1LL << kk;
   const long long ws = (lanes + lanes / 16 + 31) / 32 * 32;
+  if (stages == 0)                        // code source: the buffer alone
+    return (size_t)r1 * ws * 4;
   return (size_t)stages * (4LL << kk) + (size_t)r1 * ws * 4 + 1024 +
          kTmaMaxStages * 8 + 16;
 }
 
 // The first group of a binary Hamming cell read from cnt, its axis 0 inside
 // the pair, one contiguous tile of 2^(k+1) words (Bo = 1).
+// (stages 0: the code-sourced form of a recount's first group)
 bool tma_first_ok(const GroupArgs &a, int r1, int stages) {
-  if (stages < 2 || stages > kTmaMaxStages) return false;
+  const int src = a.src == kSrcCnt ? 0 : a.src == kSrcCode ? 1 : -1;
+  if (src < 0 || (src == 0 && (stages < 2 || stages > kTmaMaxStages)) ||
+      (src == 1 && stages != 0))
+    return false;
   const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
-  if (out == 2 || !find_first(a.k, r1, out)) return false;
-  if (a.prob != kHamming || !a.pair_axis || !a.pack || a.src != kSrcCnt ||
-      a.W != 2 || a.inner != 2 || a.Bo != 1 || a.R + 1 != r1 ||
-      a.nchunk != 1)
+  if (!find_first(src, a.k, r1, out)) return false;
+  if (a.prob != kHamming || !a.pair_axis || !a.pack || a.W != 2 ||
+      a.inner != 2 || a.Bo != 1 || a.R + 1 != r1 || a.nchunk != 1)
     return false;
   if (out == 0 && !a.out16) return false;
   if (a.plane % 8 || (reinterpret_cast<uintptr_t>(a.cnt) & 15) != 0)
@@ -671,7 +722,7 @@ namespace {
 const FirstEntry *first_of(const GroupPlan &p) {
   const GroupArgs &a = p.a;
   const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
-  return find_first(a.k, a.R + 1, out);
+  return find_first(a.src == kSrcCode ? 1 : 0, a.k, a.R + 1, out);
 }
 
 int first_opt_in(const FirstEntry *e) {
@@ -744,7 +795,10 @@ int tma_blocks_per_sm(const GroupPlan &p) {
 int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
   const GroupArgs &a = p.a;
   const FirstEntry *f = first_of(p);
-  if (!f || a.stages < 2 || a.stages > kTmaMaxStages) return -9;
+  const bool from_code = a.src == kSrcCode;
+  if (!f || (!from_code && (a.stages < 2 || a.stages > kTmaMaxStages)) ||
+      (from_code && (!a.code_bounds || !a.code)))
+    return -9;
   int *fault = nullptr;
   if (fault_word(&fault)) return -9;
   int rc = first_opt_in(f);
@@ -765,7 +819,10 @@ int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
   t.lout = a.lout;
   t.stages = a.stages;
   t.fault = fault;
-  const size_t smem = tma_first_smem_bytes(a.k, a.R + 1, a.stages);
+  t.code = a.code;
+  t.code_bounds = a.code_bounds;
+  const size_t smem = tma_first_smem_bytes(a.k, a.R + 1,
+                                           from_code ? 0 : a.stages);
   int grid = p.grid;
   if (grid < 1) {
     const int per_sm = tma_blocks_per_sm(p);

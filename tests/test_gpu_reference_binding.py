@@ -225,7 +225,8 @@ def test_legacy_inits(ref, init):
         cnt = np.zeros(q ** n, dtype=np.uint16)
         assert lib.dct_read_cnt(ctypes.c_longlong(0),
                                 ctypes.c_longlong(q ** n),
-                                cnt.ctypes.data_as(ctypes.c_void_p)) == 0
+                                cnt.ctypes.data_as(
+                                    ctypes.POINTER(ctypes.c_uint16))) == 0
         assert np.array_equal(cnt.astype(np.int64),
                               np.asarray(c.read_cnt(), dtype=np.int64))
     finally:

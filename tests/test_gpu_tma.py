@@ -1,7 +1,8 @@
 """The streamed form of the strided groups (tensor loads into shared-memory
 stages, transform_tma.cu) against the oracle: with CC_TMA=1 every group it
-serves takes it; recount, gain and loss fields must equal the oracle's,
-bit for bit, for binary and ternary Hamming cells, mu = 1 and 2."""
+serves takes it (the strided groups and the first group, read from cnt or
+from the code); recount, gain and loss fields must equal the oracle's, bit
+for bit, on binary Hamming cells of one to four groups, mu = 1 and 2."""
 import numpy as np
 import pytest
 
@@ -15,7 +16,7 @@ TMA = 32                                 # GpuBackend.plan_forms bit
 
 @pytest.mark.parametrize("axes,R,mu", [
     ([2] * 20, 3, 1), ([2] * 21, 3, 2), ([2] * 16, 3, 1),
-    ([3] * 13, 4, 1), ([3] * 12, 3, 1), ([3] * 11, 4, 2)])
+    ([2] * 12, 3, 1), ([2] * 23, 3, 1), ([2] * 10 + [3, 2], 3, 1)])
 def test_streamed_groups_match_the_oracle(monkeypatch, axes, R, mu):
     monkeypatch.setenv("CC_TMA", "1")
     monkeypatch.setenv("CC_TUNE", "0")
