@@ -247,7 +247,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
         }
   for (int stages : {0, 2, 3})
     if (!tma_off && tma_first_ok(p.a, R1, stages))
-      for (int th : {256, 512}) {
+      for (int th : {128, 256, 512}) {
         GroupPlan v = tma_first_variant(p, stages, th);
         v.grid = occupancy_grid(v);
         out.push_back(v);

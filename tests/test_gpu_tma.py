@@ -16,7 +16,7 @@ TMA = 32                                 # GpuBackend.plan_forms bit
 
 @pytest.mark.parametrize("axes,R,mu", [
     ([2] * 20, 3, 1), ([2] * 21, 3, 2), ([2] * 16, 3, 1),
-    ([2] * 12, 3, 1), ([2] * 23, 3, 1), ([2] * 10 + [3, 2], 3, 1)])
+    ([2] * 12, 3, 1), ([2] * 23, 3, 1), ([2] * 13 + [3], 3, 1)])
 def test_streamed_groups_match_the_oracle(monkeypatch, axes, R, mu):
     monkeypatch.setenv("CC_TMA", "1")
     monkeypatch.setenv("CC_TUNE", "0")
