@@ -15,6 +15,8 @@
 // block owns one word (or a slice of its ball when the ball is large): the
 // word's digits, axis sizes and strides sit in shared memory, and each
 // thread resolves one pattern at a time with a few integer ops per slot.
+#include <cstdlib>
+
 #include "engine.h"
 
 namespace cc {
@@ -417,6 +419,110 @@ int launch_greedy_step(const WalkArgs &w, int32_t *map, long long N,
 }
 
 // blocks per word so that single-word walks still fill the GPU
+// ------------------------------------------------------------ tiled gather
+// Many candidates over a large ball: the per-word kernel above re-reads the
+// whole support table for every candidate (|B| x slots x 4 bytes, 546 KB a
+// candidate at ternary n=16, R=4), so a call with 10^5 candidates streams
+// tens of GB of table through L2.  Here a block takes a tile of kTilePat
+// patterns and a group of kTileCand candidates: the tile's slots are decoded
+// once into contribution indices, each candidate's per-(position, shift)
+// index offsets sit in shared memory (32-bit: cells below 2^31 words), and
+// every thread walks its patterns for every candidate of the group; a
+// warp's counts reduce in one instruction and one shared atomic.  The table
+// is then read once per candidate group instead of once per candidate.
+constexpr int kTilePat = 1024;          // patterns per block (4 per thread)
+constexpr int kTileCand = 32;           // candidates per block
+constexpr int kTileMaxOff = 256;        // sum over axes of (a_j - 1)
+
+template <int MAXS>
+__global__ void __launch_bounds__(256)
+k_gather_tiled(const WalkArgs a, const long long *words, int nb, int mode,
+               int target, int32_t *out, int noff) {
+  __shared__ int32_t off[kTileCand * kTileMaxOff];
+  __shared__ int32_t base[kMaxAxes];
+  __shared__ int32_t cand[kTileCand];
+  __shared__ int32_t acc[kTileCand];
+  const int c0 = blockIdx.y * kTileCand;
+  const int nc = min(kTileCand, nb - c0);
+  if (threadIdx.x == 0) {
+    int b = 0;
+    for (int j = 0; j < a.g.n; j++) { base[j] = b; b += a.g.ax[j] - 1; }
+  }
+  if (threadIdx.x < kTileCand) {
+    cand[threadIdx.x] = threadIdx.x < nc ? (int32_t)words[c0 + threadIdx.x]
+                                         : 0;
+    acc[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  // index offsets of every (position, shift) around each candidate
+  for (int i = threadIdx.x; i < nc * noff; i += blockDim.x) {
+    const int c = i / noff, e = i % noff;
+    int j = 0;
+    while (j + 1 < a.g.n && base[j + 1] <= e) j++;
+    const int q = a.g.ax[j], dl = e - base[j] + 1;
+    const int pw = (int)a.g.pw[j];
+    const int dg = (cand[c] / pw) % q;
+    const int nd = dg + dl >= q ? dg + dl - q : dg + dl;
+    off[c * kTileMaxOff + e] = (nd - dg) * pw;
+  }
+  // this thread's patterns, decoded to offset indices
+  constexpr int P = kTilePat / 256;
+  int16_t ek[P][MAXS];
+  bool live[P];
+  const long long t0 = (long long)blockIdx.x * kTilePat + threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < P; j++) {
+    const long long t = t0 + j * 256;
+    live[j] = t < a.len;
+#pragma unroll
+    for (int k = 0; k < MAXS; k++) {
+      int code = 0;
+      if (live[j] && k < a.slots) code = a.tbl[(long long)k * a.len + t];
+      ek[j][k] = code ? (int16_t)(base[code >> 24] + (code & 0xFFFFFF) - 1)
+                      : (int16_t)-1;
+    }
+  }
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31;
+  for (int c = 0; c < nc; c++) {
+    const int32_t *oc = off + c * kTileMaxOff;
+    const int32_t w = cand[c];
+    int hits = 0;
+#pragma unroll
+    for (int j = 0; j < P; j++) {
+      if (!live[j]) continue;
+      int32_t x = w;
+#pragma unroll
+      for (int k = 0; k < MAXS; k++) {
+        if (ek[j][k] < 0) break;
+        x += oc[ek[j][k]];
+      }
+      hits += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
+    }
+    hits = __reduce_add_sync(0xffffffffu, hits);
+    if (lane == 0 && hits) atomicAdd(&acc[c], hits);
+  }
+  __syncthreads();
+  if (threadIdx.x < nc && acc[threadIdx.x])
+    atomicAdd(&out[c0 + threadIdx.x], acc[threadIdx.x]);
+}
+
+// the tiled gather applies: Hamming / Lee / torus cells below 2^31 words,
+// offsets table within bounds, at most 8 slots, enough candidates to share
+// a table tile (CC_GATHER_TILED=0 turns it off, =1 forces it on)
+bool gather_tiled_ok(const WalkArgs &w, int nb, int *noff) {
+  if (w.g.prob == kGrid || w.g.space >= (1LL << 31) || w.slots > 8 ||
+      w.len >= (1LL << 31))
+    return false;
+  int n = 0;
+  for (int j = 0; j < w.g.n; j++) n += w.g.ax[j] - 1;
+  if (n > kTileMaxOff || n >= 32768) return false;
+  *noff = n;
+  const char *e = getenv("CC_GATHER_TILED");
+  if (e) return atoi(e) != 0;
+  return nb >= 16 && w.len >= 2048;
+}
+
 int pick_split(long long len, int nb) {
   long long cover = (len + 255) / 256;
   long long split = (long long)sm_count() * 64 / (nb > 0 ? nb : 1);
@@ -449,6 +555,20 @@ int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
                   int mode, int target, int32_t *out, bool zeroed,
                   cudaStream_t s) {
   if (nb <= 0) return 0;
+  int noff = 0;
+  if (gather_tiled_ok(w, nb, &noff)) {
+    if (!zeroed) CC_CK(cudaMemsetAsync(out, 0, (size_t)nb * 4, s));
+    const dim3 tg((unsigned)((w.len + kTilePat - 1) / kTilePat),
+                  (unsigned)((nb + kTileCand - 1) / kTileCand));
+    if (w.slots <= 4)
+      k_gather_tiled<4><<<tg, 256, 0, s>>>(w, dwords, nb, mode, target, out,
+                                           noff);
+    else
+      k_gather_tiled<8><<<tg, 256, 0, s>>>(w, dwords, nb, mode, target, out,
+                                           noff);
+    CC_CK(cudaGetLastError());
+    return 0;
+  }
   const int split = pick_split(w.len, nb);
   if (split > 1 && !zeroed)
     CC_CK(cudaMemsetAsync(out, 0, (size_t)nb * 4, s));
