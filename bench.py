@@ -289,11 +289,13 @@ def measure_cell(cell, args, dist, timed=True):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed")     # ncu --nvtx-include timed/
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         dist.barrier()
         ms = dist.max(e0.elapsed_time(e1)) / args.steps
         res["clocks"] = clocks.stop() if timed else None

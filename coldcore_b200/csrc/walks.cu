@@ -484,23 +484,33 @@ k_gather_tiled(const WalkArgs a, const long long *words, int nb, int mode,
   }
   __syncthreads();
   const unsigned lane = threadIdx.x & 31;
-  for (int c = 0; c < nc; c++) {
-    const int32_t *oc = off + c * kTileMaxOff;
-    const int32_t w = cand[c];
-    int hits = 0;
+  // eight candidates at a time, their counts in registers: 8 x P loads in
+  // flight per thread before the first reduction waits on any of them
+  constexpr int U = 8;
+  for (int cb = 0; cb < nc; cb += U) {
+    int hits[U];
 #pragma unroll
-    for (int j = 0; j < P; j++) {
-      if (!live[j]) continue;
-      int32_t x = w;
+    for (int u = 0; u < U; u++) {
+      hits[u] = 0;
+      const int c = cb + u;
+      if (c >= nc) continue;
+      const int32_t *oc = off + c * kTileMaxOff;
+      const int32_t w = cand[c];
 #pragma unroll
-      for (int k = 0; k < MAXS; k++) {
-        if (ek[j][k] < 0) break;
-        x += oc[ek[j][k]];
+      for (int j = 0; j < P; j++) {
+        if (!live[j]) continue;
+        int32_t x = w;
+#pragma unroll
+        for (int k = 0; k < MAXS; k++)
+          if (ek[j][k] >= 0) x += oc[ek[j][k]];
+        hits[u] += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
       }
-      hits += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
     }
-    hits = __reduce_add_sync(0xffffffffu, hits);
-    if (lane == 0 && hits) atomicAdd(&acc[c], hits);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int h = __reduce_add_sync(0xffffffffu, hits[u]);
+      if (lane == 0 && h) atomicAdd(&acc[cb + u], h);
+    }
   }
   __syncthreads();
   if (threadIdx.x < nc && acc[threadIdx.x])
