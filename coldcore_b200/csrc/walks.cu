@@ -424,97 +424,97 @@ int launch_greedy_step(const WalkArgs &w, int32_t *map, long long N,
 // whole support table for every candidate (|B| x slots x 4 bytes, 546 KB a
 // candidate at ternary n=16, R=4), so a call with 10^5 candidates streams
 // tens of GB of table through L2.  Here a block takes a tile of kTilePat
-// patterns and a group of kTileCand candidates: the tile's slots are decoded
-// once into contribution indices, each candidate's per-(position, shift)
-// index offsets sit in shared memory (32-bit: cells below 2^31 words), and
-// every thread walks its patterns for every candidate of the group; a
-// warp's counts reduce in one instruction and one shared atomic.  The table
-// is then read once per candidate group instead of once per candidate.
-constexpr int kTilePat = 1024;          // patterns per block (4 per thread)
+// patterns and a group of kTileCand candidates:
+//   * the tile is decoded once into 16-bit offset indices, four to a 64-bit
+//     shared word (a missing slot points at a zero entry, so every pattern
+//     takes the same adds, branch-free);
+//   * each candidate's index offsets per (position, shift) sit in shared
+//     memory (32-bit: cells below 2^31 words);
+//   * each warp walks the whole tile for one candidate at a time, 32
+//     consecutive patterns a step and eight steps in flight, so one
+//     candidate's loads stay close together in time and in address (the
+//     table is sorted by offset) and reuse L1 like a per-word sweep.
+// The table is read once per candidate group instead of once per candidate.
+constexpr int kTilePat = 512;           // patterns per block
 constexpr int kTileCand = 32;           // candidates per block
-constexpr int kTileMaxOff = 256;        // sum over axes of (a_j - 1)
+constexpr int kTileMaxOff = 128;        // offset entries per candidate
 
 template <int MAXS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_gather_tiled(const WalkArgs a, const long long *words, int nb, int mode,
                int target, int32_t *out, int noff) {
+  constexpr int NQ = MAXS / 4;            // 64-bit words of indices a pattern
   __shared__ int32_t off[kTileCand * kTileMaxOff];
+  __shared__ unsigned long long idx[kTilePat * NQ];
   __shared__ int32_t base[kMaxAxes];
   __shared__ int32_t cand[kTileCand];
-  __shared__ int32_t acc[kTileCand];
   const int c0 = blockIdx.y * kTileCand;
   const int nc = min(kTileCand, nb - c0);
+  const long long t0 = (long long)blockIdx.x * kTilePat;
+  const int np = (int)min((long long)kTilePat, a.len - t0);
   if (threadIdx.x == 0) {
     int b = 0;
     for (int j = 0; j < a.g.n; j++) { base[j] = b; b += a.g.ax[j] - 1; }
   }
-  if (threadIdx.x < kTileCand) {
+  if (threadIdx.x < kTileCand)
     cand[threadIdx.x] = threadIdx.x < nc ? (int32_t)words[c0 + threadIdx.x]
                                          : 0;
-    acc[threadIdx.x] = 0;
-  }
   __syncthreads();
-  // index offsets of every (position, shift) around each candidate
-  for (int i = threadIdx.x; i < nc * noff; i += blockDim.x) {
-    const int c = i / noff, e = i % noff;
-    int j = 0;
-    while (j + 1 < a.g.n && base[j + 1] <= e) j++;
-    const int q = a.g.ax[j], dl = e - base[j] + 1;
-    const int pw = (int)a.g.pw[j];
-    const int dg = (cand[c] / pw) % q;
-    const int nd = dg + dl >= q ? dg + dl - q : dg + dl;
-    off[c * kTileMaxOff + e] = (nd - dg) * pw;
-  }
-  // this thread's patterns, decoded to offset indices
-  constexpr int P = kTilePat / 256;
-  int16_t ek[P][MAXS];
-  bool live[P];
-  const long long t0 = (long long)blockIdx.x * kTilePat + threadIdx.x;
-#pragma unroll
-  for (int j = 0; j < P; j++) {
-    const long long t = t0 + j * 256;
-    live[j] = t < a.len;
-#pragma unroll
-    for (int k = 0; k < MAXS; k++) {
-      int code = 0;
-      if (live[j] && k < a.slots) code = a.tbl[(long long)k * a.len + t];
-      ek[j][k] = code ? (int16_t)(base[code >> 24] + (code & 0xFFFFFF) - 1)
-                      : (int16_t)-1;
+  // index offsets of every (position, shift) around each candidate; entry
+  // noff is the zero a missing slot adds
+  for (int i = threadIdx.x; i < nc * (noff + 1); i += blockDim.x) {
+    const int c = i / (noff + 1), e = i % (noff + 1);
+    int v = 0;
+    if (e < noff) {
+      int j = 0;
+      while (j + 1 < a.g.n && base[j + 1] <= e) j++;
+      const int q = a.g.ax[j], dl = e - base[j] + 1;
+      const int pw = (int)a.g.pw[j];
+      const int dg = (cand[c] / pw) % q;
+      const int nd = dg + dl >= q ? dg + dl - q : dg + dl;
+      v = (nd - dg) * pw;
     }
+    off[c * kTileMaxOff + e] = v;
   }
-  __syncthreads();
-  const unsigned lane = threadIdx.x & 31;
-  // eight candidates at a time, their counts in registers: 8 x P loads in
-  // flight per thread before the first reduction waits on any of them
-  constexpr int U = 8;
-  for (int cb = 0; cb < nc; cb += U) {
-    int hits[U];
+  // the tile's patterns as offset indices
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      hits[u] = 0;
-      const int c = cb + u;
-      if (c >= nc) continue;
-      const int32_t *oc = off + c * kTileMaxOff;
-      const int32_t w = cand[c];
+    for (int h = 0; h < NQ; h++) {
+      unsigned long long wv = 0;
 #pragma unroll
-      for (int j = 0; j < P; j++) {
-        if (!live[j]) continue;
-        int32_t x = w;
-#pragma unroll
-        for (int k = 0; k < MAXS; k++)
-          if (ek[j][k] >= 0) x += oc[ek[j][k]];
-        hits[u] += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
+      for (int k = 0; k < 4; k++) {
+        const int s = 4 * h + k;
+        int code = 0;
+        if (s < a.slots) code = a.tbl[(long long)s * a.len + t0 + p];
+        const unsigned e = code ? (unsigned)(base[code >> 24] +
+                                             (code & 0xFFFFFF) - 1)
+                                : (unsigned)noff;
+        wv |= (unsigned long long)e << (16 * k);
       }
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int h = __reduce_add_sync(0xffffffffu, hits[u]);
-      if (lane == 0 && h) atomicAdd(&acc[cb + u], h);
+      idx[p * NQ + h] = wv;
     }
   }
   __syncthreads();
-  if (threadIdx.x < nc && acc[threadIdx.x])
-    atomicAdd(&out[c0 + threadIdx.x], acc[threadIdx.x]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  for (int c = warp; c < nc; c += nwarps) {
+    const int32_t *oc = off + c * kTileMaxOff;
+    const int32_t w = cand[c];
+    int hits = 0;
+#pragma unroll 8
+    for (int p = lane; p < np; p += 32) {
+      int32_t x = w;
+#pragma unroll
+      for (int h = 0; h < NQ; h++) {
+        const unsigned long long wv = idx[p * NQ + h];
+        x += oc[wv & 0xFFFF] + oc[(wv >> 16) & 0xFFFF] +
+             oc[(wv >> 32) & 0xFFFF] + oc[wv >> 48];
+      }
+      hits += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
+    }
+    hits = __reduce_add_sync(0xffffffffu, hits);
+    if (lane == 0 && hits) atomicAdd(&out[c0 + c], hits);
+  }
 }
 
 // the tiled gather applies: Hamming / Lee / torus cells below 2^31 words,
@@ -526,8 +526,9 @@ bool gather_tiled_ok(const WalkArgs &w, int nb, int *noff) {
     return false;
   int n = 0;
   for (int j = 0; j < w.g.n; j++) n += w.g.ax[j] - 1;
-  if (n > kTileMaxOff || n >= 32768) return false;
+  if (n >= kTileMaxOff) return false;          // entry n is the zero
   *noff = n;
+  if ((long long)nb > 65535LL * kTileCand) return false;   // grid y
   const char *e = getenv("CC_GATHER_TILED");
   if (e) return atoi(e) != 0;
   return nb >= 16 && w.len >= 2048;
