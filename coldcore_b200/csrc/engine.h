@@ -211,9 +211,12 @@ struct WordsParam { long long w[kParamWords]; };
 int launch_update(const WalkArgs &w, const long long *dwords,
                   const WordsParam *pw, int nb, int delta,
                   unsigned long long *trans, cudaStream_t s);
+// bits: (|X|+7)/8 bytes of scratch for the predicate bit plane of a large
+// call (gather_bits_pay), or nullptr
 int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
                   int mode, int target, int32_t *out, bool zeroed,
-                  cudaStream_t s);
+                  cudaStream_t s, uint8_t *bits = nullptr);
+bool gather_bits_pay(const WalkArgs &w, int nb);
 int pick_split(long long len, int nb);
 // set side (setside.cu): list {x : pred(cnt[x])} as packed digit words, then
 // count, per candidate, the listed words within distance R

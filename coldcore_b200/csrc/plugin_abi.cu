@@ -78,6 +78,8 @@ struct State {
   long long *h_words = nullptr, *d_words = nullptr;
   int32_t *h_out = nullptr, *d_out = nullptr;
   long long *h_scalar = nullptr, *d_scalar = nullptr;
+  // one bit per word, the predicate of a large gather call (walks.cu)
+  uint8_t *d_bits = nullptr;
   int32_t *d_hist = nullptr;
   uint32_t *d_ext32 = nullptr;
   int64_t *d_ext64 = nullptr;
@@ -300,6 +302,7 @@ void free_all() {
   F(S.d_ext64); F(S.d_extv); F(S.zbuf); F(S.d_found);
   F(S.d_swap); F(S.d_list); FH(S.h_swap);
   F(S.d_greedy); F(S.d_placed); F(S.d_fresh); FH(S.h_placed);
+  F(S.d_bits);
   FH(S.h_layers);
   FH(S.h_words); FH(S.h_out); FH(S.h_scalar);
   S.~State();
@@ -939,8 +942,15 @@ int gather_launch(int mode, int target, int nb, const long long *dw,
                              g_stream);
   }
   S.stats[1]++;
-  return launch_gather(walk_args(), dw, nb, mode, target, dout, zeroed,
-                       g_stream);
+  const WalkArgs wa = walk_args();
+  uint8_t *bits = nullptr;
+  if (gather_bits_pay(wa, nb)) {
+    if (!S.d_bits)
+      CC_CK(cudaMalloc(&S.d_bits, (size_t)((S.g.space + 7) / 8 + 16)));
+    bits = S.d_bits;
+  }
+  return launch_gather(wa, dw, nb, mode, target, dout, zeroed, g_stream,
+                       bits);
 }
 
 int gather_impl(const long long *words, int nwords, int mode, int target,

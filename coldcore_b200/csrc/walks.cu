@@ -439,10 +439,39 @@ constexpr int kTilePat = 512;           // patterns per block
 constexpr int kTileCand = 32;           // candidates per block
 constexpr int kTileMaxOff = 128;        // offset entries per candidate
 
-template <int MAXS>
+// The predicate of one gather call as a bit plane: bit x of bits is
+// pred(cnt[x]).  Eight counters (one 16-byte load) per thread and byte.
+__global__ void __launch_bounds__(256)
+k_pred_bits(const uint16_t *cnt, long long n, int mode, int target, int mu,
+            uint8_t *bits) {
+  const long long nbytes = (n + 7) / 8;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       i < nbytes; i += stride) {
+    unsigned m = 0;
+    if (8 * i + 8 <= n) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(cnt) + i);
+      const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        m |= (unsigned)cnt_pred(mode, (int)(w[k] & 0xFFFFu), target, mu)
+             << (2 * k);
+        m |= (unsigned)cnt_pred(mode, (int)(w[k] >> 16), target, mu)
+             << (2 * k + 1);
+      }
+    } else {
+      for (long long x = 8 * i; x < n; x++)
+        m |= (unsigned)cnt_pred(mode, (int)cnt[x], target, mu)
+             << (int)(x - 8 * i);
+    }
+    bits[i] = (uint8_t)m;
+  }
+}
+
+template <int MAXS, bool BITS>
 __global__ void __launch_bounds__(256, 6)
 k_gather_tiled(const WalkArgs a, const long long *words, int nb, int mode,
-               int target, int32_t *out, int noff) {
+               int target, int32_t *out, int noff, const uint8_t *bits) {
   constexpr int NQ = MAXS / 4;            // 64-bit words of indices a pattern
   __shared__ int32_t off[kTileCand * kTileMaxOff];
   __shared__ unsigned long long idx[kTilePat * NQ];
@@ -510,7 +539,10 @@ k_gather_tiled(const WalkArgs a, const long long *words, int nb, int mode,
         x += oc[wv & 0xFFFF] + oc[(wv >> 16) & 0xFFFF] +
              oc[(wv >> 32) & 0xFFFF] + oc[wv >> 48];
       }
-      hits += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
+      if (BITS)
+        hits += (__ldg(bits + (x >> 3)) >> (x & 7)) & 1;
+      else
+        hits += cnt_pred(mode, (int)__ldg(a.cnt + x), target, a.g.mu);
     }
     hits = __reduce_add_sync(0xffffffffu, hits);
     if (lane == 0 && hits) atomicAdd(&out[c0 + c], hits);
@@ -532,6 +564,17 @@ bool gather_tiled_ok(const WalkArgs &w, int nb, int *noff) {
   const char *e = getenv("CC_GATHER_TILED");
   if (e) return atoi(e) != 0;
   return nb >= 16 && w.len >= 2048;
+}
+
+// A bit plane pays when the call reads many more ball words than the plane
+// costs to build (one pass over cnt): candidates x |B| >= 8 |X|.
+// CC_GATHER_BITS=0 turns it off, =1 forces it on.
+bool gather_bits_pay(const WalkArgs &w, int nb) {
+  int noff = 0;
+  if (!gather_tiled_ok(w, nb, &noff)) return false;
+  const char *e = getenv("CC_GATHER_BITS");
+  if (e) return atoi(e) != 0;
+  return (double)nb * (double)w.len >= 8.0 * (double)w.g.space;
 }
 
 int pick_split(long long len, int nb) {
@@ -564,19 +607,26 @@ int launch_update(const WalkArgs &w, const long long *dwords,
 
 int launch_gather(const WalkArgs &w, const long long *dwords, int nb,
                   int mode, int target, int32_t *out, bool zeroed,
-                  cudaStream_t s) {
+                  cudaStream_t s, uint8_t *bits) {
   if (nb <= 0) return 0;
   int noff = 0;
   if (gather_tiled_ok(w, nb, &noff)) {
     if (!zeroed) CC_CK(cudaMemsetAsync(out, 0, (size_t)nb * 4, s));
+    if (bits) {
+      const long long nbytes = (w.g.space + 7) / 8;
+      long long nbk = (nbytes + 255) / 256;
+      if (nbk > (long long)sm_count() * 32) nbk = (long long)sm_count() * 32;
+      k_pred_bits<<<(unsigned)nbk, 256, 0, s>>>(w.cnt, w.g.space, mode,
+                                                target, w.g.mu, bits);
+      CC_CK(cudaGetLastError());
+    }
     const dim3 tg((unsigned)((w.len + kTilePat - 1) / kTilePat),
                   (unsigned)((nb + kTileCand - 1) / kTileCand));
-    if (w.slots <= 4)
-      k_gather_tiled<4><<<tg, 256, 0, s>>>(w, dwords, nb, mode, target, out,
-                                           noff);
-    else
-      k_gather_tiled<8><<<tg, 256, 0, s>>>(w, dwords, nb, mode, target, out,
-                                           noff);
+#define TG(M, B) k_gather_tiled<M, B><<<tg, 256, 0, s>>>(                  \
+        w, dwords, nb, mode, target, out, noff, bits)
+    if (w.slots <= 4) { if (bits) TG(4, true); else TG(4, false); }
+    else { if (bits) TG(8, true); else TG(8, false); }
+#undef TG
     CC_CK(cudaGetLastError());
     return 0;
   }

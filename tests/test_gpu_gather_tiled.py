@@ -1,6 +1,7 @@
 """The tiled gather (a block walks a tile of the support table for a group
-of candidates) against the oracle and against the per-word walk, for
-Hamming, Lee, torus and mixed-radix cells, mu = 1 and 2, every role."""
+of candidates), with and without the predicate bit plane, against the
+oracle and against the per-word walk, for Hamming, Lee, torus and
+mixed-radix cells, mu = 1 and 2, every role."""
 import numpy as np
 import pytest
 
@@ -26,8 +27,12 @@ def test_tiled_gather_matches(monkeypatch, problem, axes, R, mu):
         for role in (0, 1, 2):
             want = o.ball_gather(cands, role)
             monkeypatch.setenv("CC_GATHER_TILED", "1")
+            monkeypatch.setenv("CC_GATHER_BITS", "1")
+            bits = b.ball_gather(cands, role)
+            monkeypatch.setenv("CC_GATHER_BITS", "0")
             tiled = b.ball_gather(cands, role)
             monkeypatch.setenv("CC_GATHER_TILED", "0")
             walk = b.ball_gather(cands, role)
+            assert np.array_equal(bits, want), role
             assert np.array_equal(tiled, want), role
             assert np.array_equal(walk, want), role
