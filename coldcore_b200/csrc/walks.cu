@@ -566,15 +566,15 @@ bool gather_tiled_ok(const WalkArgs &w, int nb, int *noff) {
   return nb >= 16 && w.len >= 2048;
 }
 
-// A bit plane pays when the call reads many more ball words than the plane
-// costs to build (one pass over cnt): candidates x |B| >= 8 |X|.
+// A bit plane pays when the call reads more ball words than the plane
+// costs to build (one pass over cnt): candidates x |B| >= |X|.
 // CC_GATHER_BITS=0 turns it off, =1 forces it on.
 bool gather_bits_pay(const WalkArgs &w, int nb) {
   int noff = 0;
   if (!gather_tiled_ok(w, nb, &noff)) return false;
   const char *e = getenv("CC_GATHER_BITS");
   if (e) return atoi(e) != 0;
-  return (double)nb * (double)w.len >= 8.0 * (double)w.g.space;
+  return (double)nb * (double)w.len >= (double)w.g.space;
 }
 
 int pick_split(long long len, int nb) {
