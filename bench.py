@@ -634,6 +634,13 @@ def run_b200(args, dist):
         leg("lns", lambda: measure_lns(args))
     if not args.no_batch:
         leg("batched_small", lambda: measure_batch_small(args))
+    if not args.no_batch and dist.world == 1:
+        # a campaign of searches on the batched engine against one
+        # singleton context per cell
+        def campaign():
+            from harness.campaign_bench import measure as camp_measure
+            return camp_measure()
+        leg("campaign", campaign)
     if not args.no_ops and dist.world == 1:
         # updates, per-candidate gathers and the Lee / king fields
         def ops():

@@ -39,6 +39,23 @@ def _bind(lib):
     lib.dct_batch_info.argtypes = [_LL, ctypes.POINTER(_LL), I]
     lib.dct_batch_free.restype = I
     lib.dct_batch_free.argtypes = [_LL]
+    I32P = ctypes.POINTER(ctypes.c_int32)
+    lib.dct_batch_set_code.restype = I
+    lib.dct_batch_set_code.argtypes = [_LL, I, ctypes.POINTER(_LL), I]
+    lib.dct_batch_set_table.restype = I
+    lib.dct_batch_set_table.argtypes = [_LL, I, I32P, I, _LL]
+    lib.dct_batch_update.restype = I
+    lib.dct_batch_update.argtypes = [_LL, I, ctypes.POINTER(_LL), I, I]
+    lib.dct_batch_gather.restype = I
+    lib.dct_batch_gather.argtypes = [_LL, I, ctypes.POINTER(_LL), I, I, I32P]
+    lib.dct_batch_extract.restype = _LL
+    lib.dct_batch_extract.argtypes = [_LL, I, I, ctypes.c_int32,
+                                      ctypes.POINTER(_LL), I32P, I]
+    lib.dct_batch_count.restype = _LL
+    lib.dct_batch_count.argtypes = [_LL, I, I, I]
+    lib.dct_batch_read_at.restype = I
+    lib.dct_batch_read_at.argtypes = [_LL, I, I, ctypes.POINTER(_LL), I,
+                                      I32P]
     lib._batch_bound = True
     return lib
 
@@ -101,6 +118,83 @@ class BatchEngine:
         if n < 0:
             _check("batch_scalars", n)
         return buf.reshape(-1, 3)
+
+    # ---------------- per cell, between runs
+    def set_code(self, cell, code):
+        """Replace a cell's code; the next run recounts from it."""
+        code = np.ascontiguousarray(np.atleast_1d(code), dtype=np.int64)
+        _check("batch_set_code", self._lib.dct_batch_set_code(
+            self.h, int(cell), code.ctypes.data_as(ctypes.POINTER(_LL)),
+            len(code)))
+
+    def set_table(self, cell, tbl):
+        """The cell's support table: (len, slots) int32 slots as
+        ``patterns.wide_table`` builds them."""
+        tbl = np.ascontiguousarray(tbl, dtype=np.int32)
+        _check("batch_set_table", self._lib.dct_batch_set_table(
+            self.h, int(cell),
+            tbl.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            tbl.shape[1], tbl.shape[0]))
+
+    def update(self, cell, words, delta):
+        words = np.ascontiguousarray(np.atleast_1d(words), dtype=np.int64)
+        for lo in range(0, len(words), 1 << 16):
+            part = np.ascontiguousarray(words[lo:lo + (1 << 16)])
+            _check("batch_update", self._lib.dct_batch_update(
+                self.h, int(cell), part.ctypes.data_as(ctypes.POINTER(_LL)),
+                len(part), int(delta)))
+
+    def gather(self, cell, words, role):
+        words = np.ascontiguousarray(np.atleast_1d(words), dtype=np.int64)
+        out = np.zeros(len(words), dtype=np.int32)
+        for lo in range(0, len(words), 1 << 16):
+            part = np.ascontiguousarray(words[lo:lo + (1 << 16)])
+            o = np.zeros(len(part), dtype=np.int32)
+            _check("batch_gather", self._lib.dct_batch_gather(
+                self.h, int(cell), part.ctypes.data_as(ctypes.POINTER(_LL)),
+                len(part), int(role),
+                o.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+            out[lo:lo + len(part)] = o
+        return out
+
+    def extract(self, cell, field, thr, cap):
+        idx = np.zeros(max(1, cap), dtype=np.int64)
+        val = np.zeros(max(1, cap), dtype=np.int32)
+        found = int(self._lib.dct_batch_extract(
+            self.h, int(cell), int(field), int(thr),
+            idx.ctypes.data_as(ctypes.POINTER(_LL)),
+            val.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(cap)))
+        if found < 0:
+            _check("batch_extract", found)
+        n = min(found, cap)
+        return idx[:n].copy(), val[:n].copy(), found
+
+    def count(self, cell, mode, target=0):
+        r = int(self._lib.dct_batch_count(self.h, int(cell), int(mode),
+                                          int(target)))
+        if r < 0:
+            _check("batch_count", r)
+        return r
+
+    def read_at(self, cell, field, idx):
+        idx = np.ascontiguousarray(np.atleast_1d(idx), dtype=np.int64)
+        out = np.zeros(len(idx), dtype=np.int32)
+        for lo in range(0, len(idx), 1 << 16):
+            part = np.ascontiguousarray(idx[lo:lo + (1 << 16)])
+            o = np.zeros(len(part), dtype=np.int32)
+            _check("batch_read_at", self._lib.dct_batch_read_at(
+                self.h, int(cell), int(field),
+                part.ctypes.data_as(ctypes.POINTER(_LL)), len(part),
+                o.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+            out[lo:lo + len(part)] = o
+        return out
+
+    def read_range(self, cell, field, off, length):
+        out = np.empty(length, dtype=np.uint16 if field == 0 else np.int32)
+        _check("batch_read", self._lib.dct_batch_read(
+            self.h, int(cell), int(field), int(off), int(length),
+            out.ctypes.data_as(ctypes.c_void_p)))
+        return out
 
     def info(self):
         buf = (_LL * 6)()

@@ -41,7 +41,38 @@ struct Cell {
   int first_pass = 0, npass = 0;     // global pass range (small cells)
   bool big = false;                  // own register-blocked launches
   std::vector<GroupPlan> fast[3];    // recount, gain, loss (big cells)
+  // codes may be replaced between launches (dct_batch_set_code): the
+  // device buffer holds code_cap words, its length lives on the device
+  long long code_cap = 0;
+  long long *dncode = nullptr;
+  // support table for the cell's walks (dct_batch_set_table), SoA slots
+  int32_t *dtbl = nullptr;
+  int slots = 0;
+  long long tlen = 0;
 };
+
+// one cell's code slices per first-group tile, computed on the device from
+// the code length on the device (so a replaced code needs no re-capture)
+struct BoundsJob {
+  const long long *code;
+  const long long *ncode;
+  long long tile_words, ntiles;
+  long long *bounds;
+};
+
+__global__ void k_batch_bounds(const BoundsJob *jobs) {
+  const BoundsJob j = jobs[blockIdx.x];
+  const long long n = *j.ncode;
+  for (long long t = threadIdx.x; t <= j.ntiles; t += blockDim.x) {
+    const long long x = t * j.tile_words;
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+      const long long md = (lo + hi) >> 1;
+      if (j.code[md] < x) lo = md + 1; else hi = md;
+    }
+    j.bounds[t] = lo;
+  }
+}
 
 // Cells of at least 2^16 words whose axes all have one size with a
 // register-blocked kernel run as their own launches (captured on forked
@@ -69,6 +100,15 @@ struct Batch {
   long long *d_scal = nullptr;       // per cell: deficit, gain max, loss max
   long long *d_bounds = nullptr;     // per-tile code slices of every cell
   long long bounds_cap = 0;
+  long long *d_ncode = nullptr;      // per cell: its code length
+  BoundsJob *d_jobs = nullptr;       // per cell: its bounds job
+  // staging of the per-cell calls (updates, gathers, extraction)
+  long long *d_words = nullptr;
+  int32_t *d_out = nullptr;
+  void *d_ext = nullptr;
+  int32_t *d_extv = nullptr;
+  long long ext_cap = 0;
+  long long *d_count = nullptr;
   size_t tile_budget = 48 * 1024;
   size_t smem = 0;
   int grid = 0;
@@ -176,6 +216,12 @@ void release(Batch *b) {
   auto F = [](void *p) { if (p) cudaFree(p); };
   F(b->arena); F(b->d_passes); F(b->d_dep); F(b->d_need); F(b->d_items);
   F(b->d_done); F(b->d_next); F(b->d_err); F(b->d_scal); F(b->d_bounds);
+  F(b->d_ncode); F(b->d_jobs); F(b->d_words); F(b->d_out); F(b->d_ext);
+  F(b->d_extv); F(b->d_count);
+  for (Cell &c : b->cells) { F(c.dtbl); c.dtbl = nullptr; }
+  b->d_ncode = nullptr; b->d_jobs = nullptr; b->d_words = nullptr;
+  b->d_out = nullptr; b->d_ext = nullptr; b->d_extv = nullptr;
+  b->d_count = nullptr; b->ext_cap = 0;
   b->d_bounds = nullptr;
   b->bounds_cap = 0;
   b->arena = nullptr; b->d_passes = nullptr; b->d_dep = nullptr;
@@ -271,6 +317,32 @@ int make_schedule(Batch *b) {
       for (int t = 0; t < 3; t++)
         for (auto &gp : c.fast[t]) gp.a.code_bounds = c.bounds;
   }
+  // the bounds job of every cell (its first group's tiles)
+  std::vector<BoundsJob> jobs;
+  for (const Cell &c : b->cells) {
+    BoundsJob j{};
+    j.code = c.dcode;
+    j.ncode = c.dncode;
+    j.bounds = c.bounds;
+    if (c.big) {
+      const GroupArgs &a0 = c.fast[0][0].a;
+      j.tile_words = (long long)a0.Bo * a0.mid * a0.inner;
+      j.ntiles = a0.ntiles;
+    } else {
+      const GroupArgs &a0 = b->passes[c.first_pass];
+      j.tile_words = (long long)a0.Bo * a0.mid;
+      j.ntiles = a0.ntiles;
+    }
+    jobs.push_back(j);
+  }
+  if (b->d_jobs) cudaFree(b->d_jobs);
+  b->d_jobs = nullptr;
+  CC_CK(cudaMalloc(&b->d_jobs, std::max<size_t>(1, jobs.size()) *
+                                   sizeof(BoundsJob)));
+  if (!jobs.empty())
+    CC_CK(cudaMemcpyAsync(b->d_jobs, jobs.data(),
+                          jobs.size() * sizeof(BoundsJob),
+                          cudaMemcpyHostToDevice, b->stream));
   std::vector<int4> items;
   for (auto &lv : by_level) {
     // largest passes first inside a level: long tails start early
@@ -316,15 +388,12 @@ int make_schedule(Batch *b) {
   return 0;
 }
 
-// one big cell's step on stream s: code bounds, recount, deficit, gain,
-// gain max, loss, loss max (register-blocked group kernels)
+// one big cell's step on stream s (its code bounds computed before):
+// recount, deficit, gain, gain max, loss, loss max (register-blocked group
+// kernels)
 int run_big_cell(Batch *b, size_t i, cudaStream_t s) {
   Cell &c = b->cells[i];
-  const GroupArgs &a0 = c.fast[0][0].a;
-  int rc = launch_code_bounds(c.dcode, (long long)c.code.size(),
-                              (long long)a0.Bo * a0.mid * a0.inner,
-                              a0.ntiles, c.bounds, s);
-  if (rc) return rc;
+  int rc = 0;
   for (int t = 0; t < 3; t++) {
     for (const auto &gp : c.fast[t])
       if ((rc = launch_group(gp, s))) return rc;
@@ -356,6 +425,10 @@ int capture_graph(Batch *b) {
      "memset done");
   ck(cudaMemsetAsync(b->d_scal, 0, b->cells.size() * 3 * 8, b->stream),
      "memset scalars");
+  // every cell's code slices, from the code lengths on the device
+  k_batch_bounds<<<(unsigned)b->cells.size(), 256, 0, b->stream>>>(
+      b->d_jobs);
+  ck(cudaGetLastError(), "bounds launch");
   // big cells fork onto side streams, small cells share one persistent
   // launch on the main stream, and everything joins before the end
   ck(cudaEventRecord(b->fork, b->stream), "fork record");
@@ -392,20 +465,27 @@ int run_persistent(Batch *b) {
   return err ? -7 : 0;
 }
 
-// One launch sequence per cell, cell after cell, synchronising after every
-// transform as the singleton dct_transform does — how a campaign of
-// single-cell contexts runs today; the baseline of the persistent launch.
-int run_per_cell(Batch *b) {
+// The same step as one launch per pass: every big cell's own launches on
+// the same four side streams as the graph, every small cell's passes as
+// one launch each of the same tile code on the main stream, no host wait
+// until the end.  Only the launch structure differs from the persistent
+// graph launch, which is what the comparison measures.
+int run_per_pass(Batch *b) {
   CC_CK(cudaMemsetAsync(b->d_scal, 0, b->cells.size() * 3 * 8, b->stream));
+  k_batch_bounds<<<(unsigned)b->cells.size(), 256, 0, b->stream>>>(
+      b->d_jobs);
+  CC_CK(cudaGetLastError());
+  CC_CK(cudaEventRecord(b->fork, b->stream));
+  for (int k = 0; k < kSideStreams; k++)
+    CC_CK(cudaStreamWaitEvent(b->side[k], b->fork, 0));
+  int nbig = 0;
   for (size_t i = 0; i < b->cells.size(); i++) {
     const Cell &c = b->cells[i];
     if (c.big) {
-      const int rc = run_big_cell(b, i, b->stream);
+      const int rc = run_big_cell(b, i, b->side[nbig++ % kSideStreams]);
       if (rc) return rc;
-      CC_CK(cudaStreamSynchronize(b->stream));
       continue;
     }
-    const int per_t = c.npass / 3;
     for (int p = c.first_pass; p < c.first_pass + c.npass; p++) {
       GroupPlan gp;
       gp.a = b->passes[p];
@@ -414,11 +494,13 @@ int run_per_cell(Batch *b) {
       gp.smem = group_smem_bytes(gp.a, c.R1);
       gp.grid = (int)std::min<long long>(gp.a.ntiles,
                                          (long long)sm_count() * 4);
-      int rc = launch_group(gp, b->stream);
+      const int rc = launch_group(gp, b->stream);
       if (rc) return rc;
-      if ((p - c.first_pass + 1) % per_t == 0)
-        CC_CK(cudaStreamSynchronize(b->stream));
     }
+  }
+  for (int k = 0; k < kSideStreams; k++) {
+    CC_CK(cudaEventRecord(b->join[k], b->side[k]));
+    CC_CK(cudaStreamWaitEvent(b->stream, b->join[k], 0));
   }
   CC_CK(cudaStreamSynchronize(b->stream));
   return 0;
@@ -496,7 +578,12 @@ int dct_batch_build(long long h, int tile_kb) {
   Batch *b = get(h);
   if (!b || b->built || b->cells.empty()) return -1;
   if (tile_kb > 0) b->tile_budget = (size_t)std::max(16, tile_kb) * 1024;
-  // arena: per cell layers, cnt, gain, loss, code
+  // arena: per cell layers, cnt, gain, loss, code (room for a code of
+  // four times its first size, at least 4096 words)
+  for (Cell &c : b->cells)
+    c.code_cap = std::max<long long>(
+        4 * (long long)c.code.size(),
+        std::min<long long>(c.g.space, 1LL << 18));
   size_t total = 0;
   std::vector<size_t> off(b->cells.size());
   for (size_t i = 0; i < b->cells.size(); i++) {
@@ -504,13 +591,20 @@ int dct_batch_build(long long h, int tile_kb) {
     off[i] = total;
     total += align256((size_t)c.plane * c.R1 * 4) + align256(c.plane * 2) +
              2 * align256((size_t)c.plane * 4) +
-             align256(std::max<size_t>(1, c.code.size()) * 8);
+             align256((size_t)b->cells[i].code_cap * 8);
   }
   CC_CK(cudaMalloc(&b->arena, total));
   b->arena_bytes = total;
   CC_CK(cudaMalloc(&b->d_next, 8));
   CC_CK(cudaMalloc(&b->d_err, 4));
   CC_CK(cudaMalloc(&b->d_scal, b->cells.size() * 3 * 8));
+  CC_CK(cudaMalloc(&b->d_ncode, b->cells.size() * 8));
+  {
+    std::vector<long long> nc;
+    for (const Cell &c : b->cells) nc.push_back((long long)c.code.size());
+    CC_CK(cudaMemcpy(b->d_ncode, nc.data(), nc.size() * 8,
+                     cudaMemcpyHostToDevice));
+  }
   for (size_t i = 0; i < b->cells.size(); i++) {
     Cell &c = b->cells[i];
     char *p = b->arena + off[i];
@@ -523,6 +617,7 @@ int dct_batch_build(long long h, int tile_kb) {
     c.loss = reinterpret_cast<int32_t *>(p);
     p += align256((size_t)c.plane * 4);
     c.dcode = reinterpret_cast<long long *>(p);
+    c.dncode = b->d_ncode + i;
     if (!c.code.empty())
       CC_CK(cudaMemcpyAsync(c.dcode, c.code.data(), c.code.size() * 8,
                             cudaMemcpyHostToDevice, b->stream));
@@ -532,16 +627,7 @@ int dct_batch_build(long long h, int tile_kb) {
   auto schedule = [&]() -> int {
     int rc = make_schedule(b);
     if (rc) return rc;
-    for (size_t i = 0; i < b->cells.size(); i++) {
-      const Cell &c = b->cells[i];
-      if (c.big) continue;             // bounds computed inside the graph
-      const GroupArgs &a0 = b->passes[c.first_pass];
-      rc = launch_code_bounds(c.dcode, (long long)c.code.size(),
-                              (long long)a0.Bo * a0.mid, a0.ntiles, c.bounds,
-                              b->stream);
-      if (rc) return rc;
-    }
-    return capture_graph(b);
+    return capture_graph(b);          // code bounds inside the graph
   };
   int rc;
   if (tile_kb > 0) return schedule();
@@ -573,7 +659,7 @@ int dct_batch_run(long long h, int mode) {
   Batch *b = get(h);
   if (!b || !b->built) return -1;
   if (mode == 0) return run_persistent(b);
-  if (mode == 1) return run_per_cell(b);
+  if (mode == 1) return run_per_pass(b);
   if (mode == 2) {
     // self-test of the bounded dependency wait: one launch in which the
     // first pass needs one more tile than it has, so its dependents time
@@ -632,6 +718,215 @@ int dct_batch_info(long long h, long long *out, int cap) {
   out[4] = b->grid;
   out[5] = (long long)(b->tuned_ms * 1000.0f);
   return 6;
+}
+
+// ------------------------------------------------------------ per cell
+// The calls a search on one cell of a batch makes between graph launches.
+// They run on the batch's stream and return after it drains.
+
+int dct_batch_set_code(long long h, int cell, const long long *code, int M) {
+  Batch *b = get(h);
+  if (!b || !b->built || cell < 0 || cell >= (int)b->cells.size() || M < 0 ||
+      (M && !code))
+    return -1;
+  Cell &c = b->cells[cell];
+  if (M > c.code_cap) return -3;                   // beyond the room kept
+  std::vector<long long> v(code, code + M);
+  for (long long w : v)
+    if (w < 0 || w >= c.g.space) return -1;
+  std::sort(v.begin(), v.end());
+  long long maxmult = 0, run = 0;
+  for (size_t i = 0; i < v.size(); i++) {
+    run = (i && v[i] == v[i - 1]) ? run + 1 : 1;
+    if (run > maxmult) maxmult = run;
+  }
+  if (std::min<long long>(M, maxmult * ball_cardinality(c.g)) > 65535)
+    return -1;                                     // the uint16 bound
+  c.code.swap(v);
+  const long long n = (long long)c.code.size();
+  if (n)
+    CC_CK(cudaMemcpyAsync(c.dcode, c.code.data(), (size_t)n * 8,
+                          cudaMemcpyHostToDevice, b->stream));
+  CC_CK(cudaMemcpyAsync(c.dncode, &n, 8, cudaMemcpyHostToDevice, b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+// the cell's support table: `len` patterns of `slots` int32 slots
+// (pos << 24) | shift, row-major as dct_init3w takes it; entry 0 the centre
+int dct_batch_set_table(long long h, int cell, const int32_t *tbl, int slots,
+                        long long len) {
+  Batch *b = get(h);
+  if (!b || !b->built || cell < 0 || cell >= (int)b->cells.size() ||
+      !tbl || slots < 1 || slots > kMaxSlots || len < 1)
+    return -1;
+  Cell &c = b->cells[cell];
+  std::vector<int32_t> soa((size_t)slots * len);
+  for (long long t = 0; t < len; t++)
+    for (int k = 0; k < slots; k++) {
+      const int32_t v = tbl[t * slots + k];
+      if (v) {
+        const int pos = v >> 24, dl = v & 0xFFFFFF;
+        if (pos < 0 || pos >= c.g.n || dl < 1 || dl >= c.g.ax[pos]) return -1;
+      }
+      soa[(size_t)k * len + t] = v;
+    }
+  if (c.dtbl) cudaFree(c.dtbl);
+  c.dtbl = nullptr;
+  CC_CK(cudaMalloc(&c.dtbl, soa.size() * 4));
+  CC_CK(cudaMemcpy(c.dtbl, soa.data(), soa.size() * 4,
+                   cudaMemcpyHostToDevice));
+  c.slots = slots;
+  c.tlen = len;
+  return 0;
+}
+
+namespace {
+
+int stage_cell_words(Batch *b, const Cell &c, const long long *words,
+                     int nw) {
+  if (nw < 0 || nw > (1 << 16) || (nw && !words)) return -1;
+  for (int i = 0; i < nw; i++)
+    if (words[i] < 0 || words[i] >= c.g.space) return -1;
+  if (!b->d_words) {
+    CC_CK(cudaMalloc(&b->d_words, (size_t)(1 << 16) * 8));
+    CC_CK(cudaMalloc(&b->d_out, (size_t)(1 << 16) * 4));
+    CC_CK(cudaMalloc(&b->d_count, 16));
+  }
+  if (nw)
+    CC_CK(cudaMemcpyAsync(b->d_words, words, (size_t)nw * 8,
+                          cudaMemcpyHostToDevice, b->stream));
+  return 0;
+}
+
+WalkArgs cell_walk(const Cell &c) {
+  WalkArgs w{};
+  w.g = c.g;
+  w.tbl = c.dtbl;
+  w.slots = c.slots;
+  w.len = c.tlen;
+  w.cnt = c.cnt;
+  return w;
+}
+
+Cell *live_cell(long long h, int cell, Batch **pb) {
+  Batch *b = get(h);
+  if (!b || !b->built || cell < 0 || cell >= (int)b->cells.size())
+    return nullptr;
+  *pb = b;
+  return &b->cells[cell];
+}
+
+}  // namespace
+
+// cnt += delta over the balls of nw words (delta +1 or -1; the caller keeps
+// the multiset valid, as the search core does)
+int dct_batch_update(long long h, int cell, const long long *words, int nw,
+                     int delta) {
+  Batch *b = nullptr;
+  Cell *c = live_cell(h, cell, &b);
+  if (!c || !c->dtbl || (delta != 1 && delta != -1)) return -1;
+  int rc = stage_cell_words(b, *c, words, nw);
+  if (rc || !nw) return rc;
+  rc = launch_update(cell_walk(*c), b->d_words, nullptr, nw, delta, nullptr,
+                     b->stream);
+  if (rc) return rc;
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+// out[i] = #{x in B(w_i) : role(cnt[x])}: role 0 deficient (cnt < mu),
+// 1 critical (1 <= cnt <= mu), else the literal cnt == role
+int dct_batch_gather(long long h, int cell, const long long *words, int nw,
+                     int role, int32_t *out) {
+  Batch *b = nullptr;
+  Cell *c = live_cell(h, cell, &b);
+  if (!c || !c->dtbl || role < 0 || (nw && !out)) return -1;
+  int rc = stage_cell_words(b, *c, words, nw);
+  if (rc || !nw) return rc;
+  const int mode = role == 0 ? (c->g.mu > 1 ? kPredDef : kPredEq)
+                   : role == 1 ? (c->g.mu > 1 ? kPredCrit : kPredEq)
+                               : kPredEq;
+  rc = launch_gather(cell_walk(*c), b->d_words, nw, mode, role, b->d_out,
+                     false, b->stream);
+  if (rc) return rc;
+  CC_CK(cudaMemcpyAsync(out, b->d_out, (size_t)nw * 4,
+                        cudaMemcpyDeviceToHost, b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+// entries of the gain (field 1) or loss (field 2) map at or above thr:
+// up to cap (index, value) pairs, unordered; returns how many there are
+long long dct_batch_extract(long long h, int cell, int field, int32_t thr,
+                            long long *idx, int32_t *val, int cap) {
+  Batch *b = nullptr;
+  Cell *c = live_cell(h, cell, &b);
+  if (!c || (field != 1 && field != 2) || cap < 0 || (cap && (!idx || !val)))
+    return -1;
+  if (cap > b->ext_cap) {
+    if (b->d_ext) cudaFree(b->d_ext);
+    if (b->d_extv) cudaFree(b->d_extv);
+    b->d_ext = nullptr;
+    b->d_extv = nullptr;
+    CC_CK(cudaMalloc(&b->d_ext, (size_t)cap * 8));
+    CC_CK(cudaMalloc(&b->d_extv, (size_t)cap * 4));
+    b->ext_cap = cap;
+  }
+  if (!b->d_count) CC_CK(cudaMalloc(&b->d_count, 16));
+  CC_CK(cudaMemsetAsync(b->d_count, 0, 8, b->stream));
+  const int32_t *A = field == 1 ? c->gain : c->loss;
+  int rc = launch_extract(A, c->g.space, thr, b->d_ext, true, b->d_extv, cap,
+                          b->d_count, b->stream);
+  if (rc) return rc;
+  long long found = 0;
+  CC_CK(cudaMemcpyAsync(&found, b->d_count, 8, cudaMemcpyDeviceToHost,
+                        b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  const long long n = std::min<long long>(found, cap);
+  if (n) {
+    CC_CK(cudaMemcpyAsync(idx, b->d_ext, (size_t)n * 8,
+                          cudaMemcpyDeviceToHost, b->stream));
+    CC_CK(cudaMemcpyAsync(val, b->d_extv, (size_t)n * 4,
+                          cudaMemcpyDeviceToHost, b->stream));
+    CC_CK(cudaStreamSynchronize(b->stream));
+  }
+  return found;
+}
+
+// mode 0: #{x : cnt[x] == target}; 1: the deficit sum max(0, mu - cnt)
+long long dct_batch_count(long long h, int cell, int mode, int target) {
+  Batch *b = nullptr;
+  Cell *c = live_cell(h, cell, &b);
+  if (!c || mode < 0 || mode > 1) return -1;
+  if (!b->d_count) CC_CK(cudaMalloc(&b->d_count, 16));
+  CC_CK(cudaMemsetAsync(b->d_count, 0, 8, b->stream));
+  const int rc = launch_cnt_reduce(c->cnt, c->g.space,
+                                   mode == 1 ? kPredDef : kPredEq, target,
+                                   c->g.mu, b->d_count, b->stream);
+  if (rc) return rc;
+  long long v = 0;
+  CC_CK(cudaMemcpyAsync(&v, b->d_count, 8, cudaMemcpyDeviceToHost,
+                        b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return v;
+}
+
+// the gain (field 1) or loss (field 2) map at k words
+int dct_batch_read_at(long long h, int cell, int field, const long long *idx,
+                      int k, int32_t *out) {
+  Batch *b = nullptr;
+  Cell *c = live_cell(h, cell, &b);
+  if (!c || (field != 1 && field != 2) || (k && !out)) return -1;
+  int rc = stage_cell_words(b, *c, idx, k);
+  if (rc || !k) return rc;
+  rc = launch_read_at(field == 1 ? c->gain : c->loss, b->d_words, k,
+                      b->d_out, b->stream);
+  if (rc) return rc;
+  CC_CK(cudaMemcpyAsync(out, b->d_out, (size_t)k * 4, cudaMemcpyDeviceToHost,
+                        b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  return 0;
 }
 
 int dct_batch_free(long long h) {

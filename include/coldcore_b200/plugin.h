@@ -192,8 +192,9 @@ CCP_API int  dct_batch_add(long long h, int problem, int n, const int *ax,
                            int R, int mu, const long long *code, int M);
 /* allocates and schedules; tile_kb = shared memory per tile, 0 = autotune */
 CCP_API int  dct_batch_build(long long h, int tile_kb);
-/* mode 0: the persistent graph launch; 1: one launch per pass per cell;
- * 2: self-test of the bounded dependency wait (returns -7, no hang) */
+/* mode 0: the persistent graph launch; 1: one launch per pass per cell
+ * (same kernels and streams, no graph); 2: self-test of the bounded
+ * dependency wait (returns -7, no hang) */
 CCP_API int  dct_batch_run(long long h, int mode);
 /* field 0 cnt (uint16), 1 gain map (int32), 2 loss map (int32) */
 CCP_API int  dct_batch_read(long long h, int cell, int field, long long off,
@@ -202,6 +203,32 @@ CCP_API int  dct_batch_read(long long h, int cell, int field, long long off,
 CCP_API int  dct_batch_scalars(long long h, long long *out, int cap);
 /* cells, passes, work items, tile KB, grid, tuned step microseconds */
 CCP_API int  dct_batch_info(long long h, long long *out, int cap);
+/* Per-cell calls between launches, so a search can run on each cell
+ * (the role of a campaign job's own plugin context, campaign.py:88-179).
+ * set_code replaces a cell's code (room for 4x its first size, at least
+ * min(|X|, 2^18) words, else -3); the next launch recounts from it.  set_table gives
+ * the cell's support table (len x slots int32, (pos << 24) | shift, as
+ * dct_init3w takes it).  update adds delta (+1 / -1) over the balls of nw
+ * <= 65,536 words; gather counts ball words by role (0 deficient, 1
+ * critical, else cnt == role); extract lists the gain (field 1) or loss
+ * (field 2) map entries >= thr, unordered, and returns how many exist. */
+CCP_API int  dct_batch_set_code(long long h, int cell, const long long *code,
+                                int M);
+CCP_API int  dct_batch_set_table(long long h, int cell, const int32_t *tbl,
+                                 int slots, long long len);
+CCP_API int  dct_batch_update(long long h, int cell, const long long *words,
+                              int nw, int delta);
+CCP_API int  dct_batch_gather(long long h, int cell, const long long *words,
+                              int nw, int role, int32_t *out);
+CCP_API long long dct_batch_extract(long long h, int cell, int field,
+                                   int32_t thr, long long *idx, int32_t *val,
+                                   int cap);
+/* mode 0: #{x : cnt[x] == target}; mode 1: sum max(0, mu - cnt[x]) */
+CCP_API long long dct_batch_count(long long h, int cell, int mode,
+                                 int target);
+/* the gain (field 1) or loss (field 2) map at k <= 65,536 words */
+CCP_API int  dct_batch_read_at(long long h, int cell, int field,
+                               const long long *idx, int k, int32_t *out);
 CCP_API int  dct_batch_free(long long h);
 
 /* ---- learned ruin proposal scorer (no counterpart in the reference): a
