@@ -56,6 +56,10 @@ def _bind(lib):
     lib.dct_batch_read_at.restype = I
     lib.dct_batch_read_at.argtypes = [_LL, I, I, ctypes.POINTER(_LL), I,
                                       I32P]
+    IP = ctypes.POINTER(I)
+    lib.dct_batch_greedy.restype = I
+    lib.dct_batch_greedy.argtypes = [_LL, IP, I, IP, ctypes.POINTER(_LL), I,
+                                     IP, ctypes.POINTER(_LL)]
     lib._batch_bound = True
     return lib
 
@@ -168,6 +172,25 @@ class BatchEngine:
             _check("batch_extract", found)
         n = min(found, cap)
         return idx[:n].copy(), val[:n].copy(), found
+
+    def greedy(self, cells, max_add):
+        """Exact greedy on several cells at once (dct_batch_greedy):
+        returns per cell (placed words in order, deficit left)."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        adds = np.ascontiguousarray(max_add, dtype=np.int32)
+        n = len(cells)
+        cap = max(1, int(adds.max()) if n else 1)
+        placed = np.zeros(n * cap, dtype=np.int64)
+        nplaced = np.zeros(n, dtype=np.int32)
+        deficit = np.zeros(n, dtype=np.int64)
+        IP = ctypes.POINTER(ctypes.c_int)
+        _check("batch_greedy", self._lib.dct_batch_greedy(
+            self.h, cells.ctypes.data_as(IP), n, adds.ctypes.data_as(IP),
+            placed.ctypes.data_as(ctypes.POINTER(_LL)), cap,
+            nplaced.ctypes.data_as(IP),
+            deficit.ctypes.data_as(ctypes.POINTER(_LL))))
+        return [(placed[k * cap:k * cap + nplaced[k]].copy(), int(deficit[k]))
+                for k in range(n)]
 
     def count(self, cell, mode, target=0):
         r = int(self._lib.dct_batch_count(self.h, int(cell), int(mode),

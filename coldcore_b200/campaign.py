@@ -23,6 +23,7 @@ incremental updates.
 cell, seed, final size M, the uncovered count (0 = a verified cover), the
 solution trace and the search's counters.
 """
+import sys
 import threading
 import time
 import traceback
@@ -48,6 +49,9 @@ class Ticker:
         self.scalars = None
         self.ticks = 0
         self.error = None
+        self.greedy_req = {}            # cell -> words it may place
+        self.greedy_out = {}            # cell -> (placed, deficit)
+        self.greedy_calls = 0
 
     def join(self):
         with self.cv:
@@ -58,17 +62,25 @@ class Ticker:
             self.live -= 1
             self.cv.notify_all()
 
-    def request(self):
+    def request(self, greedy_cell=None, max_add=0):
         """Block until the next tick has run (every cell recounted from
-        its code, every gain and loss map rebuilt)."""
+        its code, every gain and loss map rebuilt).  With ``greedy_cell``,
+        that cell's exact greedy repair (up to ``max_add`` words) runs in
+        the same tick, beside every other cell asking for one; returns its
+        (placed words, deficit)."""
         with self.cv:
             t = self.tick
+            if greedy_cell is not None:
+                self.greedy_req[greedy_cell] = int(max_add)
             self.waiting += 1
             self.cv.notify_all()
             while self.tick == t and self.error is None:
                 self.cv.wait()
             if self.error is not None:
                 raise RuntimeError(f"batched tick failed: {self.error}")
+            if greedy_cell is not None:
+                return self.greedy_out.pop(greedy_cell)
+            return None
 
     def serve(self):
         """The driver loop: run a tick whenever every live search waits;
@@ -85,6 +97,17 @@ class Ticker:
                     self.engine.run(0)
                     self.scalars = self.engine.scalars()
                     self.ticks += 1
+                    if self.greedy_req:
+                        ids = sorted(self.greedy_req)
+                        # each placement serves a deficient word: no cell
+                        # places more words than its deficit
+                        adds = [max(0, min(self.greedy_req[k],
+                                           int(self.scalars[k, 0])))
+                                for k in ids]
+                        res = self.engine.greedy(ids, adds)
+                        self.greedy_out.update(zip(ids, res))
+                        self.greedy_req.clear()
+                        self.greedy_calls += 1
                 except Exception as e:          # noqa: BLE001
                     self.error = repr(e)
                 self.waiting = 0
@@ -139,6 +162,15 @@ class BatchCellBackend:
         self.ticker.request()
         self.field = 2
 
+    def greedy_fill_device(self, max_add):
+        """Exact greedy repair on the device, batched with every other
+        cell's in one tick: (placed words in order, deficit left)."""
+        placed, deficit = self.ticker.request(self.i, max_add)
+        if len(placed):
+            self.code.update(placed.tolist())
+            self._dirty = True
+        return placed, deficit
+
     # ---------------- incremental / exact
     def ball_update(self, idx, delta):
         idx = np.atleast_1d(np.asarray(idx, dtype=np.int64))
@@ -191,7 +223,7 @@ class _LockedEngine:
     stream and staging buffers, and ctypes releases the GIL during them."""
 
     _CALLS = ("set_code", "update", "gather", "count", "extract", "read_at",
-              "read_range")
+              "read_range", "greedy")
 
     def __init__(self, engine, lock):
         self._e, self._lock = engine, lock
@@ -236,7 +268,8 @@ def run_job(job, backend):
 
     try:
         s = Searcher(backend, seed=rec["seed"], deadline=t0 + budget,
-                     on_solved=on_solved)
+                     on_solved=on_solved,
+                     repair=job.get("repair", "exact"))
         s.build_reserve_s = s.loop_reserve_s = 0.0
         s.load(np.zeros(0, dtype=np.int64))
         s.greedy_fill(10 ** 9)
@@ -261,7 +294,8 @@ def run_job(job, backend):
     return rec
 
 
-def run_campaign(jobs, plugin_path=None, tile_kb=0, engine=None):
+def run_campaign(jobs, plugin_path=None, tile_kb=0, engine=None,
+                 switch_s=5e-5):
     """Every job's search on one batched engine (see the module text);
     returns one record per job, in job order, and the number of ticks.
     ``engine``: a stand-in with BatchEngine's methods (host tests)."""
@@ -290,11 +324,18 @@ def run_campaign(jobs, plugin_path=None, tile_kb=0, engine=None):
             ticker.join()
         threads = [threading.Thread(target=work, args=(k,), daemon=True)
                    for k in range(len(jobs))]
-        for t in threads:
-            t.start()
-        ticker.serve()
-        for t in threads:
-            t.join()
+        # a search thread returning from a device call waits for the GIL;
+        # hand it over often, or every call waits out the default 5 ms
+        switch = sys.getswitchinterval()
+        sys.setswitchinterval(switch_s)
+        try:
+            for t in threads:
+                t.start()
+            ticker.serve()
+            for t in threads:
+                t.join()
+        finally:
+            sys.setswitchinterval(switch)
         return recs, ticker.ticks
     finally:
         eng.close()

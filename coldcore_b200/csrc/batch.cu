@@ -894,6 +894,144 @@ long long dct_batch_extract(long long h, int cell, int field, int32_t thr,
   return found;
 }
 
+// Exact greedy on the listed cells at once (the device repair of a
+// campaign's searches): from each cell's gain map as the last launch left
+// it — the caller runs the step after its last update — with the cell's
+// code words excluded, each step places, in every cell still placing, the
+// word of largest gain (ties: smallest index) until the cell's deficit is 0,
+// no word gains, or max_add[k] words are placed.  placed_out holds cap words
+// per listed cell; nplaced_out and deficit_out one value per listed cell.
+int dct_batch_greedy(long long h, const int *cells, int n, const int *max_add,
+                     long long *placed_out, int cap, int *nplaced_out,
+                     long long *deficit_out) {
+  Batch *b = get(h);
+  if (!b || !b->built || n < 0 || (n && (!cells || !max_add || !placed_out ||
+                                         !nplaced_out || !deficit_out)) ||
+      cap < 0)
+    return -1;
+  if (n == 0) return 0;
+  std::vector<long long> sc(b->cells.size() * 3);
+  CC_CK(cudaMemcpyAsync(sc.data(), b->d_scal, sc.size() * 8,
+                        cudaMemcpyDeviceToHost, b->stream));
+  CC_CK(cudaStreamSynchronize(b->stream));
+  long long max_space = 0, steps = 0, fresh_words = 0;
+  for (int k = 0; k < n; k++) {
+    if (cells[k] < 0 || cells[k] >= (int)b->cells.size() || max_add[k] < 0 ||
+        max_add[k] > cap)
+      return -1;
+    const Cell &c = b->cells[cells[k]];
+    if (!c.dtbl || c.g.space >= (1LL << 32)) return -1;
+    // placed words are new (multiplicity 1): the counters stay within
+    // min(occurrences, max multiplicity x |B|) <= 65,535
+    long long maxmult = 1, run = 0;
+    for (size_t i = 0; i < c.code.size(); i++) {
+      run = (i && c.code[i] == c.code[i - 1]) ? run + 1 : 1;
+      if (run > maxmult) maxmult = run;
+    }
+    if (std::min<long long>((long long)c.code.size() + max_add[k],
+                            maxmult * ball_cardinality(c.g)) > 65535)
+      return -1;
+    max_space = std::max(max_space, c.g.space);
+    steps = std::max<long long>(steps, std::min<long long>(
+        max_add[k], sc[3 * cells[k]]));
+    fresh_words += c.tlen;
+  }
+  // device state: per cell a GreedyState, its placed list and fresh list
+  char *ws = nullptr;
+  const size_t st_b = (size_t)n * kGreedyStateBytes;
+  const size_t pl_b = (size_t)n * std::max(cap, 1) * 8;
+  const size_t fr_b = (size_t)fresh_words * 8;
+  const size_t tb_b = (size_t)n * sizeof(BatchGreedyCell);
+  CC_CK(cudaMalloc(&ws, st_b + pl_b + fr_b + tb_b));
+  int rc = 0;
+  std::vector<BatchGreedyCell> tab(n);
+  std::vector<unsigned char> st0(st_b, 0);
+  {
+    long long fo = 0;
+    for (int k = 0; k < n; k++) {
+      Cell &c = b->cells[cells[k]];
+      BatchGreedyCell &g = tab[k];
+      g.w = WalkArgs{};
+      g.w.g = c.g;
+      g.w.tbl = c.dtbl;
+      g.w.slots = c.slots;
+      g.w.len = c.tlen;
+      g.w.cnt = c.cnt;
+      g.map = c.gain;
+      g.st = ws + (size_t)k * kGreedyStateBytes;
+      g.placed = reinterpret_cast<long long *>(ws + st_b) +
+                 (size_t)k * std::max(cap, 1);
+      g.fresh = reinterpret_cast<long long *>(ws + st_b + pl_b) + fo;
+      g.max_add = max_add[k];
+      fo += c.tlen;
+      // state: best 0, deficit from the last launch, done when nothing to do
+      long long *words = reinterpret_cast<long long *>(&st0[(size_t)k *
+                                                          kGreedyStateBytes]);
+      words[1] = sc[3 * cells[k]];
+      int *flags = reinterpret_cast<int *>(words + 2);
+      flags[0] = (max_add[k] == 0 || sc[3 * cells[k]] == 0) ? 1 : 0;
+      deficit_out[k] = sc[3 * cells[k]];
+      nplaced_out[k] = 0;
+    }
+  }
+  BatchGreedyCell *dtab = reinterpret_cast<BatchGreedyCell *>(
+      ws + st_b + pl_b + fr_b);
+  constexpr int32_t kExcluded = INT_MIN / 2;
+  auto ck = [&](cudaError_t e) {
+    if (e != cudaSuccess && !rc) rc = -(100 + (int)e);
+  };
+  ck(cudaMemcpyAsync(ws, st0.data(), st_b, cudaMemcpyHostToDevice,
+                     b->stream));
+  ck(cudaMemcpyAsync(dtab, tab.data(), tb_b, cudaMemcpyHostToDevice,
+                     b->stream));
+  // incumbents never re-enter
+  for (int k = 0; k < n && !rc; k++) {
+    const Cell &c = b->cells[cells[k]];
+    if (!c.code.empty())
+      rc = launch_greedy_exclude(c.gain, c.dcode, (int)c.code.size(),
+                                 kExcluded, b->stream);
+  }
+  // steps in chunks, with one look at the states between chunks
+  long long issued = 0, chunk = 32;
+  std::vector<unsigned char> stv(st_b);
+  while (!rc && issued < steps) {
+    const long long m = std::min(chunk, steps - issued);
+    for (long long i = 0; i < m && !rc; i++)
+      rc = launch_batch_greedy_step(dtab, n, max_space, kExcluded,
+                                    b->stream);
+    issued += m;
+    ck(cudaMemcpyAsync(stv.data(), ws, st_b, cudaMemcpyDeviceToHost,
+                       b->stream));
+    ck(cudaStreamSynchronize(b->stream));
+    bool all = true;
+    for (int k = 0; k < n; k++)
+      all &= reinterpret_cast<int *>(&stv[(size_t)k * kGreedyStateBytes +
+                                          16])[0] != 0;
+    if (all) break;
+    chunk = std::min<long long>(chunk * 2, 512);
+  }
+  if (!rc) {
+    ck(cudaMemcpyAsync(stv.data(), ws, st_b, cudaMemcpyDeviceToHost,
+                       b->stream));
+    ck(cudaStreamSynchronize(b->stream));
+    for (int k = 0; k < n && !rc; k++) {
+      const long long *words = reinterpret_cast<const long long *>(
+          &stv[(size_t)k * kGreedyStateBytes]);
+      const int *flags = reinterpret_cast<const int *>(words + 2);
+      deficit_out[k] = words[1];
+      nplaced_out[k] = flags[1];
+      if (flags[1])
+        ck(cudaMemcpyAsync(placed_out + (size_t)k * cap, tab[k].placed,
+                           (size_t)flags[1] * 8, cudaMemcpyDeviceToHost,
+                           b->stream));
+    }
+    ck(cudaStreamSynchronize(b->stream));
+  }
+  cudaStreamSynchronize(b->stream);
+  cudaFree(ws);
+  return rc;
+}
+
 // mode 0: #{x : cnt[x] == target}; 1: the deficit sum max(0, mu - cnt)
 long long dct_batch_count(long long h, int cell, int mode, int target) {
   Batch *b = nullptr;

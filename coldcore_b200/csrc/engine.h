@@ -232,6 +232,18 @@ struct GreedyState;
 constexpr int kGreedyStateBytes = 32;
 int launch_greedy_exclude(int32_t *map, const long long *dwords, int n,
                           int32_t exclude, cudaStream_t s);
+// the batched form: one cell's walk, gain map, state and buffers
+struct BatchGreedyCell {
+  WalkArgs w;
+  int32_t *map;
+  void *st;                 // GreedyState (kGreedyStateBytes)
+  long long *placed;
+  long long *fresh;         // |B| words
+  int max_add;
+};
+int launch_batch_greedy_step(const BatchGreedyCell *dcells, int ncells,
+                             long long max_space, int32_t exclude,
+                             cudaStream_t s);
 int launch_greedy_step(const WalkArgs &w, int32_t *map, long long N,
                        GreedyState *st, long long *placed, int max_add,
                        long long *fresh, int32_t exclude, cudaStream_t s);

@@ -388,6 +388,127 @@ k_greedy_refresh(const WalkArgs a, int32_t *map, const GreedyState *st,
   }
 }
 
+// ------------------------------------------------------------ batched greedy
+// The same exact greedy over many cells at once (the batched engine's
+// campaign repair): one argmax, one place and one refresh launch per step
+// for every cell, each cell's state and buffers in its BatchGreedyCell.
+// Cells that are done return at once, so the launches of a step cost only
+// the cells still placing.
+constexpr int kArgmaxChunk = 8192;        // words per argmax block
+
+__global__ void __launch_bounds__(256)
+k_bgreedy_argmax(const BatchGreedyCell *cells) {
+  const BatchGreedyCell &c = cells[blockIdx.y];
+  GreedyState *st = reinterpret_cast<GreedyState *>(c.st);
+  if (st->done) return;
+  const long long N = c.w.g.space;
+  const long long x0 = (long long)blockIdx.x * kArgmaxChunk;
+  if (x0 >= N) return;
+  const long long x1 = min(N, x0 + (long long)kArgmaxChunk);
+  unsigned long long k = 0;
+  for (long long x = x0 + threadIdx.x; x < x1; x += blockDim.x)
+    k = max(k, greedy_key(__ldcg(c.map + x), x));
+  for (int o = 16; o > 0; o >>= 1)
+    k = max(k, __shfl_down_sync(0xffffffffu, k, o));
+  if ((threadIdx.x & 31) == 0 && k) atomicMax(&st->best, k);
+}
+
+template <bool GRID>
+__device__ __forceinline__ void bgreedy_place(const BatchGreedyCell &c,
+                                              int32_t exclude) {
+  __shared__ WordSmem s;
+  __shared__ long long w_s;
+  __shared__ int stop;
+  __shared__ int nfresh;
+  GreedyState *st = reinterpret_cast<GreedyState *>(c.st);
+  const WalkArgs &a = c.w;
+  if (threadIdx.x == 0) {
+    stop = st->done;
+    if (!stop) {
+      const unsigned long long k = st->best;
+      const int32_t v = (int32_t)((uint32_t)(k >> 32) ^ 0x80000000u);
+      const long long x = (long long)(uint32_t)~(uint32_t)k;
+      if (k == 0 || v <= 0 || st->deficit <= 0 || st->placed >= c.max_add) {
+        st->done = 1;
+        stop = 1;
+      } else {
+        w_s = x;
+        c.placed[st->placed] = x;
+        st->placed += 1;
+        c.map[x] = exclude;
+      }
+    }
+    st->best = 0;
+    st->nnew = 0;
+    nfresh = 0;
+  }
+  __syncthreads();
+  if (stop) return;
+  const long long w = w_s;
+  word_setup(a.g, w, s);
+  long long mine = 0;
+  for (long long t = threadIdx.x; t < a.len; t += blockDim.x) {
+    const long long x = walk_word<GRID>(a, w, t, s);
+    if (x < 0) continue;
+    uint32_t *cell = reinterpret_cast<uint32_t *>(a.cnt + (x & ~1LL));
+    const int sh = (x & 1) ? 16 : 0;
+    const uint32_t old = atomicAdd(cell, 1u << sh);
+    const int cv = (int)((old >> sh) & 0xFFFFu);
+    if (cv < a.g.mu) mine++;
+    if (cv == a.g.mu - 1) c.fresh[atomicAdd(&nfresh, 1)] = x;
+  }
+  mine = block_sum(mine);
+  if (threadIdx.x == 0) {
+    st->deficit -= mine;
+    st->nnew = nfresh;
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_bgreedy_place(const BatchGreedyCell *cells, int32_t exclude) {
+  const BatchGreedyCell &c = cells[blockIdx.x];
+  if (c.w.g.prob == kGrid) bgreedy_place<true>(c, exclude);
+  else bgreedy_place<false>(c, exclude);
+}
+
+template <bool GRID>
+__device__ __forceinline__ void bgreedy_refresh(const BatchGreedyCell &c) {
+  __shared__ WordSmem s;
+  const GreedyState *st = reinterpret_cast<const GreedyState *>(c.st);
+  if (st->done) return;
+  const int n = st->nnew;
+  for (int u = blockIdx.x; u < n; u += gridDim.x) {
+    const long long x0 = c.fresh[u];
+    __syncthreads();
+    word_setup(c.w.g, x0, s);
+    for (long long t = threadIdx.x; t < c.w.len; t += blockDim.x) {
+      const long long y = walk_word<GRID>(c.w, x0, t, s);
+      if (y >= 0) atomicSub(&c.map[y], 1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_bgreedy_refresh(const BatchGreedyCell *cells) {
+  const BatchGreedyCell &c = cells[blockIdx.y];
+  if (c.w.g.prob == kGrid) bgreedy_refresh<true>(c);
+  else bgreedy_refresh<false>(c);
+}
+
+// one step for every cell of the table
+int launch_batch_greedy_step(const BatchGreedyCell *dcells, int ncells,
+                             long long max_space, int32_t exclude,
+                             cudaStream_t s) {
+  if (ncells <= 0) return 0;
+  const dim3 ga((unsigned)((max_space + kArgmaxChunk - 1) / kArgmaxChunk),
+                (unsigned)ncells);
+  k_bgreedy_argmax<<<ga, 256, 0, s>>>(dcells);
+  k_bgreedy_place<<<(unsigned)ncells, 256, 0, s>>>(dcells, exclude);
+  k_bgreedy_refresh<<<dim3(16, (unsigned)ncells), 256, 0, s>>>(dcells);
+  CC_CK(cudaGetLastError());
+  return 0;
+}
+
 int launch_greedy_exclude(int32_t *map, const long long *dwords, int n,
                           int32_t exclude, cudaStream_t s) {
   if (n <= 0) return 0;

@@ -411,7 +411,9 @@ class GpuBackend:
     def greedy_fill_device(self, max_add):
         """Exact greedy repair on the GPU: places up to ``max_add`` words of
         largest exact gain (ties: smallest index), non-active words only;
-        returns (placed words in order, deficit left)."""
+        returns (placed words in order, deficit left).  Every placement
+        serves a deficient word, so at most the deficit is placed."""
+        max_add = min(int(max_add), self.uncovered())
         placed = np.zeros(max(1, int(max_add)), dtype=np.int64)
         deficit = _LL(0)
         n = self._lib.dct_b200_greedy_fill(int(max_add), _p(placed),

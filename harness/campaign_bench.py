@@ -4,7 +4,10 @@ per cell.
 Jobs: ``workloads.batch_cells(count, seed, lo, hi)`` geometries (q in 2..6,
 q^n log-uniform in 10^lo..10^hi words, R in 1..4, 80% Hamming / 20% Lee),
 each job a greedy cover from empty followed by peel (a fixed amount of
-search work, no time budget).  The batched arm runs every job in lock step
+search work, no time budget), the greedy on the device by default
+(``repair="device"``: in the batched arm all cells' greedy steps share one
+launch per step; in the serial arm each cell runs the singleton's device
+greedy), or the Python lazy greedy (``--repair exact``).  The batched arm runs every job in lock step
 on one BatchEngine (``coldcore_b200.campaign.run_campaign``); the serial
 arm runs the same jobs one after another, each on its own singleton cell
 context (``run_serial``), the pattern of coldcore's process-per-cell
@@ -18,17 +21,17 @@ import json
 import time
 
 
-def jobs_for(count=64, seed=13, lo=3.0, hi=5.0):
+def jobs_for(count=64, seed=13, lo=3.0, hi=5.0, repair="device"):
     from coldcore_b200.workloads import batch_cells
     return [{"problem": p, "axes": list(a), "R": R, "seed": 100 + k,
-             "budget_s": 600.0, "mode": "build"}
+             "budget_s": 600.0, "mode": "build", "repair": repair}
             for k, (p, a, R, _code) in enumerate(
                 batch_cells(count, seed=seed, lo=lo, hi=hi))]
 
 
-def measure(count=64, seed=13, lo=3.0, hi=5.0):
+def measure(count=64, seed=13, lo=3.0, hi=5.0, repair="device"):
     from coldcore_b200.campaign import run_campaign, run_serial
-    jobs = jobs_for(count, seed, lo, hi)
+    jobs = jobs_for(count, seed, lo, hi, repair)
     run_campaign(jobs[:4])                  # warm the library and tables
     t0 = time.perf_counter()
     recs, ticks = run_campaign(jobs)
@@ -38,7 +41,9 @@ def measure(count=64, seed=13, lo=3.0, hi=5.0):
     ts = time.perf_counter() - t0
     ok_b = sum(1 for r in recs if r["error"] is None and r["uncov"] == 0)
     ok_s = sum(1 for r in srecs if r["error"] is None and r["uncov"] == 0)
+    same = sum(1 for r, q in zip(recs, srecs) if r.get("code") == q.get("code"))
     return {"jobs": len(jobs), "work": "greedy cover from empty + peel",
+            "repair": repair, "identical_covers": same,
             "cells": f"batch_cells({count}, seed={seed}, lo={lo}, hi={hi})",
             "batched": {"seconds": round(tb, 3), "ticks": ticks,
                         "instances_per_s": round(len(jobs) / tb, 2),
@@ -58,8 +63,10 @@ def main():
     ap.add_argument("--seed", type=int, default=13)
     ap.add_argument("--lo", type=float, default=3.0)
     ap.add_argument("--hi", type=float, default=5.0)
+    ap.add_argument("--repair", default="device", choices=("device", "exact"))
     a = ap.parse_args()
-    print(json.dumps(measure(a.count, a.seed, a.lo, a.hi), indent=1))
+    print(json.dumps(measure(a.count, a.seed, a.lo, a.hi, a.repair),
+                     indent=1))
 
 
 if __name__ == "__main__":

@@ -223,6 +223,16 @@ CCP_API int  dct_batch_gather(long long h, int cell, const long long *words,
 CCP_API long long dct_batch_extract(long long h, int cell, int field,
                                    int32_t thr, long long *idx, int32_t *val,
                                    int cap);
+/* Exact greedy on n listed cells at once, one argmax / place / refresh
+ * launch per step for all of them: from each cell's gain map as the last
+ * launch left it (no update since), code words excluded, place the word of
+ * largest gain (ties: smallest index) until the deficit is 0, nothing
+ * gains, or max_add[k] (<= cap) words are placed; the same rule as
+ * dct_b200_greedy_fill.  placed_out: cap words per listed cell. */
+CCP_API int  dct_batch_greedy(long long h, const int *cells, int n,
+                              const int *max_add, long long *placed_out,
+                              int cap, int *nplaced_out,
+                              long long *deficit_out);
 /* mode 0: #{x : cnt[x] == target}; mode 1: sum max(0, mu - cnt[x]) */
 CCP_API long long dct_batch_count(long long h, int cell, int mode,
                                  int target);

@@ -54,6 +54,14 @@ class OracleBatch:
     def gather(self, cell, words, role):
         return self.cells[cell]["o"].ball_gather(words, role)
 
+    def greedy(self, cells, adds):
+        from oracle.dp_oracle import exact_greedy
+        out = []
+        for k, add in zip(cells, adds):
+            c = self.cells[k]
+            out.append(exact_greedy(c["o"], c["code"], add))
+        return out
+
     def count(self, cell, mode, target=0):
         o = self.cells[cell]["o"]
         return o.uncovered() if mode == 1 else o.count_eq(target)
@@ -104,3 +112,18 @@ def test_a_failing_search_is_recorded_and_the_others_finish():
     recs, _ = run_campaign(JOBS[:3], engine=OracleBatch(fail_cell=1))
     assert recs[1]["error"] and "planted failure" in recs[1]["error"]
     assert recs[0]["uncov"] == 0 and recs[2]["uncov"] == 0
+
+
+def test_device_repair_runs_in_the_ticks():
+    """repair="device": every search's greedy runs inside a tick, batched
+    with the others, and ends in the same cover as the exact greedy."""
+    jobs = [dict(j, repair="device") for j in JOBS]
+    eng = OracleBatch()
+    recs, ticks = run_campaign(jobs, engine=eng)
+    for j, r in zip(jobs, recs):
+        assert r["error"] is None, r["error"]
+        assert r["uncov"] == 0
+        o = OracleBackend(j["axes"], j["R"], problem=j["problem"],
+                          mu=j.get("mu", 1))
+        o.recount(np.asarray(r["code"], np.int64))
+        assert o.uncovered() == 0

@@ -87,3 +87,22 @@ def test_campaign_covers_verify_and_match_the_serial_arm():
         # same algorithm and seed; extraction order may differ on a GPU
         assert sr["uncov"] == 0
         assert abs(r["M"] - sr["M"]) <= max(3, sr["M"] // 20), (r, sr)
+
+
+def test_batched_device_repair_equals_the_singleton_repair():
+    """repair="device": the batched greedy (one launch per step for every
+    cell) places exactly the words the singleton's device greedy places,
+    so both campaigns end in the same covers, word for word."""
+    jobs = [{"problem": p, "axes": list(a), "R": R, "mu": mu, "seed": 11 + k,
+             "budget_s": 60.0, "repair": "device"}
+            for k, (p, a, R, mu) in enumerate(CELLS)]
+    recs, ticks = run_campaign(jobs)
+    serial = run_serial(jobs)
+    for j, r, sr in zip(jobs, recs, serial):
+        assert r["error"] is None and sr["error"] is None, (r, sr)
+        assert r["uncov"] == 0 == sr["uncov"]
+        assert r["code"] == sr["code"], j
+        o = OracleBackend(j["axes"], j["R"], problem=j["problem"],
+                          mu=j.get("mu", 1))
+        o.recount(np.asarray(r["code"], np.int64))
+        assert o.uncovered() == 0
