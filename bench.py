@@ -647,6 +647,12 @@ def run_b200(args, dist):
             from harness.ops_bench import measure as ops_measure
             return ops_measure(cpu=not args.no_cpu)
         leg("ops", ops)
+    if not args.no_ooc and dist.world == 1:
+        # a cell streamed through a forced 8 GB device budget
+        def ooc():
+            from harness.ooc_bench import measure as ooc_measure
+            return ooc_measure()
+        leg("out_of_hbm", ooc)
     if not args.no_incidence and dist.world == 1:
         # the explicit-incidence engine (plugin ABI 2) on a covering design
         def incidence():
@@ -675,6 +681,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-lns", action="store_true")
     ap.add_argument("--no-ops", action="store_true")
+    ap.add_argument("--no-ooc", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--lns-budget", type=float, default=60.0)
     ap.add_argument("--lns-moves", type=int, default=30000)
