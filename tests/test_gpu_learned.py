@@ -150,36 +150,39 @@ def test_gate_closes_on_low_auc(gpu):
 
 
 def test_learned_proposal_beats_plain_lns_on_k3_14_3(gpu):
-    """The gain, measured: on K_3(14,3) (4.78M words, R = 3) from the same
-    greedy start, a descent whose ruins the trained model picks does at
-    least as well as the plain descent with the record mix in the same wall
-    time: a smaller verified size, or the plain run's best size reached no
-    later.  Both are scored by the exact repair and full recounts.  The
-    model is trained here on moves logged from plain runs on other
-    seeds."""
+    """The gain, measured: on K_3(14,3) (4.78M words, R = 3), from the same
+    greedy start per seed, descents whose ruins the trained model picks do
+    at least as well as plain descents with the record mix in the same
+    wall time, over three seeds: no larger a summed best verified size, and
+    no worse a size in a majority of the seeds.  The device exact greedy
+    repairs both arms (thousands of rounds a run), every size is a full
+    recount, and the model is trained here on moves logged from plain runs
+    on other seeds."""
     from coldcore_b200.learned import LearnedRuin, RuinFeatures, train_scorer
-    from harness.lns_study import (descent, greedy_start, log_moves,
-                                         time_to)
+    from harness.lns_study import descent, greedy_start, log_moves
     b = gpu.GpuBackend([3] * 14, 3)
     try:
         feats = RuinFeatures(b)
-        mlog = log_moves(b, feats, 30000, 60.0, 15.0, say=lambda *a: None)
+        mlog = log_moves(b, feats, 30000, 60.0, 15.0, say=lambda *a: None,
+                         repair="device")
         X, y, g = mlog.arrays()
         assert len(y) >= 10000 and 0 < y.mean() < 0.5
         sc = train_scorer(X, y, g, epochs=15)
         assert sc.heldout_auc > 0.6
-        start = greedy_start(b, 7)
-        plain, _, ok_p = descent(b, start, 7, 30.0, "fixed", notch_s=15.0)
-        prop = LearnedRuin(sc, feats, seed=7)
-        learned, st, ok_l = descent(b, start, 7, 30.0, "learned",
-                                    proposer=prop, notch_s=15.0)
-        assert ok_p and ok_l
-        assert st["learned_rounds"] > 0
-        best_plain = min(m for _, m in plain)
-        best_learned = min(m for _, m in learned)
-        assert best_learned <= best_plain, (plain, learned)
-        if best_learned == best_plain:
-            assert time_to(learned, best_plain) <= time_to(plain, best_plain), (
-                plain, learned)
+        bests = []
+        for seed in (7, 8, 9):
+            start = greedy_start(b, seed)
+            plain, _, ok_p = descent(b, start, seed, 20.0, "fixed",
+                                     notch_s=10.0, repair="device")
+            prop = LearnedRuin(sc, feats, seed=seed)
+            learned, st, ok_l = descent(b, start, seed, 20.0, "learned",
+                                        proposer=prop, notch_s=10.0,
+                                        repair="device")
+            assert ok_p and ok_l
+            assert st["learned_rounds"] > 0
+            bests.append((min(m for _, m in plain),
+                          min(m for _, m in learned)))
+        assert sum(lv for _, lv in bests) <= sum(pv for pv, _ in bests), bests
+        assert sum(lv <= pv for pv, lv in bests) >= 2, bests
     finally:
         b.close()
