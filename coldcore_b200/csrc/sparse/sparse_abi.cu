@@ -458,13 +458,15 @@ int stage_words(const long long *idx, long long m) {
   return 0;
 }
 
-// The role-bit form of a dense field or gather (CC_SPARSE_BITS=1): the
-// bits of the whole universe in at most 48 KB of shared memory a CTA.
+// The role-bit form of a dense field or gather, the default (CC_SPARSE_BITS
+// =0 turns it off): the bits of the whole universe in at most 48 KB of
+// shared memory a CTA.  On C(30,8,4) a field took 0.763 ms in this form
+// against 0.848 ms with per-entry counter reads.
 constexpr long long kBitsMaxWords = 48 * 1024 / 4;
 
 bool use_bits() {
   const char *e = getenv("CC_SPARSE_BITS");
-  return e && atoi(e) == 1 && !C.csr &&
+  return !(e && atoi(e) == 0) && !C.csr &&
          (C.nuniv + 31) / 32 <= kBitsMaxWords;
 }
 
