@@ -13,14 +13,27 @@
 
 namespace cc {
 
-template <bool GRID, int SRC16, int DST16>
+// The word x = (o * q + a) * stride + i of the pass's axis position a:
+// with the space below 2^31 words the digit comes from two 32-bit
+// divisions (a 64-bit division costs several times more instructions, and
+// the pass is issue-bound: one read of each of 2R+1 neighbours a word).
+template <bool GRID, int SRC16, int DST16, bool I32>
 __global__ void __launch_bounds__(256) window_axis(const WindowArgs w) {
   const long long gs = (long long)gridDim.x * blockDim.x;
   for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
        x < w.space; x += gs) {
-    const long long hi = x / w.stride;
-    const int a = (int)(hi % w.q);
-    const long long base = x - (long long)a * w.stride;
+    int a;
+    long long base;
+    if (I32) {
+      const unsigned xs = (unsigned)x, st = (unsigned)w.stride;
+      const unsigned hi = xs / st;
+      a = (int)(hi % (unsigned)w.q);
+      base = (long long)(xs - (unsigned)a * st);
+    } else {
+      const long long hi = x / w.stride;
+      a = (int)(hi % w.q);
+      base = x - (long long)a * w.stride;
+    }
     int lo = a - w.R, up = a + w.R;
     if (GRID) { if (lo < 0) lo = 0; if (up > w.q - 1) up = w.q - 1; }
     int32_t s = 0;
@@ -42,7 +55,10 @@ int launch_window(const WindowArgs &w, cudaStream_t s) {
   if (nb > cap) nb = cap;
   if (nb < 1) nb = 1;
   const bool s16 = w.src16 != nullptr, d16 = w.dst16 != nullptr;
-#define WL(G, A, B) window_axis<G, A, B><<<(int)nb, 256, 0, s>>>(w)
+  const bool i32 = w.space < (1LL << 31);
+#define WL(G, A, B)                                                         \
+  (i32 ? window_axis<G, A, B, true><<<(int)nb, 256, 0, s>>>(w)              \
+       : window_axis<G, A, B, false><<<(int)nb, 256, 0, s>>>(w))
   if (w.grid) {
     if (s16 && d16) WL(true, 1, 1); else if (s16) WL(true, 1, 0);
     else if (d16) WL(true, 0, 1); else WL(true, 0, 0);
