@@ -83,6 +83,14 @@ struct GroupArgs {
   // group staged from cnt by bulk copies (tma 2)
   int tma;
   int stages;
+  // padded layout of the 16-bit planes (ternary cells): every run of t0
+  // words (the first group's mid) is stored at a pitch of `pitch` words
+  // (a multiple of 64), so rows of the later groups start on 128-byte
+  // boundaries.  The first group writes its layers padded; the later
+  // groups' `inner` is then the padded one, and the last group's map or
+  // cnt goes back to the canonical index.  0 = the canonical layout.
+  long long pitch;
+  long long t0;
 };
 
 // arguments of a streamed group launch (transform_tma.cu)
@@ -101,6 +109,9 @@ struct TmaArgs {
   // first group of a recount (code_first): the sorted code, per-tile slices
   const long long *code;
   const long long *code_bounds;
+  // padded planes (GroupArgs::pitch): the canonical inner stride, the
+  // pitch and the valid words of each padded run
+  long long inner_c, pitch, t0;
 };
 
 struct GroupPlan {
@@ -114,7 +125,9 @@ struct GroupPlan {
 // planner.cu: schedule knobs and the group plan of one transform
 // pipe: see plan_groups; half: 16-bit planes between the launches
 // pair: allow the pair first group (binary Hamming, 16-bit planes)
-struct Knobs { size_t budget; int pipe; int half = 0; int pair = 1; };
+// pad: the padded 16-bit layout for a ternary cell (streamed later groups)
+struct Knobs { size_t budget; int pipe; int half = 0; int pair = 1;
+               int pad = 0; };
 struct PlanPtrs {
   int32_t *layers; long long plane; uint16_t *cnt;
   const long long *code; long long ncode; int32_t *map;

@@ -245,6 +245,9 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
           v.grid = occupancy_grid(v);
           out.push_back(v);
         }
+  // a padded plan's later groups run streamed only (the register kernels
+  // address the canonical layout)
+  if (p.a.pitch && p.a.tma) return out;
   for (int stages : {0, 2, 3})
     if (!tma_off && tma_first_ok(p.a, R1, stages))
       for (int th : {128, 256, 512}) {

@@ -341,6 +341,56 @@ bool half_planes_ok(int src, int dst) {
   return src == kSrcCode || S.len <= 65535;
 }
 
+// The padded plan of a cell whose first group has an odd word count T0
+// (ternary): the first group writes its 16-bit layers at a pitch of P0 =
+// round_up(T0, 64) words a row, so every later group's rows start on 128-
+// byte boundaries and run as streamed launches over packed pairs; the last
+// writes the map or cnt back at the canonical index.  false when the cell
+// does not qualify or the padded planes do not fit the allocation.
+bool pad_plan(Plan &P) {
+  if (P.groups.size() < 2 || S.g.prob != kHamming) return false;
+  GroupPlan &f = P.groups[0];
+  const GroupArgs &a0 = f.a;
+  if (f.kernel < 0 || a0.inner != 1 || a0.W != 1 || !a0.out16 || a0.pack ||
+      a0.pair_axis || (a0.mid & 1) == 0)
+    return false;
+  const long long T0 = a0.mid;
+  const long long P0 = (T0 + 63) / 64 * 64;
+  const long long rows = S.g.space / T0;
+  const long long plane16 = (rows * P0 + kPlaneAlign - 1) / kPlaneAlign *
+                            kPlaneAlign;
+  // 16-bit planes from int32 plane 1 on: (nplanes - 1) planes of room
+  if ((long long)S.R1 * plane16 > (long long)(S.nplanes - 1) * S.plane * 2)
+    return false;
+  f.a.pitch = P0;
+  f.a.t0 = T0;
+  f.a.plane = plane16;
+  for (size_t k = 1; k < P.groups.size(); k++) {
+    GroupPlan &gp = P.groups[k];
+    GroupArgs t = gp.a;
+    if (gp.kernel < 0 || !t.in16 || t.inner % T0) return false;
+    t.inner = t.inner / T0 * P0;
+    t.pitch = P0;
+    t.t0 = T0;
+    t.plane = plane16;
+    t.pack = 1;
+    GroupPlan base = gp;
+    base.a = t;
+    bool done = false;
+    for (int lanes : {32, 16})
+      for (int stages : {3, 2}) {
+        if (done) break;
+        GroupPlan v = tma_variant(base, lanes, stages, 256);
+        if (tma_group_ok(v.a, t.rq[0], S.R1, lanes, stages)) {
+          gp = v;
+          done = true;
+        }
+      }
+    if (!done) return false;
+  }
+  return true;
+}
+
 Plan build_group_plan(int src, int dst, Knobs kn) {
   Plan P;
   PlanPtrs ptr{S.layers, S.plane, S.cnt, S.d_code, S.codeM, nullptr};
@@ -349,6 +399,11 @@ Plan build_group_plan(int src, int dst, Knobs kn) {
   Geometry g = S.g;
   g.mu = g_mu;
   P.groups = plan_groups(g, S.R1, ptr, src, dst, kn);
+  if (kn.pad) {
+    // a padded plan or none (the tuner then skips this knob setting)
+    if (!kn.half || !pad_plan(P)) P.groups.clear();
+    return P;
+  }
   // CC_TMA=1: every group the streamed form serves takes it (64-word rows
   // first, three stages where they fit); the autotuner otherwise times it
   // beside the other forms
@@ -427,8 +482,17 @@ Plan make_plan(int init_mode, int out_mode, Knobs kn) {
 
 Plan &plan_for(int init_mode, int out_mode) {
   if (!S.plan_ok[init_mode][out_mode]) {
-    S.plans[init_mode][out_mode] = make_plan(init_mode, out_mode,
-                                             default_knobs());
+    Plan P;
+    // CC_TMA=1 also asks for the padded plan where a cell has one
+    const char *te = getenv("CC_TMA");
+    if (te && atoi(te) == 1) {
+      Knobs kn = default_knobs();
+      kn.pad = 1;
+      P = make_plan(init_mode, out_mode, kn);
+    }
+    if (P.groups.empty() && !P.window)
+      P = make_plan(init_mode, out_mode, default_knobs());
+    S.plans[init_mode][out_mode] = P;
     S.plan_ok[init_mode][out_mode] = true;
   }
   return S.plans[init_mode][out_mode];
@@ -607,7 +671,7 @@ std::vector<long long> grouping_key(const Plan &P) {
   std::vector<long long> k;
   for (const auto &g : P.groups)
     k.push_back(((long long)g.a.k << 32) | (g.a.W << 8) | (g.a.pipe << 1) |
-                g.a.pair_axis);
+                g.a.pair_axis | ((g.a.pitch ? 1LL : 0LL) << 24));
   return k;
 }
 
@@ -630,7 +694,12 @@ int autotune(int init_mode, int out_mode) {
                                 {64 << 10, 1}, {200 << 10, 1},
                                 {100 << 10, 2}, {100 << 10, 3},
                                 {200 << 10, 3}, {160 << 10, 2},
-                                {200 << 10, 2}};
+                                {200 << 10, 2},
+                                // padded plans (ternary cells)
+                                {64 << 10, 1, 0, 1, 1},
+                                {100 << 10, 1, 0, 1, 1},
+                                {160 << 10, 1, 0, 1, 1},
+                                {200 << 10, 1, 0, 1, 1}};
   EventPair ev;
   int rc = ev.create();
   if (rc) return rc;

@@ -409,10 +409,16 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
           p += gstep;
         }
       } else if (dst == kIoLayers && g.out16) {
+        // a first group (inner 1) of a padded plan: the slab's row starts
+        // at a pitch of g.pitch words
+        const long long xo = g.pitch
+            ? (o0 + ob) * g.pitch + (long long)(mlo + S * ne * mhi) *
+                  g.inner + i0 + wi
+            : xb;
 #pragma unroll
         for (int d = 0; d < R1; d++) {
           if (d >= g.lout) break;
-          uint16_t *p = g.layers16 + d * g.plane + xb;
+          uint16_t *p = g.layers16 + d * g.plane + xo;
 #pragma unroll
           for (int e = 0; e < QB; e++) {
             if (!FULL && e >= ne) break;

@@ -190,7 +190,7 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
         for (int e = 0; e < QB; e++)
           __stcs(reinterpret_cast<unsigned *>(q + e * step), v[d][e]);
       }
-    } else {
+    } else if (OUT == 1 || OUT == 2) {
 #pragma unroll
       for (int e = 0; e < QB; e++) {
         uint32_t s = 0;
@@ -201,6 +201,28 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
                  make_int2((int)(s & 0xFFFFu), (int)(s >> 16)));
         else
           *reinterpret_cast<unsigned *>(a.cnt + x0 + e * step) = s;
+      }
+    } else {
+      // OUT 3 (map) / 4 (cnt) of a padded plan: the pair's words j', j'+1
+      // of the padded inner go back to the canonical index, padding dropped
+      const long long jp = i0 + 2 * l;
+      const long long r = jp / a.pitch, i = jp - r * a.pitch;
+      const bool ok0 = i < a.t0, ok1 = i + 1 < a.t0;
+      const long long xc = (o * MID + mb) * a.inner_c + r * a.t0 + i;
+      const long long stepc = (long long)QA * a.inner_c;
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int d = 0; d < R1; d++) s += v[d][e];
+        const long long x = xc + e * stepc;
+        if (OUT == 3) {
+          if (ok0) __stcs(a.map + x, (int)(s & 0xFFFFu));
+          if (ok1) __stcs(a.map + x + 1, (int)(s >> 16));
+        } else {
+          if (ok0) a.cnt[x] = (uint16_t)(s & 0xFFFFu);
+          if (ok1) a.cnt[x + 1] = (uint16_t)(s >> 16);
+        }
       }
     }
   }
@@ -549,11 +571,22 @@ struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; };
   {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0>},                              \
   {Q, K, R1, L, 1, tma_group<Q, K, R1, L, 1>},                              \
   {Q, K, R1, L, 2, tma_group<Q, K, R1, L, 2>}
+// ternary groups run only in the padded layout: OUT 0 (layers), 3 (map)
+// and 4 (cnt), the last two back to the canonical index
+#define TE3(Q, K, R1, L)                                                    \
+  {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0>},                              \
+  {Q, K, R1, L, 3, tma_group<Q, K, R1, L, 3>},                              \
+  {Q, K, R1, L, 4, tma_group<Q, K, R1, L, 4>}
 const TmaEntry kTma[] = {
     TE(2, 5, 4, 16), TE(2, 6, 4, 16), TE(2, 7, 4, 16), TE(2, 8, 4, 16),
     TE(2, 5, 4, 32), TE(2, 6, 4, 32), TE(2, 7, 4, 32),
+    TE3(3, 3, 4, 16), TE3(3, 4, 4, 16), TE3(3, 5, 4, 16),
+    TE3(3, 3, 4, 32), TE3(3, 4, 4, 32),
+    TE3(3, 3, 5, 16), TE3(3, 4, 5, 16), TE3(3, 5, 5, 16),
+    TE3(3, 3, 5, 32), TE3(3, 4, 5, 32),
 };
 #undef TE
+#undef TE3
 
 typedef void (*FirstFn)(const TmaArgs);
 // src 0: the cnt predicate (tma_first), 1: the sorted code (code_first)
@@ -570,6 +603,13 @@ const FirstEntry *find_first(int src, int kk, int r1, int out) {
   for (const auto &e : kFirst)
     if (e.src == src && e.kk == kk && e.r1 == r1 && e.out == out) return &e;
   return nullptr;
+}
+
+// the kernel's OUT: 0 layers, 1 map, 2 cnt; 3 map and 4 cnt of a padded
+// plan (canonical stores)
+int out_code(const GroupArgs &a) {
+  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  return (a.pitch && out) ? out + 2 : out;
 }
 
 const TmaEntry *find_tma(int q, int k, int r1, int lanes, int out) {
@@ -639,7 +679,7 @@ size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages) {
 // layers, lanes) and its stages within 227 KB of shared memory.
 bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
   if (stages < 2 || stages > kTmaMaxStages || !encode_fn()) return false;
-  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  const int out = out_code(a);
   if (!find_tma(q, a.k, r1, lanes, out)) return false;
   if (a.prob != kHamming || !a.pack || !a.in16 || a.pair_axis ||
       a.src != kSrcLayers || a.R + 1 != r1)
@@ -741,7 +781,7 @@ int first_opt_in(const FirstEntry *e) {
 
 const TmaEntry *entry_of(const GroupPlan &p) {
   const GroupArgs &a = p.a;
-  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  const int out = out_code(a);
   return find_tma(a.rq[0] ? a.rq[0] : a.qax[0], a.k, a.R + 1, a.W / 2, out);
 }
 
@@ -882,6 +922,9 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   t.lout = a.lout;
   t.stages = a.stages;
   t.fault = fault;
+  t.pitch = a.pitch;
+  t.t0 = a.t0;
+  t.inner_c = a.pitch ? a.inner / a.pitch * a.t0 : a.inner;
   const size_t smem = tma_smem_bytes(q, a.k, a.R + 1, lanes, a.stages);
   int grid = p.grid;
   if (grid < 1) {

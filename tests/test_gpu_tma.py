@@ -42,3 +42,33 @@ def test_streamed_groups_match_the_oracle(monkeypatch, axes, R, mu):
             for im, om in ((0, 2), (1, 1), (2, 1)):
                 used += int(np.count_nonzero(b.plan_forms(im, om) & TMA))
         assert used > 0, "no launch took the streamed form"
+
+
+@pytest.mark.parametrize("axes,R,mu", [
+    ([3] * 11, 4, 1), ([3] * 13, 4, 1), ([3] * 12, 3, 2), ([3] * 14, 3, 1)])
+def test_padded_ternary_plan_matches_the_oracle(monkeypatch, axes, R, mu):
+    """Ternary cells: the first group writes its 16-bit planes with rows
+    padded to a multiple of 64 words, so the later groups stream them in
+    packed pairs and the last one stores the canonical layout."""
+    monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_TUNE", "0")
+    size = int(np.prod(axes))
+    rng = np.random.default_rng(size % 997 + R)
+    o = OracleBackend(axes, R, mu=mu)
+    with GpuBackend(axes, R, mu=mu) as b:
+        used = 0
+        for step in range(2):
+            code = np.sort(rng.choice(size, size=size // (90 + 60 * step),
+                                      replace=False))
+            b.recount(code)
+            o.recount(code)
+            assert np.array_equal(b.read_cnt(), o.read_cnt()), step
+            b.gain_map()
+            o.gain_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            b.loss_map()
+            o.loss_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            for im, om in ((0, 2), (1, 1), (2, 1)):
+                used += int(np.count_nonzero(b.plan_forms(im, om) & TMA))
+        assert used > 0, "no launch took the streamed form"
