@@ -295,6 +295,17 @@ int launch_scatter(int32_t *A, const long long *idx, long long M,
                    cudaStream_t s);
 
 int sm_count();
+// DCT_BLOCKS, read at each cell's init as coldcore's plugin reads it: when
+// set, the grid of every persistent transform launch (at least 256 CTAs, at
+// most one per tile; every such kernel strides its tiles by the grid); 0
+// leaves the grids to the occupancy rule.
+extern int g_dct_blocks;
+inline int grid_knob(int grid, long long ntiles) {
+  if (g_dct_blocks <= 0) return grid;
+  long long g = g_dct_blocks;
+  if (g > ntiles) g = ntiles;
+  return (int)(g < 1 ? 1 : g);
+}
 
 }  // namespace cc
 

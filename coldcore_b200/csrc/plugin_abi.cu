@@ -30,6 +30,8 @@ int sm_count() {
   return n;
 }
 
+int g_dct_blocks = 0;
+
 }  // namespace cc
 
 using namespace cc;
@@ -817,6 +819,9 @@ int init_common(int problem, int n, const int *ax, int R, long long len,
   free_all();
   int rc = ensure_stream();
   if (rc) return rc;
+  // coldcore's launch-size knob: 256 CTAs at least (dct_hc.cu:274-276)
+  const char *bl = getenv("DCT_BLOCKS");
+  g_dct_blocks = bl ? std::max(256, atoi(bl)) : 0;
   S.g.prob = problem; S.g.n = n; S.g.R = R; S.g.mu = g_mu;
   S.g.space = space;
   S.g.pw[0] = 1;

@@ -1120,7 +1120,7 @@ int launch_group(const GroupPlan &p, cudaStream_t s) {
   GroupFn fn = group_fn(p);
   const int rc = ensure_group_smem(p);
   if (rc) return rc;
-  fn<<<p.grid, p.threads, p.smem, s>>>(p.a);
+  fn<<<grid_knob(p.grid, p.a.ntiles), p.threads, p.smem, s>>>(p.a);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     fprintf(stderr, "coldcore_b200: group launch (kernel %d pipe %d grid %d "

@@ -870,6 +870,7 @@ int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
     if (gr > a.ntiles) gr = a.ntiles;
     grid = (int)(gr < 1 ? 1 : gr);
   }
+  grid = grid_knob(grid, a.ntiles);
   f->fn<<<grid, p.threads, smem, s>>>(t);
   CC_CK(cudaGetLastError());
   return 0;
@@ -933,6 +934,7 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
     if (gr > a.ntiles) gr = a.ntiles;
     grid = (int)(gr < 1 ? 1 : gr);
   }
+  grid = grid_knob(grid, a.ntiles);
   e->fn<<<grid, p.threads, smem, s>>>(map, t);
   CC_CK(cudaGetLastError());
   return 0;

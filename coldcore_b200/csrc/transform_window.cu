@@ -50,10 +50,12 @@ __global__ void __launch_bounds__(256) window_axis(const WindowArgs w) {
 }
 
 int launch_window(const WindowArgs &w, cudaStream_t s) {
-  long long nb = (w.space + 255) / 256;
+  const long long nblk = (w.space + 255) / 256;
+  long long nb = nblk;
   const long long cap = (long long)sm_count() * 16;
   if (nb > cap) nb = cap;
   if (nb < 1) nb = 1;
+  nb = grid_knob((int)nb, nblk);
   const bool s16 = w.src16 != nullptr, d16 = w.dst16 != nullptr;
   const bool i32 = w.space < (1LL << 31);
 #define WL(G, A, B)                                                         \
