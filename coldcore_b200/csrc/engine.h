@@ -80,7 +80,8 @@ struct GroupArgs {
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
   // streamed form (transform_tma.cu): tensor loads into `stages` shared
   // memory stages, W = 2 x lanes inner words a tile (tma 1); the first
-  // group staged from cnt by bulk copies (tma 2)
+  // group staged from cnt by bulk copies (tma 2); a ternary first group
+  // over row pairs packed in 32-bit lanes (tma 3, Bo = 2)
   int tma;
   int stages;
   // padded layout of the 16-bit planes (ternary cells): every run of t0
@@ -112,6 +113,8 @@ struct TmaArgs {
   // padded planes (GroupArgs::pitch): the canonical inner stride, the
   // pitch and the valid words of each padded run
   long long inner_c, pitch, t0;
+  // ternary first group (tern_first): the rows of the cell
+  long long rows;
 };
 
 struct GroupPlan {
@@ -173,6 +176,9 @@ GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages, int threads);
 size_t tma_first_smem_bytes(int kk, int r1, int stages);
 bool tma_first_ok(const GroupArgs &a, int r1, int stages);
 GroupPlan tma_first_variant(const GroupPlan &p, int stages, int threads);
+// the first group of a ternary Hamming cell over row pairs, a.tma == 3
+bool tern_first_ok(const GroupArgs &a, int r1);
+GroupPlan tern_first_variant(const GroupPlan &p, int threads);
 int launch_tma_group(const GroupPlan &p, cudaStream_t s);
 int tma_prepare(const GroupPlan &p);
 int tma_blocks_per_sm(const GroupPlan &p);

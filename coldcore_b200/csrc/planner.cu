@@ -236,6 +236,15 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   // group qualifies: 32 or 64-word rows, 2 or 3 stages, 256 or 512 threads
   const char *tma_env = getenv("CC_TMA");
   const bool tma_off = tma_env && atoi(tma_env) == 0;
+  // a ternary first group over packed row pairs (its tiles are the pairs
+  // the group already has, so a recount's code bounds stay valid)
+  for (int th : {256, 512}) {
+    if (tma_off || (p.a.tma == 3 && p.threads == th)) continue;
+    GroupPlan v = tern_first_variant(p, th);
+    if (!tern_first_ok(v.a, R1)) continue;
+    v.grid = occupancy_grid(v);
+    out.push_back(v);
+  }
   for (int lanes : {16, 32})
     for (int stages : {2, 3})
       if (!tma_off && tma_group_ok(tma_variant(p, lanes, stages, 256).a, q, R1, lanes,
@@ -247,7 +256,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
         }
   // a padded plan's later groups run streamed only (the register kernels
   // address the canonical layout)
-  if (p.a.pitch && p.a.tma) return out;
+  if (p.a.pitch && p.a.tma == 1) return out;
   for (int stages : {0, 2, 3})
     if (!tma_off && tma_first_ok(p.a, R1, stages))
       for (int th : {128, 256, 512}) {
@@ -260,6 +269,8 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {
     GroupPlan t = p;
     t.kernel = kids[i];
+    t.a.tma = 0;
+    t.a.stages = 0;
     t.a.pipe = pipe;
     if (W != p.a.W) {
       t.a.W = W;
@@ -283,7 +294,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
       v.threads = th;
       v.grid = occupancy_grid(v);
       if (v.kernel == p.kernel && v.threads == p.threads &&
-          v.a.pipe == p.a.pipe && v.a.W == p.a.W)
+          v.a.pipe == p.a.pipe && v.a.W == p.a.W && v.a.tma == p.a.tma)
         continue;
       out.push_back(v);
     }

@@ -417,6 +417,13 @@ bool pad_plan(Plan &P, const Geometry &g, const PlanPtrs &ptr, int dst) {
   f.a.pitch = P0;
   f.a.t0 = T0;
   f.a.plane = plane16;
+  // row pairs as the first group's tiles: the packed ternary form runs on
+  // them (the register kernels take them as Bo = 2)
+  GroupPlan fv = f;
+  fv.a.Bo = 2;
+  fv.a.ntiles = (fv.a.outer + 1) / 2;
+  if (f.a.Bo == 1 && f.a.nchunk == 1 && tern_first_ok(fv.a, S.R1))
+    f = tern_first_variant(fv, 256);
   P.groups.resize(1);
   P.groups.insert(P.groups.end(), later.begin(), later.end());
   return true;

@@ -562,6 +562,140 @@ code_first(const TmaArgs a) {
   }
 }
 
+// ------------------------------------------------------------ ternary first
+// The first group of a ternary Hamming cell: axes 0..KK-1, T0 = 3^KK words a
+// row at inner stride 1.  Ternary rows are odd, so no word pair lies inside
+// a row; instead a tile is TWO consecutive rows, and the 32-bit lane of row
+// position m carries row 2t in its low half and row 2t+1 in its high half.
+// The q = 3 recurrence is adds only (A_d[a] += the other two entries of
+// layer d-1), so every partial sum is a layer value, below 2^16 by the
+// planner's 16-bit bound, and one add serves both rows.  Rounds of two axes
+// (9-word register blocks) run on one shared buffer of R1 x T0 lanes: the
+// first round takes the two highest axes and reads the cnt predicate (or
+// the code counts) with consecutive threads on consecutive words; the last
+// takes the two below them and stores both rows' u16 layers at the plan's
+// row pitch (the padded layout, or T0); the low axes run in between.
+// No waits: plain loads, one CTA buffer, a barrier between rounds.
+template <int KK, int I>
+struct TernRound {
+  static_assert(KK >= 5 && KK <= 8, "ternary first group of 5..8 axes");
+  static constexpr int N = (KK + 1) / 2;
+  static constexpr int A = I == 0 ? KK - 2 : I == N - 1 ? KK - 4 : 2 * (I - 1);
+  static constexpr int B = (I == 0 || I == N - 1) ? 2
+                           : ((KK - 4 - A) < 2 ? (KK - 4 - A) : 2);
+};
+
+template <int KK, int R1, int SRC, int I>
+__device__ __forceinline__ void tern_round(uint32_t *work, const TmaArgs &a,
+                                           long long r0, bool two,
+                                           uint32_t plo, uint32_t pspan) {
+  using TR = TernRound<KK, I>;
+  constexpr int A = TR::A, B = TR::B;
+  constexpr int T0 = P<3, KK>::v;
+  constexpr int WS = (T0 + 31) / 32 * 32;
+  constexpr int QA = P<3, A>::v, QB = P<3, B>::v;
+  constexpr bool FIRST = I == 0, LAST = I == TR::N - 1;
+  constexpr int NB = T0 / QB;
+  for (int blk = threadIdx.x; blk < NB; blk += blockDim.x) {
+    const int pb = blk % QA + (blk / QA) * (QA * QB);
+    uint32_t v[R1][QB];
+    if (FIRST) {
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        const int m = pb + e * QA;
+        if (SRC == 0) {                       // the cnt predicate, two rows
+          const uint16_t *c = a.cnt_in + r0 * T0 + m;
+          const uint32_t lo = ((uint32_t)__ldcs(c) - plo) <= pspan;
+          const uint32_t hi =
+              two ? (((uint32_t)__ldcs(c + T0) - plo) <= pspan) : 0u;
+          v[0][e] = lo | (hi << 16);
+        } else {                              // code counts, staged
+          v[0][e] = work[m];
+        }
+#pragma unroll
+        for (int d = 1; d < R1; d++) v[d][e] = 0;
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < R1; d++)
+#pragma unroll
+        for (int e = 0; e < QB; e++) v[d][e] = work[d * WS + pb + e * QA];
+    }
+    Axes<3, R1, B, 0>::run(v);
+    if (!LAST) {
+#pragma unroll
+      for (int d = 0; d < R1; d++)
+#pragma unroll
+        for (int e = 0; e < QB; e++) work[d * WS + pb + e * QA] = v[d][e];
+      continue;
+    }
+    const long long x0 = r0 * a.pitch + pb;
+#pragma unroll
+    for (int d = 0; d < R1; d++) {
+      if (d >= a.lout) break;
+      uint16_t *q = a.layers16 + d * a.plane + x0;
+#pragma unroll
+      for (int e = 0; e < QB; e++) {
+        __stcs(q + e * QA, (uint16_t)(v[d][e] & 0xFFFFu));
+        if (two) __stcs(q + a.pitch + e * QA, (uint16_t)(v[d][e] >> 16));
+      }
+    }
+  }
+}
+
+template <int KK, int R1, int SRC, int I, int N>
+struct TernRounds {
+  static __device__ __forceinline__ void run(uint32_t *work,
+                                             const TmaArgs &a, long long r0,
+                                             bool two, uint32_t plo,
+                                             uint32_t pspan) {
+    tern_round<KK, R1, SRC, I>(work, a, r0, two, plo, pspan);
+    __syncthreads();
+    TernRounds<KK, R1, SRC, I + 1, N>::run(work, a, r0, two, plo, pspan);
+  }
+};
+template <int KK, int R1, int SRC, int N>
+struct TernRounds<KK, R1, SRC, N, N> {
+  static __device__ __forceinline__ void run(uint32_t *, const TmaArgs &,
+                                             long long, bool, uint32_t,
+                                             uint32_t) {}
+};
+
+// SRC 0: the cnt predicate (gain, loss); 1: the sorted code (a recount),
+// the tile's slice [bounds[t], bounds[t+1]) counted into layer 0 first
+template <int KK, int R1, int SRC>
+__global__ void __launch_bounds__(512)
+tern_first(const TmaArgs a) {
+  extern __shared__ __align__(16) uint8_t dyn[];
+  constexpr int T0 = P<3, KK>::v;
+  constexpr int NR = TernRound<KK, 0>::N;
+  uint32_t *work = reinterpret_cast<uint32_t *>(dyn);
+  const uint32_t plo = a.pmode == kPredDef ? 0u
+                       : a.pmode == kPredCrit ? 1u : (uint32_t)a.ptarget;
+  const uint32_t phi = a.pmode == kPredDef ? (uint32_t)(a.mu - 1)
+                       : a.pmode == kPredCrit ? (uint32_t)a.mu
+                       : (uint32_t)a.ptarget;
+  const uint32_t pspan = phi - plo;
+  for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const long long r0 = 2 * t;
+    const bool two = r0 + 1 < a.rows;
+    if (SRC == 1) {
+      for (int i = threadIdx.x; i < T0; i += blockDim.x) work[i] = 0;
+      __syncthreads();
+      const long long lo = a.code_bounds[t], hi = a.code_bounds[t + 1];
+      const long long x0 = r0 * T0;
+      for (long long c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+        const long long w = a.code[c] - x0;
+        if (w < 0 || w >= 2 * T0) continue;   // outside this tile's rows
+        const int h = w >= T0 ? 1 : 0;
+        atomicAdd(&work[(int)w - h * T0], 1u << (16 * h));
+      }
+      __syncthreads();
+    }
+    TernRounds<KK, R1, SRC, 0, NR>::run(work, a, r0, two, plo, pspan);
+  }
+}
+
 // ------------------------------------------------------------ dispatch
 typedef void (*TmaFn)(const CUtensorMap, const TmaArgs);
 
@@ -598,6 +732,19 @@ struct FirstEntry { int src, kk, r1, out; FirstFn fn; };
 const FirstEntry kFirst[] = {FE(9, 4), FE(10, 4), FE(11, 4), FE(12, 4),
                              FE(13, 4)};
 #undef FE
+
+// the ternary first group: src 0 cnt, 1 code; KK axes; R1 layers
+struct TernEntry { int src, kk, r1; FirstFn fn; };
+#define TF(KK, R1) {0, KK, R1, tern_first<KK, R1, 0>},                     \
+                   {1, KK, R1, tern_first<KK, R1, 1>}
+const TernEntry kTern[] = {TF(6, 4), TF(7, 4), TF(6, 5), TF(7, 5)};
+#undef TF
+
+const TernEntry *find_tern(int src, int kk, int r1) {
+  for (const auto &e : kTern)
+    if (e.src == src && e.kk == kk && e.r1 == r1) return &e;
+  return nullptr;
+}
 
 const FirstEntry *find_first(int src, int kk, int r1, int out) {
   for (const auto &e : kFirst)
@@ -749,6 +896,43 @@ bool tma_first_ok(const GroupArgs &a, int r1, int stages) {
   return tma_first_smem_bytes(a.k, r1, stages) <= kTmaSmemMax;
 }
 
+size_t tern_first_smem_bytes(int kk, int r1) {
+  long long t0 = 1;
+  for (int i = 0; i < kk; i++) t0 *= 3;
+  return (size_t)r1 * ((t0 + 31) / 32 * 32) * 4;
+}
+
+// The ternary first groups tern_first serves: Hamming, every axis q = 3,
+// inner stride 1, row pairs (Bo = 2) as the tiles, 16-bit layers out (at
+// the plan's pitch, or T0), the cnt or the code as the source.
+bool tern_first_ok(const GroupArgs &a, int r1) {
+  const int src = a.src == kSrcCnt ? 0 : a.src == kSrcCode ? 1 : -1;
+  if (src < 0 || a.prob != kHamming || a.dst != kDstLayers || !a.out16 ||
+      a.inner != 1 || a.W != 1 || a.Bo != 2 || a.pair_axis || a.pack ||
+      a.R + 1 != r1 || a.lin != 1 || a.k < 1)
+    return false;
+  long long t0 = 1;
+  for (int i = 0; i < a.k; i++) {
+    if (a.qax[i] != 3) return false;
+    t0 *= 3;
+  }
+  if (t0 != a.mid || !find_tern(src, a.k, r1)) return false;
+  if (a.pitch && (a.pitch < t0 || a.t0 != t0)) return false;
+  if (a.outer < 1 || a.ntiles != (a.outer + 1) / 2) return false;
+  return tern_first_smem_bytes(a.k, r1) <= kTmaSmemMax;
+}
+
+GroupPlan tern_first_variant(const GroupPlan &p, int threads) {
+  GroupPlan v = p;
+  v.a.tma = 3;
+  v.a.stages = 0;
+  v.a.pipe = 0;
+  v.threads = threads;
+  v.smem = tern_first_smem_bytes(v.a.k, v.a.R + 1);
+  v.grid = 0;
+  return v;
+}
+
 int tma_fault_pending() {
   return g_fault_host && *(volatile int *)g_fault_host ? 1 : 0;
 }
@@ -770,6 +954,24 @@ int first_opt_in(const FirstEntry *e) {
   static bool done[sizeof(kFirst) / sizeof(kFirst[0])];
   std::lock_guard<std::mutex> g(mu);
   const size_t idx = (size_t)(e - kFirst);
+  if (!done[idx]) {
+    CC_CK(cudaFuncSetAttribute((const void *)e->fn,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTmaSmemMax));
+    done[idx] = true;
+  }
+  return 0;
+}
+
+const TernEntry *tern_of(const GroupPlan &p) {
+  return find_tern(p.a.src == kSrcCode ? 1 : 0, p.a.k, p.a.R + 1);
+}
+
+int tern_opt_in(const TernEntry *e) {
+  static std::mutex mu;
+  static bool done[sizeof(kTern) / sizeof(kTern[0])];
+  std::lock_guard<std::mutex> g(mu);
+  const size_t idx = (size_t)(e - kTern);
   if (!done[idx]) {
     CC_CK(cudaFuncSetAttribute((const void *)e->fn,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -803,6 +1005,10 @@ int opt_in(const TmaEntry *e) {
 }  // namespace
 
 int tma_prepare(const GroupPlan &p) {
+  if (p.a.tma == 3) {
+    const TernEntry *f = tern_of(p);
+    return f ? tern_opt_in(f) : -9;
+  }
   if (p.a.tma == 2) {
     const FirstEntry *f = first_of(p);
     return f ? first_opt_in(f) : -9;
@@ -814,7 +1020,11 @@ int tma_prepare(const GroupPlan &p) {
 
 int tma_blocks_per_sm(const GroupPlan &p) {
   const void *fn = nullptr;
-  if (p.a.tma == 2) {
+  if (p.a.tma == 3) {
+    const TernEntry *f = tern_of(p);
+    if (!f || tern_opt_in(f)) return 0;
+    fn = (const void *)f->fn;
+  } else if (p.a.tma == 2) {
     const FirstEntry *f = first_of(p);
     if (!f || first_opt_in(f)) return 0;
     fn = (const void *)f->fn;
@@ -830,6 +1040,44 @@ int tma_blocks_per_sm(const GroupPlan &p) {
     return 0;
   }
   return n;
+}
+
+int launch_tern_first(const GroupPlan &p, cudaStream_t s) {
+  const GroupArgs &a = p.a;
+  const TernEntry *f = tern_of(p);
+  const bool from_code = a.src == kSrcCode;
+  if (!f || !tern_first_ok(a, a.R + 1) ||
+      (from_code && (!a.code_bounds || !a.code)))
+    return -9;
+  int rc = tern_opt_in(f);
+  if (rc) return rc;
+  TmaArgs t{};
+  t.layers16 = a.layers16;
+  t.plane = a.plane;
+  t.cnt_in = a.cnt;
+  t.pmode = a.pmode;
+  t.ptarget = a.ptarget;
+  t.mu = a.mu;
+  t.ntiles = a.ntiles;
+  t.lin = 1;
+  t.lout = a.lout;
+  t.code = a.code;
+  t.code_bounds = a.code_bounds;
+  t.pitch = a.pitch ? a.pitch : a.mid;
+  t.t0 = a.mid;
+  t.rows = a.outer;
+  const size_t smem = tern_first_smem_bytes(a.k, a.R + 1);
+  int grid = p.grid;
+  if (grid < 1) {
+    const int per_sm = tma_blocks_per_sm(p);
+    long long gr = (long long)sm_count() * (per_sm < 1 ? 1 : per_sm);
+    if (gr > a.ntiles) gr = a.ntiles;
+    grid = (int)(gr < 1 ? 1 : gr);
+  }
+  grid = grid_knob(grid, a.ntiles);
+  f->fn<<<grid, p.threads, smem, s>>>(t);
+  CC_CK(cudaGetLastError());
+  return 0;
 }
 
 int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
@@ -877,6 +1125,7 @@ int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
 }
 
 int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
+  if (p.a.tma == 3) return launch_tern_first(p, s);
   if (p.a.tma == 2) return launch_tma_first(p, s);
   const GroupArgs &a = p.a;
   const int q = a.rq[0] ? a.rq[0] : a.qax[0];
