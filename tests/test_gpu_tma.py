@@ -47,16 +47,16 @@ def test_streamed_groups_match_the_oracle(monkeypatch, axes, R, mu):
 @pytest.mark.parametrize("axes,R,mu", [
     ([3] * 11, 4, 1), ([3] * 13, 4, 1), ([3] * 12, 3, 2), ([3] * 14, 3, 1)])
 def test_padded_ternary_plan_matches_the_oracle(monkeypatch, axes, R, mu):
-    """Ternary cells: the first group writes its 16-bit planes with rows
-    padded to a multiple of 64 words, so the later groups stream them in
-    packed pairs and the last one stores the canonical layout."""
+    """Ternary cells: the first group (row pairs packed in 32-bit lanes)
+    writes its 16-bit planes with rows padded to a multiple of 64 words, so
+    the later groups stream them in packed pairs and the last one stores
+    the canonical layout.  Every launch of every transform is streamed."""
     monkeypatch.setenv("CC_TMA", "1")
     monkeypatch.setenv("CC_TUNE", "0")
     size = int(np.prod(axes))
     rng = np.random.default_rng(size % 997 + R)
     o = OracleBackend(axes, R, mu=mu)
     with GpuBackend(axes, R, mu=mu) as b:
-        used = 0
         for step in range(2):
             code = np.sort(rng.choice(size, size=size // (90 + 60 * step),
                                       replace=False))
@@ -70,5 +70,28 @@ def test_padded_ternary_plan_matches_the_oracle(monkeypatch, axes, R, mu):
             o.loss_map()
             assert np.array_equal(b.map_all(), o.map), step
             for im, om in ((0, 2), (1, 1), (2, 1)):
-                used += int(np.count_nonzero(b.plan_forms(im, om) & TMA))
-        assert used > 0, "no launch took the streamed form"
+                forms = b.plan_forms(im, om)
+                assert len(forms) >= 2 and (forms & TMA).all(), (im, forms)
+
+
+def test_padded_ternary_plan_counts_a_multiset(monkeypatch):
+    """A code with repeated words (the counts of the packed row pairs carry
+    multiplicities) and mu = 3 (deficit and critical predicates)."""
+    monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_TUNE", "0")
+    axes, R, mu = [3] * 12, 3, 3
+    size = 3 ** 12
+    rng = np.random.default_rng(12)
+    code = np.sort(rng.integers(0, size, size // 40))
+    o = OracleBackend(axes, R, mu=mu)
+    with GpuBackend(axes, R, mu=mu) as b:
+        b.recount(code)
+        o.recount(code)
+        assert np.array_equal(b.read_cnt(), o.read_cnt())
+        b.gain_map()
+        o.gain_map()
+        assert np.array_equal(b.map_all(), o.map)
+        b.loss_map()
+        o.loss_map()
+        assert np.array_equal(b.map_all(), o.map)
+        assert (b.plan_forms(0, 2) & TMA).all()
