@@ -412,6 +412,14 @@ def measure_batch_small(args):
                         "instances_per_s": round(len(cells) / dt, 1)}
     out["speedup"] = round(out["persistent"]["instances_per_s"]
                            / out["per_pass_launches"]["instances_per_s"], 2)
+    # the step's achieved DRAM-side rate: its algorithmic bytes (each
+    # launch's source read once, its destination written once) over the
+    # persistent step time
+    peak, peak_kind = peaks()
+    gbs = out["step_bytes"] / (out["persistent"]["ms_per_step"] * 1e-3) / 1e9
+    out["step_GBps"] = round(gbs, 1)
+    out["step_frac"] = round(gbs / peak, 4)
+    out["peak_kind"] = peak_kind
     if not args.no_cpu:
         from oracle.cport import campaign_rate     # the CPU baseline leg
         rate, wall, busy, workers = campaign_rate(cells)

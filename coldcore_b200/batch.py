@@ -220,10 +220,15 @@ class BatchEngine:
         return out
 
     def info(self):
-        buf = (_LL * 6)()
-        _check("batch_info", 0 if self._lib.dct_batch_info(self.h, buf, 6) == 6
+        """Plan facts of the built batch; ``step_bytes`` is one step's
+        algorithmic HBM bytes (every launch's source read once and its
+        destination written once, plus the deficit count and the two map
+        maxima), ``big_bytes`` those of the cells with their own launches."""
+        buf = (_LL * 8)()
+        _check("batch_info", 0 if self._lib.dct_batch_info(self.h, buf, 8) == 8
                else -1)
-        keys = ("cells", "passes", "items", "tile_kb", "grid", "tuned_us")
+        keys = ("cells", "passes", "items", "tile_kb", "grid", "tuned_us",
+                "step_bytes", "big_bytes")
         return {k: int(v) for k, v in zip(keys, buf)}
 
     def close(self):

@@ -237,6 +237,8 @@ int make_schedule(Batch *b) {
   b->need.clear();
   std::vector<std::vector<int>> by_level;
   size_t smem = 0;
+  const char *tma_env = getenv("CC_TMA");
+  const bool streams_off = tma_env && atoi(tma_env) == 0;
   for (size_t i = 0; i < b->cells.size(); i++) {
     Cell &c = b->cells[i];
     c.first_pass = (int)b->passes.size();
@@ -256,8 +258,21 @@ int make_schedule(Batch *b) {
         const int src = t == 0 ? kSrcCode : kSrcCnt;
         const int dst = t == 0 ? kDstCnt : kDstMap;
         c.fast[t] = plan_groups(c.g, c.R1, ptr, src, dst, kn);
+        // the streamed forms where they apply (CC_TMA=0 keeps the
+        // register kernels): a ternary cell's padded plan, else every
+        // group a streamed form serves
+        if (!streams_off && kn.half &&
+            !pad_plan(c.fast[t], c.g, ptr, dst, c.R1,
+                      (long long)(c.R1 - 1) * c.plane * 2))
+          stream_groups(c.fast[t], c.R1);
         for (auto &gp : c.fast[t]) {
           if (prepare_group(gp)) return -1;
+          if (gp.a.tma && gp.grid < 1) {
+            // sized here: the graph capture records launches only
+            const int per_sm = std::max(1, tma_blocks_per_sm(gp));
+            gp.grid = (int)std::max<long long>(1, std::min<long long>(
+                gp.a.ntiles, (long long)sm_count() * per_sm));
+          }
           gp.a.pmode = kPredEq;
           gp.a.ptarget = t == 1 ? 0 : 1;
           if (c.g.mu > 1) gp.a.pmode = t == 1 ? kPredDef : kPredCrit;
@@ -717,7 +732,34 @@ int dct_batch_info(long long h, long long *out, int cap) {
   out[3] = (long long)(b->tile_budget / 1024);
   out[4] = b->grid;
   out[5] = (long long)(b->tuned_ms * 1000.0f);
-  return 6;
+  if (cap < 8) return 6;
+  // the step's algorithmic HBM bytes (every launch's source read once and
+  // destination written once, the deficit count and the two maxima), and
+  // those of the big cells alone
+  long long all = 0, big = 0;
+  for (const Cell &c : b->cells) {
+    long long cb = 0;
+    if (c.big) {
+      for (int t = 0; t < 3; t++)
+        for (const auto &gp : c.fast[t]) {
+          GroupArgs a = gp.a;
+          a.ncode = (long long)c.code.size();
+          cb += group_bytes(a);
+        }
+    } else {
+      for (int p = c.first_pass; p < c.first_pass + c.npass; p++) {
+        GroupArgs a = b->passes[p];
+        a.ncode = (long long)c.code.size();
+        cb += group_bytes(a);
+      }
+    }
+    cb += c.g.space * (2 + 4 + 4);         // deficit count, gain / loss max
+    all += cb;
+    if (c.big) big += cb;
+  }
+  out[6] = all;
+  out[7] = big;
+  return 8;
 }
 
 // ------------------------------------------------------------ per cell

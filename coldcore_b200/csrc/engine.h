@@ -166,6 +166,14 @@ int group_kernel_variants(int prob, int q, int R1, int *kids, int *bms,
                           int cap);
 // the same group with every other register-blocked kernel and CTA width
 // (rounds, skew and grid recomputed; tiles unchanged), the plan itself first
+// the padded plan of a ternary cell (planner.cu), in place; false leaves
+// `groups` unchanged
+bool pad_plan(std::vector<GroupPlan> &groups, const Geometry &g,
+              const PlanPtrs &ptr, int dst, int R1, long long room16);
+// every group a streamed form serves takes it (planner.cu)
+void stream_groups(std::vector<GroupPlan> &groups, int R1);
+// algorithmic HBM bytes of one group launch (planner.cu)
+long long group_bytes(const GroupArgs &a);
 std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
                                       size_t smem_cap);
 // streamed form of a strided group (transform_tma.cu)

@@ -302,4 +302,134 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   return out;
 }
 
+// The padded plan of a cell whose first group has an odd word count T0
+// (ternary): the first group writes its 16-bit layers at a pitch of P0 =
+// round_up(T0, 64) words a row, so every later group's rows start on 128-
+// byte boundaries and run as streamed launches over packed pairs; the last
+// writes the map or cnt back at the canonical index.  The axes after the
+// first group are split evenly into groups of at most kPadMaxAxes (the
+// widest streamed ternary group), and the first group takes the packed
+// row-pair form where it applies.  false when the cell does not qualify or
+// the padded planes do not fit the room16 u16 words of the allocation.
+constexpr int kPadMaxAxes = 5;
+
+bool pad_plan(std::vector<GroupPlan> &groups, const Geometry &g,
+              const PlanPtrs &ptr, int dst, int R1, long long room16) {
+  if (groups.size() < 2 || g.prob != kHamming) return false;
+  GroupPlan &f = groups[0];
+  const GroupArgs &a0 = f.a;
+  if (f.kernel < 0 || a0.inner != 1 || a0.W != 1 || !a0.out16 || a0.pack ||
+      a0.pair_axis || (a0.mid & 1) == 0)
+    return false;
+  const int k0 = a0.k;
+  const int rem = g.n - k0;
+  if (rem < 1) return false;
+  for (int j = k0; j < g.n; j++)
+    if (g.ax[j] != g.ax[k0]) return false;
+  const long long T0 = a0.mid;
+  const long long P0 = (T0 + 63) / 64 * 64;
+  const long long rows = g.space / T0;
+  const long long plane16 = (rows * P0 + kPlaneAlign - 1) / kPlaneAlign *
+                            kPlaneAlign;
+  // room16: the u16 words from the start of the 16-bit planes on
+  if ((long long)R1 * plane16 > room16) return false;
+  std::vector<GroupPlan> later;
+  const int nch = (rem + kPadMaxAxes - 1) / kPadMaxAxes;
+  // one group per range: the budget only has to admit its K axes
+  const Knobs kn{(size_t)1 << 30, 0, 1, 0, 0};
+  long long reach = 0;
+  for (int i = 0; i < k0; i++) reach += axis_reach(g.prob, g.ax[i]);
+  int j = k0;
+  for (int c = 0; c < nch; c++) {
+    const int K = rem / nch + (c < rem % nch ? 1 : 0);
+    const bool last = c == nch - 1;
+    AxisRange r;
+    r.begin = j;
+    r.end = j + K;
+    r.reach0 = reach;
+    r.final = last;
+    std::vector<GroupPlan> gs = plan_groups(g, R1, ptr, kSrcLayers,
+                                            last ? dst : kDstLayers, kn, r);
+    if (gs.size() != 1 || gs[0].a.k != K || gs[0].kernel < 0) return false;
+    GroupArgs t = gs[0].a;
+    if (!t.in16 || t.inner % T0) return false;
+    t.inner = t.inner / T0 * P0;
+    t.pitch = P0;
+    t.t0 = T0;
+    t.plane = plane16;
+    t.pack = 1;
+    GroupPlan base = gs[0];
+    base.a = t;
+    bool done = false;
+    for (int lanes : {32, 16})
+      for (int stages : {3, 2}) {
+        if (done) break;
+        GroupPlan v = tma_variant(base, lanes, stages, 256);
+        if (tma_group_ok(v.a, t.rq[0], R1, lanes, stages)) {
+          later.push_back(v);
+          done = true;
+        }
+      }
+    if (!done) return false;
+    for (int i = j; i < j + K; i++) reach += axis_reach(g.prob, g.ax[i]);
+    j += K;
+  }
+  f.a.pitch = P0;
+  f.a.t0 = T0;
+  f.a.plane = plane16;
+  // row pairs as the first group's tiles: the packed ternary form runs on
+  // them (the register kernels take them as Bo = 2)
+  GroupPlan fv = f;
+  fv.a.Bo = 2;
+  fv.a.ntiles = (fv.a.outer + 1) / 2;
+  if (f.a.Bo == 1 && f.a.nchunk == 1 && tern_first_ok(fv.a, R1))
+    f = tern_first_variant(fv, 256);
+  groups.resize(1);
+  groups.insert(groups.end(), later.begin(), later.end());
+  return true;
+}
+
+// Every group that a streamed form serves takes it: the binary first group
+// staged from cnt or counted from the code (three stages, then two), a
+// strided group as tensor loads (64-word rows first, three stages where
+// they fit).
+void stream_groups(std::vector<GroupPlan> &groups, int R1) {
+  for (auto &p : groups) {
+    if (p.kernel < 0 || p.a.nrounds <= 0) continue;
+    bool done = false;
+    for (int stages : {3, 2, 0})
+      if (!done && tma_first_ok(p.a, R1, stages)) {
+        p = tma_first_variant(p, stages, 256);
+        done = true;
+      }
+    for (int lanes : {32, 16})
+      for (int stages : {3, 2}) {
+        if (done) break;
+        GroupPlan v = tma_variant(p, lanes, stages, 256);
+        if (tma_group_ok(v.a, p.a.rq[0], R1, lanes, stages)) {
+          p = v;
+          done = true;
+        }
+      }
+  }
+}
+
+// Algorithmic HBM bytes of one group launch: every word of the space read
+// once from its source (2-byte cnt, or lin layers of 2 or 4 bytes; a
+// code-sourced launch reads its 8-byte code words) and written once to its
+// destination (lout layers of 2 or 4 bytes, the 4-byte map or the 2-byte
+// cnt).  Pad words of a padded plan are not counted.
+long long group_bytes(const GroupArgs &a) {
+  const long long words = a.outer * a.mid * (a.pitch && a.t0
+                          ? a.inner / a.pitch * a.t0 : a.inner);
+  long long rd = 0, wr = 0;
+  if (a.src == kSrcCnt) rd = 2 * words;
+  else if (a.src == kSrcCode) rd = 8 * a.ncode;
+  else rd = (long long)a.lin * (a.in16 ? 2 : 4) * words;
+  if (a.dst == kDstLayers) wr = (long long)a.lout * (a.out16 ? 2 : 4) * words;
+  else if (a.dst == kDstMap) wr = 4 * words;
+  else wr = 2 * words;
+  return rd + wr;
+}
+
 }  // namespace cc

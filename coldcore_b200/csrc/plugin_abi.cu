@@ -343,92 +343,6 @@ bool half_planes_ok(int src, int dst) {
   return src == kSrcCode || S.len <= 65535;
 }
 
-// The padded plan of a cell whose first group has an odd word count T0
-// (ternary): the first group writes its 16-bit layers at a pitch of P0 =
-// round_up(T0, 64) words a row, so every later group's rows start on 128-
-// byte boundaries and run as streamed launches over packed pairs; the last
-// writes the map or cnt back at the canonical index.  The axes after the
-// first group are split evenly into groups of at most kPadMaxAxes (the
-// widest streamed ternary group).  false when the cell does not qualify or
-// the padded planes do not fit the allocation.
-constexpr int kPadMaxAxes = 5;
-
-bool pad_plan(Plan &P, const Geometry &g, const PlanPtrs &ptr, int dst) {
-  if (P.groups.size() < 2 || g.prob != kHamming) return false;
-  GroupPlan &f = P.groups[0];
-  const GroupArgs &a0 = f.a;
-  if (f.kernel < 0 || a0.inner != 1 || a0.W != 1 || !a0.out16 || a0.pack ||
-      a0.pair_axis || (a0.mid & 1) == 0)
-    return false;
-  const int k0 = a0.k;
-  const int rem = g.n - k0;
-  if (rem < 1) return false;
-  for (int j = k0; j < g.n; j++)
-    if (g.ax[j] != g.ax[k0]) return false;
-  const long long T0 = a0.mid;
-  const long long P0 = (T0 + 63) / 64 * 64;
-  const long long rows = g.space / T0;
-  const long long plane16 = (rows * P0 + kPlaneAlign - 1) / kPlaneAlign *
-                            kPlaneAlign;
-  // 16-bit planes from int32 plane 1 on: (nplanes - 1) planes of room
-  if ((long long)S.R1 * plane16 > (long long)(S.nplanes - 1) * S.plane * 2)
-    return false;
-  std::vector<GroupPlan> later;
-  const int nch = (rem + kPadMaxAxes - 1) / kPadMaxAxes;
-  // one group per range: the budget only has to admit its K axes
-  const Knobs kn{(size_t)1 << 30, 0, 1, 0, 0};
-  long long reach = 0;
-  for (int i = 0; i < k0; i++) reach += axis_reach(g.prob, g.ax[i]);
-  int j = k0;
-  for (int c = 0; c < nch; c++) {
-    const int K = rem / nch + (c < rem % nch ? 1 : 0);
-    const bool last = c == nch - 1;
-    AxisRange r;
-    r.begin = j;
-    r.end = j + K;
-    r.reach0 = reach;
-    r.final = last;
-    std::vector<GroupPlan> gs = plan_groups(g, S.R1, ptr, kSrcLayers,
-                                            last ? dst : kDstLayers, kn, r);
-    if (gs.size() != 1 || gs[0].a.k != K || gs[0].kernel < 0) return false;
-    GroupArgs t = gs[0].a;
-    if (!t.in16 || t.inner % T0) return false;
-    t.inner = t.inner / T0 * P0;
-    t.pitch = P0;
-    t.t0 = T0;
-    t.plane = plane16;
-    t.pack = 1;
-    GroupPlan base = gs[0];
-    base.a = t;
-    bool done = false;
-    for (int lanes : {32, 16})
-      for (int stages : {3, 2}) {
-        if (done) break;
-        GroupPlan v = tma_variant(base, lanes, stages, 256);
-        if (tma_group_ok(v.a, t.rq[0], S.R1, lanes, stages)) {
-          later.push_back(v);
-          done = true;
-        }
-      }
-    if (!done) return false;
-    for (int i = j; i < j + K; i++) reach += axis_reach(g.prob, g.ax[i]);
-    j += K;
-  }
-  f.a.pitch = P0;
-  f.a.t0 = T0;
-  f.a.plane = plane16;
-  // row pairs as the first group's tiles: the packed ternary form runs on
-  // them (the register kernels take them as Bo = 2)
-  GroupPlan fv = f;
-  fv.a.Bo = 2;
-  fv.a.ntiles = (fv.a.outer + 1) / 2;
-  if (f.a.Bo == 1 && f.a.nchunk == 1 && tern_first_ok(fv.a, S.R1))
-    f = tern_first_variant(fv, 256);
-  P.groups.resize(1);
-  P.groups.insert(P.groups.end(), later.begin(), later.end());
-  return true;
-}
-
 Plan build_group_plan(int src, int dst, Knobs kn) {
   Plan P;
   PlanPtrs ptr{S.layers, S.plane, S.cnt, S.d_code, S.codeM, nullptr};
@@ -439,33 +353,16 @@ Plan build_group_plan(int src, int dst, Knobs kn) {
   P.groups = plan_groups(g, S.R1, ptr, src, dst, kn);
   if (kn.pad) {
     // a padded plan or none (the tuner then skips this knob setting)
-    if (!kn.half || !pad_plan(P, g, ptr, dst)) P.groups.clear();
+    if (!kn.half || !pad_plan(P.groups, g, ptr, dst, S.R1,
+                              (long long)(S.nplanes - 1) * S.plane * 2))
+      P.groups.clear();
     return P;
   }
   // CC_TMA=1: every group the streamed form serves takes it (64-word rows
   // first, three stages where they fit); the autotuner otherwise times it
   // beside the other forms
   const char *te = getenv("CC_TMA");
-  if (te && atoi(te) == 1) {
-    for (auto &p : P.groups) {
-      if (p.kernel < 0 || p.a.nrounds <= 0) continue;
-      bool done = false;
-      for (int stages : {3, 2, 0})
-        if (!done && tma_first_ok(p.a, S.R1, stages)) {
-          p = tma_first_variant(p, stages, 256);
-          done = true;
-        }
-      for (int lanes : {32, 16})
-        for (int stages : {3, 2}) {
-          if (done) break;
-          GroupPlan v = tma_variant(p, lanes, stages, 256);
-          if (tma_group_ok(v.a, p.a.rq[0], S.R1, lanes, stages)) {
-            p = v;
-            done = true;
-          }
-        }
-    }
-  }
+  if (te && atoi(te) == 1) stream_groups(P.groups, S.R1);
   return P;
 }
 

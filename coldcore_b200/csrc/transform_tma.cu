@@ -1005,6 +1005,9 @@ int opt_in(const TmaEntry *e) {
 }  // namespace
 
 int tma_prepare(const GroupPlan &p) {
+  // the mapped fault word is allocated here, ahead of any stream capture
+  int *fault = nullptr;
+  if (fault_word(&fault)) return -9;
   if (p.a.tma == 3) {
     const TernEntry *f = tern_of(p);
     return f ? tern_opt_in(f) : -9;

@@ -201,7 +201,9 @@ CCP_API int  dct_batch_read(long long h, int cell, int field, long long off,
                             long long len, void *out);
 /* per cell: deficit, gain maximum, loss maximum; returns values written */
 CCP_API int  dct_batch_scalars(long long h, long long *out, int cap);
-/* cells, passes, work items, tile KB, grid, tuned step microseconds */
+/* cells, passes, work items, tile KB, grid, tuned step microseconds; with
+ * cap >= 8 also the step's algorithmic HBM bytes and those of the cells
+ * with their own launches (returns the values written, 6 or 8) */
 CCP_API int  dct_batch_info(long long h, long long *out, int cap);
 /* Per-cell calls between launches, so a search can run on each cell
  * (the role of a campaign job's own plugin context, campaign.py:88-179).
