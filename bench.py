@@ -21,7 +21,9 @@ cpu_baseline : the C restatement of the reference's CPU axis DP on every
         host thread (oracle/cport), a bounded sample of the same cell.
 
 lns   : (1 GPU) LNS time-to-verified-size on K_3(14,3), learned ruin
-        proposal against plain LNS from the same greedy start, one seed.
+        proposal against plain LNS from the same greedy start, five seeds
+        (1..5; the moves for training are logged on seeds 1000..), median
+        and geometric mean of the per-seed time ratios.
 
 --impl reference runs that CPU restatement alone (rank 0), on the same
 cell, metric and unit: each step one transform of the cell, rotating
@@ -510,16 +512,18 @@ def measure_batch(args, dist):
 
 
 def measure_lns(args):
-    """LNS time-to-verified-size on K_3(14,3) (4.78M words, R = 3), one
-    seed: plain LNS moves are logged on other seeds and the MLP is trained
-    on them; then, from one greedy start, a plain descent (record mix) and
-    a learned-ruin descent run for the same wall-time budget.  The ratio is
-    the learned run's time to the plain run's best size over the plain
-    run's time to it (harness.lns_study runs the multi-seed form)."""
+    """LNS time-to-verified-size on K_3(14,3) (4.78M words, R = 3) over
+    several seeds: plain LNS moves are logged on other seeds and the MLP is
+    trained on them; then, per seed, from one greedy start, a plain descent
+    (record mix) and a learned-ruin descent run for the same wall-time
+    budget.  A seed's ratio is the learned run's time to the plain run's
+    best size over the plain run's time to it; reported with the median and
+    the geometric mean over the seeds (harness.lns_study.summarize)."""
     from coldcore_b200.gpu import GpuBackend
     from coldcore_b200.learned import RuinFeatures, train_scorer
-    from harness.lns_study import evaluate, log_moves
+    from harness.lns_study import evaluate, log_moves, summarize
     t0 = time.perf_counter()
+    seeds = list(range(1, args.lns_seeds + 1))
     with GpuBackend([3] * 14, 3) as b:
         feats = RuinFeatures(b)
         # the device exact greedy repairs every arm: plain LNS then makes
@@ -529,19 +533,31 @@ def measure_lns(args):
                          say=lambda *a: None, repair="device")
         X, y, g = mlog.arrays()
         sc = train_scorer(X, y, g, epochs=15)
-        run = evaluate(b, feats, sc, [1], args.lns_budget, 15.0,
-                       ["fixed", "learned"], say=lambda *a: None,
-                       repair="device")[0]
-    return {"cell": "K_3(14,3)", "seed": 1, "start_M": run["start_M"],
-            "budget_s": args.lns_budget, "notch_s": 15.0,
+        runs = evaluate(b, feats, sc, seeds, args.lns_budget, 10.0,
+                        ["fixed", "learned"], say=lambda *a: None,
+                        repair="device")
+    summ = summarize(runs)
+    per_seed = [{"seed": r["seed"], "start_M": r["start_M"],
+                 "target_M": r.get("target_M"),
+                 "best_plain": r["fixed"]["best"],
+                 "best_learned": r["learned"]["best"],
+                 "t_plain_s": r.get("t_plain"),
+                 "t_learned_s": r.get("t_learned"),
+                 "ratio": r.get("ratio"), "ratio_bound": r.get("ratio_bound"),
+                 "rounds_plain": r["fixed"]["rounds"],
+                 "rounds_learned": r["learned"]["rounds"]} for r in runs]
+    return {"cell": "K_3(14,3)", "seeds": seeds,
+            "budget_s": args.lns_budget, "notch_s": 10.0,
             "repair": "device (both arms)",
-            "best_plain": run["fixed"]["best"],
-            "best_learned": run["learned"]["best"],
-            "target_M": run["target_M"], "t_plain_s": run["t_plain"],
-            "t_learned_s": run["t_learned"], "ratio": run["ratio"],
-            "ratio_bound": run["ratio_bound"],
-            "rounds_plain": run["fixed"]["rounds"],
-            "rounds_learned": run["learned"]["rounds"],
+            "median_ratio": summ["median_ratio"],
+            "geo_mean_ratio": summ["geo_mean_ratio"],
+            "learned_reached": summ["learned_reached"],
+            "ratios": summ["ratios"],
+            "learned_smaller_or_equal": sum(
+                1 for r in per_seed
+                if r["best_learned"] is not None and r["best_plain"] is not None
+                and r["best_learned"] <= r["best_plain"]),
+            "per_seed": per_seed,
             "moves_logged": int(len(y)), "heldout_auc": sc.heldout_auc,
             "wall_s": round(time.perf_counter() - t0, 1)}
 
@@ -696,7 +712,8 @@ def main():
     ap.add_argument("--no-ops", action="store_true")
     ap.add_argument("--no-ooc", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--lns-budget", type=float, default=60.0)
+    ap.add_argument("--lns-budget", type=float, default=30.0)
+    ap.add_argument("--lns-seeds", type=int, default=5)
     ap.add_argument("--lns-moves", type=int, default=100000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
