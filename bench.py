@@ -439,7 +439,7 @@ def measure_batch_small(args):
 def form_name(f):
     """Schedule form flags of one launch (GpuBackend.plan_forms) as text."""
     names = [("pipe", 1), ("pack", 2), ("in16", 4), ("out16", 8),
-             ("pair", 16), ("tma", 32)]
+             ("pair", 16), ("tma", 32), ("u8", 64)]
     return "+".join(n for n, bit in names if int(f) & bit) or "plain"
 
 

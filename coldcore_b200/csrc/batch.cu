@@ -263,8 +263,10 @@ int make_schedule(Batch *b) {
         // group a streamed form serves
         if (!streams_off && kn.half &&
             !pad_plan(c.fast[t], c.g, ptr, dst, c.R1,
-                      (long long)(c.R1 - 1) * c.plane * 2))
+                      (long long)(c.R1 - 1) * c.plane * 2)) {
           stream_groups(c.fast[t], c.R1);
+          u8_plan(c.fast[t], c.R1, (long long)(c.R1 - 1) * c.plane * 2);
+        }
         for (auto &gp : c.fast[t]) {
           if (prepare_group(gp)) return -1;
           if (gp.a.tma && gp.grid < 1) {

@@ -72,6 +72,15 @@ struct GroupArgs {
   // read when in16, written when out16 (values provably <= 65535)
   uint16_t *layers16;
   int in16, out16;
+  // 8-bit planes between a streamed binary first group (out8) and the
+  // streamed launch after it (in8), where every layer value after the
+  // first group's k axes stays below 256: a 0/1 predicate source and
+  // C(k, d) <= 255 for every d <= R.  Plane d at byte off8 + d*plane of
+  // the 16-bit plane region, past the 16-bit planes that the launch
+  // reading them writes (so no tile overwrites bytes another has yet to
+  // read).
+  int in8, out8;
+  long long off8;
   int pack;               // two inner words per 32-bit lane (group_kernel)
   // first group of a binary Hamming cell: axis 0 is the word pair itself
   // (inner = 2), applied once as a swap-add inside each packed lane
@@ -115,6 +124,8 @@ struct TmaArgs {
   long long inner_c, pitch, t0;
   // ternary first group (tern_first): the rows of the cell
   long long rows;
+  // 8-bit layer planes (tma_first OUT 5): their byte offset from layers16
+  long long off8;
 };
 
 struct GroupPlan {
@@ -129,8 +140,9 @@ struct GroupPlan {
 // pipe: see plan_groups; half: 16-bit planes between the launches
 // pair: allow the pair first group (binary Hamming, 16-bit planes)
 // pad: the padded 16-bit layout for a ternary cell (streamed later groups)
+// u8: 8-bit planes after a streamed binary first group (gain / loss)
 struct Knobs { size_t budget; int pipe; int half = 0; int pair = 1;
-               int pad = 0; };
+               int pad = 0; int u8 = 0; };
 struct PlanPtrs {
   int32_t *layers; long long plane; uint16_t *cnt;
   const long long *code; long long ncode; int32_t *map;
@@ -172,12 +184,16 @@ bool pad_plan(std::vector<GroupPlan> &groups, const Geometry &g,
               const PlanPtrs &ptr, int dst, int R1, long long room16);
 // every group a streamed form serves takes it (planner.cu)
 void stream_groups(std::vector<GroupPlan> &groups, int R1);
+// 8-bit planes between the streamed first group and the launch after it
+// (planner.cu), in place; false leaves `groups` unchanged
+bool u8_plan(std::vector<GroupPlan> &groups, int R1, long long room16);
 // algorithmic HBM bytes of one group launch (planner.cu)
 long long group_bytes(const GroupArgs &a);
 std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
                                       size_t smem_cap);
 // streamed form of a strided group (transform_tma.cu)
-size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages);
+size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages,
+                      int in8 = 0);
 bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages);
 GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages, int threads);
 // the first group read from cnt (axis 0 in the pair), a.tma == 2

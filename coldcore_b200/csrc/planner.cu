@@ -246,8 +246,9 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
     out.push_back(v);
   }
   for (int lanes : {16, 32})
-    for (int stages : {2, 3})
-      if (!tma_off && tma_group_ok(tma_variant(p, lanes, stages, 256).a, q, R1, lanes,
+    for (int stages : {2, 3, 4})
+      if (!tma_off && (stages < 4 || p.a.in8) &&
+          tma_group_ok(tma_variant(p, lanes, stages, 256).a, q, R1, lanes,
                        stages))
         for (int th : {256, 512}) {
           GroupPlan v = tma_variant(p, lanes, stages, th);
@@ -264,6 +265,8 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
         v.grid = occupancy_grid(v);
         out.push_back(v);
       }
+  // 8-bit planes: only the streamed forms read or write them
+  if (p.a.in8 || p.a.out8) return out;
   for (int W : rows)
   for (int i = 0; i < nk; i++)
   for (int pipe = 0; pipe <= (can_pipe ? 1 : 0); pipe++) {
@@ -425,11 +428,61 @@ long long group_bytes(const GroupArgs &a) {
   long long rd = 0, wr = 0;
   if (a.src == kSrcCnt) rd = 2 * words;
   else if (a.src == kSrcCode) rd = 8 * a.ncode;
-  else rd = (long long)a.lin * (a.in16 ? 2 : 4) * words;
-  if (a.dst == kDstLayers) wr = (long long)a.lout * (a.out16 ? 2 : 4) * words;
+  else rd = (long long)a.lin * (a.in8 ? 1 : a.in16 ? 2 : 4) * words;
+  if (a.dst == kDstLayers)
+    wr = (long long)a.lout * (a.out8 ? 1 : a.out16 ? 2 : 4) * words;
   else if (a.dst == kDstMap) wr = 4 * words;
   else wr = 2 * words;
   return rd + wr;
+}
+
+// 8-bit planes between the streamed binary first group (read from cnt:
+// gain and loss) and the streamed launch after it.  After the first group's
+// k0 axes (the pair axis included), layer d of a 0/1 predicate counts at
+// most C(k0, d) words, so max over d <= R of C(k0, d) <= 255 makes every
+// value fit a byte: the first group writes half the bytes and the next
+// launch reads half.  The byte planes sit past the R1 16-bit planes of the
+// region (room16 u16 words); the launch after the first group writes those
+// 16-bit planes while it reads the byte planes.  false leaves `groups`
+// unchanged.
+bool u8_plan(std::vector<GroupPlan> &groups, int R1, long long room16) {
+  if (groups.size() < 2) return false;
+  const GroupPlan &f = groups[0], &n = groups[1];
+  if (f.a.tma != 2 || f.a.src != kSrcCnt || f.a.dst != kDstLayers ||
+      n.a.tma != 1 || n.a.src != kSrcLayers || !n.a.in16 || n.a.pitch)
+    return false;
+  const int k0 = f.a.k + f.a.pair_axis;
+  long long c = 1, mx = 1;
+  for (int d = 1; d <= f.a.R && d <= k0; d++) {
+    c = c * (k0 - d + 1) / d;
+    mx = std::max(mx, c);
+  }
+  if (mx > 255) return false;
+  const long long off8 = 2LL * R1 * f.a.plane;
+  if (off8 + (long long)R1 * f.a.plane > 2 * room16 || n.a.plane != f.a.plane)
+    return false;
+  GroupPlan f8 = f;
+  f8.a.out8 = 1;
+  f8.a.off8 = off8;
+  if (!tma_first_ok(f8.a, R1, f8.a.stages)) return false;
+  const int q = n.a.rq[0] ? n.a.rq[0] : n.a.qax[0];
+  const int lanes = n.a.W / 2;
+  GroupPlan n8 = n;
+  n8.a.in8 = 1;
+  n8.a.off8 = off8;
+  bool done = false;
+  for (int st : {n.a.stages, 3, 4, 2}) {
+    if (done) break;
+    GroupPlan v = tma_variant(n8, lanes, st, n.threads);
+    if (tma_group_ok(v.a, q, R1, lanes, st)) {
+      n8 = v;
+      done = true;
+    }
+  }
+  if (!done) return false;
+  groups[0] = f8;
+  groups[1] = n8;
+  return true;
 }
 
 }  // namespace cc

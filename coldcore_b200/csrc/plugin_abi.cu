@@ -361,8 +361,21 @@ Plan build_group_plan(int src, int dst, Knobs kn) {
   // CC_TMA=1: every group the streamed form serves takes it (64-word rows
   // first, three stages where they fit); the autotuner otherwise times it
   // beside the other forms
+  const char *ue = getenv("CC_U8");
+  const bool u8_off = ue && atoi(ue) == 0;
+  if (kn.u8) {
+    // 8-bit planes after the streamed first group, or no plan
+    stream_groups(P.groups, S.R1);
+    if (u8_off || !u8_plan(P.groups, S.R1,
+                         (long long)(S.nplanes - 1) * S.plane * 2)) P.groups.clear();
+    return P;
+  }
   const char *te = getenv("CC_TMA");
-  if (te && atoi(te) == 1) stream_groups(P.groups, S.R1);
+  if (te && atoi(te) == 1) {
+    stream_groups(P.groups, S.R1);
+    if (!u8_off) u8_plan(P.groups, S.R1,
+                         (long long)(S.nplanes - 1) * S.plane * 2);
+  }
   return P;
 }
 
@@ -606,7 +619,8 @@ std::vector<long long> grouping_key(const Plan &P) {
   std::vector<long long> k;
   for (const auto &g : P.groups)
     k.push_back(((long long)g.a.k << 32) | (g.a.W << 8) | (g.a.pipe << 1) |
-                g.a.pair_axis | ((g.a.pitch ? 1LL : 0LL) << 24));
+                g.a.pair_axis | ((g.a.pitch ? 1LL : 0LL) << 24) |
+                ((long long)(g.a.in8 | g.a.out8) << 25));
   return k;
 }
 
@@ -634,7 +648,11 @@ int autotune(int init_mode, int out_mode) {
                                 {64 << 10, 1, 0, 1, 1},
                                 {100 << 10, 1, 0, 1, 1},
                                 {160 << 10, 1, 0, 1, 1},
-                                {200 << 10, 1, 0, 1, 1}};
+                                {200 << 10, 1, 0, 1, 1},
+                                // 8-bit planes after the first group
+                                {64 << 10, 1, 0, 1, 0, 1},
+                                {100 << 10, 1, 0, 1, 0, 1},
+                                {160 << 10, 1, 0, 1, 0, 1}};
   EventPair ev;
   int rc = ev.create();
   if (rc) return rc;
@@ -1609,8 +1627,10 @@ int dct_b200_plan(int init_mode, int out_mode, long long *info, int cap) {
   for (const auto &p : P.groups) {
     long long rd = 0, wr = 0;
     if (p.a.src == kSrcCnt) rd = 2;
-    else if (p.a.src == kSrcLayers) rd = (p.a.in16 ? 2LL : 4LL) * p.a.lin;
-    if (p.a.dst == kDstLayers) wr = (p.a.out16 ? 2LL : 4LL) * p.a.lout;
+    else if (p.a.src == kSrcLayers)
+      rd = (p.a.in8 ? 1LL : p.a.in16 ? 2LL : 4LL) * p.a.lin;
+    if (p.a.dst == kDstLayers)
+      wr = (p.a.out8 ? 1LL : p.a.out16 ? 2LL : 4LL) * p.a.lout;
     else if (p.a.dst == kDstMap) wr = 4;
     else wr = 2;
     long long by = X * (rd + wr);
@@ -1693,7 +1713,8 @@ int dct_b200_plan_forms(int init_mode, int out_mode, int *forms, int cap) {
     if (forms && n < cap)
       forms[n] = (p.a.pipe ? 1 : 0) | (p.a.pack ? 2 : 0) |
                  (p.a.in16 ? 4 : 0) | (p.a.out16 ? 8 : 0) |
-                 (p.a.pair_axis ? 16 : 0) | (p.a.tma ? 32 : 0);
+                 (p.a.pair_axis ? 16 : 0) | (p.a.tma ? 32 : 0) |
+                 (p.a.in8 || p.a.out8 ? 64 : 0);
     n++;
   }
   return n;

@@ -1076,7 +1076,13 @@ int group_blocks_per_sm(const GroupPlan &p) {
   }
   if (!have_device) return 0;
   if (p.a.tma) return tma_blocks_per_sm(p);
-  if (ensure_group_smem(p)) return 0;
+  // a tile above the per-block limit has no occupancy (a plan built only
+  // for its grouping); a refused opt-in leaves no error for later checks
+  if (p.smem > 227 * 1024) return 0;
+  if (ensure_group_smem(p)) {
+    cudaGetLastError();
+    return 0;
+  }
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
           &n, (const void *)group_fn(p), p.threads, p.smem) != cudaSuccess) {

@@ -150,9 +150,10 @@ struct RoundAxes {
 // load lays it down).  FIRST: layers >= lin start at zero.  LAST: the
 // block goes to HBM (OUT 0 layers, 1 map, 2 cnt) instead of the stage.
 template <int Q, int K, int R1, int L, int OUT, int A, int B, bool FIRST,
-          bool LAST>
+          bool LAST, bool IN8 = false>
 __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
-                                          long long o, long long i0) {
+                                          long long o, long long i0,
+                                          const uint16_t *s8 = nullptr) {
   constexpr int MID = P<Q, K>::v;
   constexpr int QB = P<Q, B>::v;
   constexpr int QA = P<Q, A>::v;
@@ -163,12 +164,27 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
     const int mb = rest % QA + (rest / QA) * (QA * QB);
     uint32_t *p = st + mb * L + l;
     uint32_t v[R1][QB];
+    if (IN8 && FIRST) {
+      // the staged 8-bit planes: one 16-bit read gives the lane's two
+      // words, widened to the two 16-bit halves of the packed lane
+      const uint16_t *p8 = s8 + mb * L + l;
 #pragma unroll
-    for (int d = 0; d < R1; d++) {
-      const bool live = !FIRST || d < a.lin;
+      for (int d = 0; d < R1; d++) {
+        const bool live = d < a.lin;
 #pragma unroll
-      for (int e = 0; e < QB; e++)
-        v[d][e] = live ? p[(d * MID + e * QA) * L] : 0u;
+        for (int e = 0; e < QB; e++)
+          v[d][e] = live ? __byte_perm((uint32_t)p8[(d * MID + e * QA) * L],
+                                       0u, 0x4140)
+                         : 0u;
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < R1; d++) {
+        const bool live = !FIRST || d < a.lin;
+#pragma unroll
+        for (int e = 0; e < QB; e++)
+          v[d][e] = live ? p[(d * MID + e * QA) * L] : 0u;
+      }
     }
     Axes<Q, R1, B, 0>::run(v);
     if (!LAST) {
@@ -230,21 +246,25 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
 
 // The rounds of a K-axis group: RoundAxes-sized rounds from axis 0 up, the
 // remainder last.
-template <int Q, int K, int R1, int L, int OUT, int A>
+template <int Q, int K, int R1, int L, int OUT, int A, bool IN8 = false>
 struct Rounds {
   static constexpr int BM = RoundAxes<Q, R1>::v;
   static constexpr int B = (K - A) < BM ? (K - A) : BM;
   static __device__ __forceinline__ void run(uint32_t *st, const TmaArgs &a,
-                                             long long o, long long i0) {
-    tma_round<Q, K, R1, L, OUT, A, B, A == 0, A + B == K>(st, a, o, i0);
+                                             long long o, long long i0,
+                                             const uint16_t *s8 = nullptr) {
+    tma_round<Q, K, R1, L, OUT, A, B, A == 0, A + B == K, IN8>(st, a, o, i0,
+                                                              s8);
     if (A + B < K) __syncthreads();
-    Rounds<Q, K, R1, L, OUT, (A + B < K ? A + B : K)>::run(st, a, o, i0);
+    Rounds<Q, K, R1, L, OUT, (A + B < K ? A + B : K), IN8>::run(st, a, o, i0,
+                                                                s8);
   }
 };
-template <int Q, int K, int R1, int L, int OUT>
-struct Rounds<Q, K, R1, L, OUT, K> {
+template <int Q, int K, int R1, int L, int OUT, bool IN8>
+struct Rounds<Q, K, R1, L, OUT, K, IN8> {
   static __device__ __forceinline__ void run(uint32_t *, const TmaArgs &,
-                                             long long, long long) {}
+                                             long long, long long,
+                                             const uint16_t *) {}
 };
 
 // stage stride: the tile's words rounded up to 1 KB (tensor loads land on
@@ -253,20 +273,32 @@ template <int Q, int K, int R1, int L>
 struct Stage {
   static constexpr int words = (R1 * P<Q, K>::v * L + 255) / 256 * 256;
 };
+// 8-bit staged planes: a stage is R1 x mid x 2L bytes (1 KB multiples),
+// and the rounds run on one 32-bit work buffer of the Stage size
+template <int Q, int K, int R1, int L>
+struct Stage8 {
+  static constexpr int bytes = (R1 * P<Q, K>::v * 2 * L + 1023) / 1024 * 1024;
+};
 
-template <int Q, int K, int R1, int L, int OUT>
+template <int Q, int K, int R1, int L, int OUT, bool IN8 = false>
 __global__ void __launch_bounds__(512)
 tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
   extern __shared__ __align__(128) uint8_t dyn[];
   constexpr int MID = P<Q, K>::v;
   constexpr int SW = Stage<Q, K, R1, L>::words;
+  // bytes a stage: the 16-bit planes' tile, or the 8-bit planes' tile
+  constexpr int SB = IN8 ? Stage8<Q, K, R1, L>::bytes : SW * 4;
   const int S = a.stages;
-  // stages on a 1 KB boundary, then the barriers and the stop flag
+  // stages on a 1 KB boundary, then (8-bit planes) the work buffer, then
+  // the barriers and the stop flag
   uint8_t *base = dyn + ((1024u - (saddr(dyn) & 1023u)) & 1023u);
-  uint32_t *stage = reinterpret_cast<uint32_t *>(base);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(base + (size_t)S * SW * 4);
+  uint8_t *stage = base;
+  uint32_t *work = IN8 ? reinterpret_cast<uint32_t *>(base + (size_t)S * SB)
+                       : nullptr;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(
+      base + (size_t)S * SB + (IN8 ? (size_t)SW * 4 : 0));
   volatile int *stop = reinterpret_cast<volatile int *>(bar + kTmaMaxStages);
-  const uint32_t bytes = (uint32_t)(2 * L * 2) * MID * a.lin;
+  const uint32_t bytes = (uint32_t)(2 * L * (IN8 ? 1 : 2)) * MID * a.lin;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; s++) mbar_init(&bar[s]);
     *stop = 0;
@@ -278,7 +310,7 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
     const int i0 = (int)((t % a.nchunk) * (2 * L));
     const int o = (int)(t / a.nchunk);
     mbar_expect(&bar[s], bytes);
-    tma_load4(stage + (size_t)s * SW, &map, &bar[s], i0, 0, o, 0);
+    tma_load4(stage + (size_t)s * SB, &map, &bar[s], i0, 0, o, 0);
   };
   if (threadIdx.x == 0) {
     asm volatile("prefetch.tensormap [%0];\n" ::"l"(
@@ -299,7 +331,13 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
     if (*stop) break;
     const long long o = t / a.nchunk;
     const long long i0 = (t % a.nchunk) * (2 * L);
-    Rounds<Q, K, R1, L, OUT, 0>::run(stage + (size_t)s * SW, a, o, i0);
+    if (IN8)
+      Rounds<Q, K, R1, L, OUT, 0, IN8>::run(
+          work, a, o, i0,
+          reinterpret_cast<const uint16_t *>(stage + (size_t)s * SB));
+    else
+      Rounds<Q, K, R1, L, OUT, 0>::run(
+          reinterpret_cast<uint32_t *>(stage + (size_t)s * SB), a, o, i0);
     __syncthreads();                          // stage s is free again
     if (threadIdx.x == 0) {
       const long long nt = t + S * grid;
@@ -408,6 +446,19 @@ __device__ __forceinline__ void first_round(uint32_t *work, int WS,
 #pragma unroll
         for (int e = 0; e < QB; e++)
           __stcs(reinterpret_cast<unsigned *>(q + 2 * e * QA), v[d][e]);
+      }
+    } else if (OUT == 5) {
+      // 8-bit planes: the low bytes of the pair's two halves (every value
+      // below 256 by the planner's bound), one 16-bit store a lane
+      uint8_t *q8 = reinterpret_cast<uint8_t *>(a.layers16) + a.off8;
+#pragma unroll
+      for (int d = 0; d < R1; d++) {
+        if (d >= a.lout) break;
+        uint8_t *q = q8 + d * a.plane + xb;
+#pragma unroll
+        for (int e = 0; e < QB; e++)
+          __stcs(reinterpret_cast<unsigned short *>(q + 2 * e * QA),
+                 (unsigned short)__byte_perm(v[d][e], 0u, 0x4420));
       }
     } else {
 #pragma unroll
@@ -699,7 +750,7 @@ tern_first(const TmaArgs a) {
 // ------------------------------------------------------------ dispatch
 typedef void (*TmaFn)(const CUtensorMap, const TmaArgs);
 
-struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; };
+struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; int in8 = 0; };
 
 #define TE(Q, K, R1, L)                                                     \
   {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0>},                              \
@@ -707,6 +758,11 @@ struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; };
   {Q, K, R1, L, 2, tma_group<Q, K, R1, L, 2>}
 // ternary groups run only in the padded layout: OUT 0 (layers), 3 (map)
 // and 4 (cnt), the last two back to the canonical index
+// the launch after an 8-bit first group: its planes staged as bytes
+#define TE8(Q, K, R1, L)                                                    \
+  {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0, true>, 1},                     \
+  {Q, K, R1, L, 1, tma_group<Q, K, R1, L, 1, true>, 1},                     \
+  {Q, K, R1, L, 2, tma_group<Q, K, R1, L, 2, true>, 1}
 #define TE3(Q, K, R1, L)                                                    \
   {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0>},                              \
   {Q, K, R1, L, 3, tma_group<Q, K, R1, L, 3>},                              \
@@ -718,9 +774,12 @@ const TmaEntry kTma[] = {
     TE3(3, 3, 4, 32), TE3(3, 4, 4, 32),
     TE3(3, 3, 5, 16), TE3(3, 4, 5, 16), TE3(3, 5, 5, 16),
     TE3(3, 3, 5, 32), TE3(3, 4, 5, 32),
+    TE8(2, 5, 4, 16), TE8(2, 6, 4, 16), TE8(2, 7, 4, 16), TE8(2, 8, 4, 16),
+    TE8(2, 5, 4, 32), TE8(2, 6, 4, 32), TE8(2, 7, 4, 32),
 };
 #undef TE
 #undef TE3
+#undef TE8
 
 typedef void (*FirstFn)(const TmaArgs);
 // src 0: the cnt predicate (tma_first), 1: the sorted code (code_first)
@@ -729,9 +788,12 @@ struct FirstEntry { int src, kk, r1, out; FirstFn fn; };
                    {0, KK, R1, 1, tma_first<KK, R1, 1>},                 \
                    {1, KK, R1, 0, code_first<KK, R1, 0>},                \
                    {1, KK, R1, 2, code_first<KK, R1, 2>}
+// OUT 5: 8-bit layer planes (C(KK + 1, d) <= 255 for d <= 3)
+#define FE8(KK) {0, KK, 4, 5, tma_first<KK, 4, 5>}
 const FirstEntry kFirst[] = {FE(9, 4), FE(10, 4), FE(11, 4), FE(12, 4),
-                             FE(13, 4)};
+                             FE(13, 4), FE8(9), FE8(10), FE8(11)};
 #undef FE
+#undef FE8
 
 // the ternary first group: src 0 cnt, 1 code; KK axes; R1 layers
 struct TernEntry { int src, kk, r1; FirstFn fn; };
@@ -759,12 +821,18 @@ int out_code(const GroupArgs &a) {
   return (a.pitch && out) ? out + 2 : out;
 }
 
-const TmaEntry *find_tma(int q, int k, int r1, int lanes, int out) {
+const TmaEntry *find_tma(int q, int k, int r1, int lanes, int out,
+                         int in8 = 0) {
   for (const auto &e : kTma)
     if (e.q == q && e.k == k && e.r1 == r1 && e.lanes == lanes &&
-        e.out == out)
+        e.out == out && e.in8 == (in8 ? 1 : 0))
       return &e;
   return nullptr;
+}
+
+// the first group's OUT: 0 16-bit layers, 5 8-bit layers, 1 map, 2 cnt
+int first_out(const GroupArgs &a) {
+  return a.dst == kDstLayers ? (a.out8 ? 5 : 0) : a.dst == kDstMap ? 1 : 2;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -813,10 +881,15 @@ int fault_word(int **dev) {
 
 }  // namespace
 
-size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages) {
+size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages,
+                      int in8) {
   long long mid = 1;
   for (int i = 0; i < k; i++) mid *= q;
   const long long words = (r1 * mid * lanes + 255) / 256 * 256;
+  if (in8) {                    // byte stages and one 32-bit work buffer
+    const long long sb = (r1 * mid * 2 * lanes + 1023) / 1024 * 1024;
+    return (size_t)(stages * sb + words * 4) + 1024 + kTmaMaxStages * 8 + 16;
+  }
   return (size_t)stages * words * 4 + 1024 + kTmaMaxStages * 8 + 16;
 }
 
@@ -827,16 +900,19 @@ size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages) {
 bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
   if (stages < 2 || stages > kTmaMaxStages || !encode_fn()) return false;
   const int out = out_code(a);
-  if (!find_tma(q, a.k, r1, lanes, out)) return false;
+  if (!find_tma(q, a.k, r1, lanes, out, a.in8)) return false;
   if (a.prob != kHamming || !a.pack || !a.in16 || a.pair_axis ||
       a.src != kSrcLayers || a.R + 1 != r1)
     return false;
   if (out == 0 && !a.out16) return false;
+  // 8-bit planes: the tensor map's byte strides are multiples of 16
+  if (a.in8 && (a.plane % 16 || a.inner % 16 || a.pitch || a.off8 % 16))
+    return false;
   if (a.inner % (2 * lanes) || a.plane % 8 || a.lin < 1 || a.lin > r1)
     return false;
   if ((reinterpret_cast<uintptr_t>(a.layers16) & 15) != 0) return false;
   if (a.outer >= (1LL << 31) || a.inner >= (1LL << 31)) return false;
-  return tma_smem_bytes(q, a.k, r1, lanes, stages) <= kTmaSmemMax;
+  return tma_smem_bytes(q, a.k, r1, lanes, stages, a.in8) <= kTmaSmemMax;
 }
 
 // The same group as a streamed launch: W = 2 x lanes inner words a tile.
@@ -863,7 +939,7 @@ GroupPlan tma_variant(const GroupPlan &p, int lanes, int stages,
   v.a.ntiles = v.a.outer * v.a.nchunk;
   v.threads = threads;
   v.smem = tma_smem_bytes(v.a.rq[0] ? v.a.rq[0] : v.a.qax[0], v.a.k,
-                          v.a.R + 1, lanes, stages);
+                          v.a.R + 1, lanes, stages, v.a.in8);
   v.grid = 0;
   return v;
 }
@@ -885,12 +961,12 @@ bool tma_first_ok(const GroupArgs &a, int r1, int stages) {
   if (src < 0 || (src == 0 && (stages < 2 || stages > kTmaMaxStages)) ||
       (src == 1 && stages != 0))
     return false;
-  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
+  const int out = first_out(a);
   if (!find_first(src, a.k, r1, out)) return false;
   if (a.prob != kHamming || !a.pair_axis || !a.pack || a.W != 2 ||
       a.inner != 2 || a.Bo != 1 || a.R + 1 != r1 || a.nchunk != 1)
     return false;
-  if (out == 0 && !a.out16) return false;
+  if ((out == 0 || out == 5) && !a.out16) return false;
   if (a.plane % 8 || (reinterpret_cast<uintptr_t>(a.cnt) & 15) != 0)
     return false;
   return tma_first_smem_bytes(a.k, r1, stages) <= kTmaSmemMax;
@@ -945,8 +1021,7 @@ namespace {
 
 const FirstEntry *first_of(const GroupPlan &p) {
   const GroupArgs &a = p.a;
-  const int out = a.dst == kDstLayers ? 0 : a.dst == kDstMap ? 1 : 2;
-  return find_first(a.src == kSrcCode ? 1 : 0, a.k, a.R + 1, out);
+  return find_first(a.src == kSrcCode ? 1 : 0, a.k, a.R + 1, first_out(a));
 }
 
 int first_opt_in(const FirstEntry *e) {
@@ -984,7 +1059,8 @@ int tern_opt_in(const TernEntry *e) {
 const TmaEntry *entry_of(const GroupPlan &p) {
   const GroupArgs &a = p.a;
   const int out = out_code(a);
-  return find_tma(a.rq[0] ? a.rq[0] : a.qax[0], a.k, a.R + 1, a.W / 2, out);
+  return find_tma(a.rq[0] ? a.rq[0] : a.qax[0], a.k, a.R + 1, a.W / 2, out,
+                  a.in8);
 }
 
 // opt every streamed kernel in to the largest dynamic shared memory once
@@ -1050,7 +1126,7 @@ int launch_tern_first(const GroupPlan &p, cudaStream_t s) {
   const TernEntry *f = tern_of(p);
   const bool from_code = a.src == kSrcCode;
   if (!f || !tern_first_ok(a, a.R + 1) ||
-      (from_code && (!a.code_bounds || !a.code)))
+      (from_code && (!a.code_bounds || (!a.code && a.ncode > 0))))
     return -9;
   int rc = tern_opt_in(f);
   if (rc) return rc;
@@ -1088,7 +1164,7 @@ int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
   const FirstEntry *f = first_of(p);
   const bool from_code = a.src == kSrcCode;
   if (!f || (!from_code && (a.stages < 2 || a.stages > kTmaMaxStages)) ||
-      (from_code && (!a.code_bounds || !a.code)))
+      (from_code && (!a.code_bounds || (!a.code && a.ncode > 0))))
     return -9;
   int *fault = nullptr;
   if (fault_word(&fault)) return -9;
@@ -1112,6 +1188,7 @@ int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
   t.fault = fault;
   t.code = a.code;
   t.code_bounds = a.code_bounds;
+  t.off8 = a.off8;
   const size_t smem = tma_first_smem_bytes(a.k, a.R + 1,
                                            from_code ? 0 : a.stages);
   int grid = p.grid;
@@ -1142,18 +1219,24 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   if (rc) return rc;
   long long mid = 1;
   for (int i = 0; i < a.k; i++) mid *= q;
-  // the live layers as a 4-D u16 tensor: inner word, mid, outer, layer
+  // the live layers as a 4-D u16 (or, 8-bit planes, u8) tensor: inner
+  // word, mid, outer, layer
   CUtensorMap map;
+  const cuuint64_t esz = a.in8 ? 1 : 2;
   const cuuint64_t dims[4] = {(cuuint64_t)a.inner, (cuuint64_t)mid,
                               (cuuint64_t)a.outer, (cuuint64_t)a.lin};
-  const cuuint64_t strides[3] = {(cuuint64_t)a.inner * 2,
-                                 (cuuint64_t)(a.inner * mid) * 2,
-                                 (cuuint64_t)a.plane * 2};
+  const cuuint64_t strides[3] = {(cuuint64_t)a.inner * esz,
+                                 (cuuint64_t)(a.inner * mid) * esz,
+                                 (cuuint64_t)a.plane * esz};
   const cuuint32_t box[4] = {(cuuint32_t)(2 * lanes), (cuuint32_t)mid, 1,
                              (cuuint32_t)a.lin};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
-                          a.layers16, dims, strides, box, estr,
+  void *gbase = a.in8 ? (void *)(reinterpret_cast<uint8_t *>(a.layers16) +
+                                 a.off8)
+                      : (void *)a.layers16;
+  const CUresult cr = enc(&map, a.in8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                      : CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+                          gbase, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE,
                           CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1178,7 +1261,8 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   t.pitch = a.pitch;
   t.t0 = a.t0;
   t.inner_c = a.pitch ? a.inner / a.pitch * a.t0 : a.inner;
-  const size_t smem = tma_smem_bytes(q, a.k, a.R + 1, lanes, a.stages);
+  const size_t smem = tma_smem_bytes(q, a.k, a.R + 1, lanes, a.stages,
+                                     a.in8);
   int grid = p.grid;
   if (grid < 1) {
     const int per_sm = tma_blocks_per_sm(p);

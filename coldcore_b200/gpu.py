@@ -430,12 +430,13 @@ class GpuBackend:
             _check("plan", n)
         return buf[:4 * n].reshape(n, 4)
 
-    PIPE, PACK, IN16, OUT16, PAIR = 1, 2, 4, 8, 16
+    PIPE, PACK, IN16, OUT16, PAIR, STREAMED, BYTE8 = 1, 2, 4, 8, 16, 32, 64
 
     def plan_forms(self, init_mode, out_mode):
         """Schedule form of each group launch of one transform, as bit flags
         (PIPE prefetching kernel, PACK word pairs, IN16 / OUT16 16-bit
-        layers, PAIR axis 0 inside each pair)."""
+        layers, PAIR axis 0 inside each pair, STREAMED a streamed form,
+        BYTE8 8-bit layers read or written)."""
         buf = np.zeros(64, dtype=np.int32)
         n = self._lib.dct_b200_plan_forms(init_mode, out_mode,
                                           _p(buf, ctypes.c_int32), len(buf))

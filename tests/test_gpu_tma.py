@@ -19,6 +19,7 @@ TMA = 32                                 # GpuBackend.plan_forms bit
     ([2] * 12, 3, 1), ([2] * 23, 3, 1), ([2] * 13 + [3], 3, 1)])
 def test_streamed_groups_match_the_oracle(monkeypatch, axes, R, mu):
     monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_U8", "0")
     monkeypatch.setenv("CC_TUNE", "0")
     size = int(np.prod(axes))
     rng = np.random.default_rng(size % 1000 + R)
@@ -95,3 +96,39 @@ def test_padded_ternary_plan_counts_a_multiset(monkeypatch):
         o.loss_map()
         assert np.array_equal(b.map_all(), o.map)
         assert (b.plan_forms(0, 2) & TMA).all()
+
+
+BYTE8 = 64                               # GpuBackend.plan_forms bit
+
+
+@pytest.mark.parametrize("axes,R,mu", [
+    ([2] * 20, 3, 1), ([2] * 21, 3, 2), ([2] * 23, 3, 1), ([2] * 26, 3, 1)])
+def test_byte_planes_after_the_first_group(monkeypatch, axes, R, mu):
+    """Gain and loss of binary R = 3 cells: the streamed first group (12
+    axes at most, so every layer value is at most C(12, 3) = 220) writes
+    8-bit planes past the 16-bit ones and the next launch stages them as
+    bytes; fields equal the oracle's, and the recount keeps 16-bit planes.
+    A 64 KB tile budget gives the 12-axis first group."""
+    monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_TUNE", "0")
+    monkeypatch.setenv("CC_SMEM_BUDGET_KB", "64")
+    size = int(np.prod(axes))
+    rng = np.random.default_rng(size % 991 + mu)
+    o = OracleBackend(axes, R, mu=mu)
+    with GpuBackend(axes, R, mu=mu) as b:
+        for step in range(2):
+            code = np.sort(rng.choice(size, size=size // (180 + 40 * step),
+                                      replace=False))
+            b.recount(code)
+            o.recount(code)
+            assert np.array_equal(b.read_cnt(), o.read_cnt()), step
+            b.gain_map()
+            o.gain_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            b.loss_map()
+            o.loss_map()
+            assert np.array_equal(b.map_all(), o.map), step
+        for im, om in ((1, 1), (2, 1)):
+            forms = b.plan_forms(im, om)
+            assert forms[0] & BYTE8 and forms[1] & BYTE8, (im, forms)
+        assert not (b.plan_forms(0, 2) & BYTE8).any()
