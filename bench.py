@@ -386,6 +386,16 @@ def measure_cell(cell, args, dist, timed=True):
         b.close()
 
 
+def step_rate(out):
+    """A batched step's achieved DRAM-side rate: its algorithmic bytes (each
+    launch's source read once, its destination written once; the batch
+    plan's own count) over the persistent step time, against the peak."""
+    peak, peak_kind = peaks()
+    gbs = out["step_bytes"] / (out["persistent"]["ms_per_step"] * 1e-3) / 1e9
+    return {"step_GBps": round(gbs, 1), "step_frac": round(gbs / peak, 4),
+            "peak_kind": peak_kind}
+
+
 def measure_batch_small(args):
     """A campaign of many small cells, where a persistent launch pays:
     1,024 seeded cells of 10^3..10^5 words (otherwise as measure_batch).
@@ -401,6 +411,7 @@ def measure_batch_small(args):
         for p, a, R, code in cells:
             b.add(p, a, R, code)
         b.build(0)
+        out["step_bytes"] = b.info()["step_bytes"]
         for mode, key in ((0, "persistent"), (1, "per_pass_launches")):
             for _ in range(2):
                 b.run(mode)
@@ -414,14 +425,7 @@ def measure_batch_small(args):
                         "instances_per_s": round(len(cells) / dt, 1)}
     out["speedup"] = round(out["persistent"]["instances_per_s"]
                            / out["per_pass_launches"]["instances_per_s"], 2)
-    # the step's achieved DRAM-side rate: its algorithmic bytes (each
-    # launch's source read once, its destination written once) over the
-    # persistent step time
-    peak, peak_kind = peaks()
-    gbs = out["step_bytes"] / (out["persistent"]["ms_per_step"] * 1e-3) / 1e9
-    out["step_GBps"] = round(gbs, 1)
-    out["step_frac"] = round(gbs / peak, 4)
-    out["peak_kind"] = peak_kind
+    out.update(step_rate(out))
     if not args.no_cpu:
         from oracle.cport import campaign_rate     # the CPU baseline leg
         rate, wall, busy, workers = campaign_rate(cells)
@@ -493,6 +497,7 @@ def measure_batch(args, dist):
     out["speedup_vs_singleton"] = round(
         out["persistent"]["instances_per_s"]
         / out["singleton_per_cell"]["instances_per_s"], 2)
+    out.update(step_rate(out))
     out["words"] = int(sum(int(np.prod(a)) for _, a, _, _ in cells))
     if not args.no_cpu and dist.world == 1:
         # the reference campaign's own parallelism: one cell per process on

@@ -40,6 +40,7 @@ struct Cell {
   long long nbounds = 0;
   int first_pass = 0, npass = 0;     // global pass range (small cells)
   bool big = false;                  // own register-blocked launches
+  int side = 0;                      // its side stream (big cells)
   std::vector<GroupPlan> fast[3];    // recount, gain, loss (big cells)
   // codes may be replaced between launches (dct_batch_set_code): the
   // device buffer holds code_cap words, its length lives on the device
@@ -79,7 +80,14 @@ __global__ void k_batch_bounds(const BoundsJob *jobs) {
 // streams of the same graph); smaller cells share the persistent kernel.
 constexpr long long kBigCell = 1LL << 16;
 constexpr long long kItemWords = 32768;   // words per work item (at least)
-constexpr int kSideStreams = 4;
+// side streams the big cells are spread over (CC_BATCH_STREAMS, 1..16,
+// default 8), largest cells first onto the least loaded stream
+constexpr int kSideStreams = 16;
+int side_streams() {
+  const char *e = getenv("CC_BATCH_STREAMS");
+  const int n = e ? atoi(e) : 8;
+  return n < 1 ? 1 : n > kSideStreams ? kSideStreams : n;
+}
 
 struct Batch {
   std::vector<Cell> cells;
@@ -118,6 +126,7 @@ struct Batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   float tuned_ms = 0;
+  int nside = 4;                     // side streams in use
 };
 
 std::unordered_map<long long, Batch *> g_batches;
@@ -311,6 +320,34 @@ int make_schedule(Batch *b) {
     }
     c.npass = (int)b->passes.size() - c.first_pass;
   }
+  // big cells onto the side streams: largest (algorithmic bytes) first,
+  // each onto the least loaded stream
+  {
+    b->nside = side_streams();
+    std::vector<std::pair<long long, size_t>> order;
+    for (size_t i = 0; i < b->cells.size(); i++) {
+      const Cell &c = b->cells[i];
+      if (!c.big) continue;
+      long long by = 0;
+      for (int t = 0; t < 3; t++)
+        for (const auto &gp : c.fast[t]) by += group_bytes(gp.a);
+      order.push_back({by, i});
+    }
+    std::sort(order.begin(), order.end(),
+              [](const std::pair<long long, size_t> &x,
+                 const std::pair<long long, size_t> &y) {
+                return x.first != y.first ? x.first > y.first
+                                          : x.second < y.second;
+              });
+    std::vector<long long> load(b->nside, 0);
+    for (const auto &o : order) {
+      int k = 0;
+      for (int j = 1; j < b->nside; j++)
+        if (load[j] < load[k]) k = j;
+      b->cells[o.second].side = k;
+      load[k] += o.first;
+    }
+  }
   // tile slices of each cell's code for this schedule's first groups
   auto first_tiles = [&](const Cell &c) {
     return c.big ? c.fast[0][0].a.ntiles : b->passes[c.first_pass].ntiles;
@@ -449,18 +486,17 @@ int capture_graph(Batch *b) {
   // big cells fork onto side streams, small cells share one persistent
   // launch on the main stream, and everything joins before the end
   ck(cudaEventRecord(b->fork, b->stream), "fork record");
-  for (int k = 0; k < kSideStreams; k++)
+  for (int k = 0; k < b->nside; k++)
     ck(cudaStreamWaitEvent(b->side[k], b->fork, 0), "fork wait");
-  int nbig = 0;
   for (size_t i = 0; i < b->cells.size() && !rc; i++)
     if (b->cells[i].big)
-      rc = run_big_cell(b, i, b->side[nbig++ % kSideStreams]);
+      rc = run_big_cell(b, i, b->side[b->cells[i].side]);
   if (!rc && b->nitems) {
     BatchLaunch L{b->d_passes, b->d_dep, b->d_need, b->d_items, b->nitems,
                   b->d_done, b->d_next, b->d_err, b->smem, b->grid};
     rc = launch_batch(L, b->stream);
   }
-  for (int k = 0; k < kSideStreams; k++) {
+  for (int k = 0; k < b->nside; k++) {
     ck(cudaEventRecord(b->join[k], b->side[k]), "join record");
     ck(cudaStreamWaitEvent(b->stream, b->join[k], 0), "join wait");
   }
@@ -493,13 +529,12 @@ int run_per_pass(Batch *b) {
       b->d_jobs);
   CC_CK(cudaGetLastError());
   CC_CK(cudaEventRecord(b->fork, b->stream));
-  for (int k = 0; k < kSideStreams; k++)
+  for (int k = 0; k < b->nside; k++)
     CC_CK(cudaStreamWaitEvent(b->side[k], b->fork, 0));
-  int nbig = 0;
   for (size_t i = 0; i < b->cells.size(); i++) {
     const Cell &c = b->cells[i];
     if (c.big) {
-      const int rc = run_big_cell(b, i, b->side[nbig++ % kSideStreams]);
+      const int rc = run_big_cell(b, i, b->side[c.side]);
       if (rc) return rc;
       continue;
     }
@@ -515,7 +550,7 @@ int run_per_pass(Batch *b) {
       if (rc) return rc;
     }
   }
-  for (int k = 0; k < kSideStreams; k++) {
+  for (int k = 0; k < b->nside; k++) {
     CC_CK(cudaEventRecord(b->join[k], b->side[k]));
     CC_CK(cudaStreamWaitEvent(b->stream, b->join[k], 0));
   }

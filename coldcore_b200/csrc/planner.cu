@@ -246,7 +246,7 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
     out.push_back(v);
   }
   for (int lanes : {16, 32})
-    for (int stages : {2, 3, 4})
+    for (int stages : {1, 2, 3, 4})
       if (!tma_off && (stages < 4 || p.a.in8) &&
           tma_group_ok(tma_variant(p, lanes, stages, 256).a, q, R1, lanes,
                        stages))

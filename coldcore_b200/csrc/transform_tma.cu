@@ -898,7 +898,9 @@ size_t tma_smem_bytes(int q, int k, int r1, int lanes, int stages,
 // one tile per W inner words x the whole group, an instantiated (q, k,
 // layers, lanes) and its stages within 227 KB of shared memory.
 bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
-  if (stages < 2 || stages > kTmaMaxStages || !encode_fn()) return false;
+  // one stage: a CTA small enough for two a SM, whose loads then overlap
+  // the other CTA's rounds
+  if (stages < 1 || stages > kTmaMaxStages || !encode_fn()) return false;
   const int out = out_code(a);
   if (!find_tma(q, a.k, r1, lanes, out, a.in8)) return false;
   if (a.prob != kHamming || !a.pack || !a.in16 || a.pair_axis ||
@@ -1212,7 +1214,7 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   const int lanes = a.W / 2;
   const TmaEntry *e = entry_of(p);
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
-  if (!e || !enc || a.stages < 2 || a.stages > kTmaMaxStages) return -9;
+  if (!e || !enc || a.stages < 1 || a.stages > kTmaMaxStages) return -9;
   int *fault = nullptr;
   if (fault_word(&fault)) return -9;
   int rc = opt_in(e);
