@@ -638,7 +638,7 @@ struct TernRound {
 
 template <int KK, int R1, int SRC, int I>
 __device__ __forceinline__ void tern_round(uint32_t *work, const TmaArgs &a,
-                                           long long r0, bool two,
+                                           long long r0, bool two, bool wide,
                                            uint32_t plo, uint32_t pspan) {
   using TR = TernRound<KK, I>;
   constexpr int A = TR::A, B = TR::B;
@@ -680,6 +680,13 @@ __device__ __forceinline__ void tern_round(uint32_t *work, const TmaArgs &a,
         for (int e = 0; e < QB; e++) work[d * WS + pb + e * QA] = v[d][e];
       continue;
     }
+    if (wide) {                 // back to the buffer; tern_copy_out stores
+#pragma unroll
+      for (int d = 0; d < R1; d++)
+#pragma unroll
+        for (int e = 0; e < QB; e++) work[d * WS + pb + e * QA] = v[d][e];
+      continue;
+    }
     const long long x0 = r0 * a.pitch + pb;
 #pragma unroll
     for (int d = 0; d < R1; d++) {
@@ -698,19 +705,53 @@ template <int KK, int R1, int SRC, int I, int N>
 struct TernRounds {
   static __device__ __forceinline__ void run(uint32_t *work,
                                              const TmaArgs &a, long long r0,
-                                             bool two, uint32_t plo,
-                                             uint32_t pspan) {
-    tern_round<KK, R1, SRC, I>(work, a, r0, two, plo, pspan);
+                                             bool two, bool wide,
+                                             uint32_t plo, uint32_t pspan) {
+    tern_round<KK, R1, SRC, I>(work, a, r0, two, wide, plo, pspan);
     __syncthreads();
-    TernRounds<KK, R1, SRC, I + 1, N>::run(work, a, r0, two, plo, pspan);
+    TernRounds<KK, R1, SRC, I + 1, N>::run(work, a, r0, two, wide, plo,
+                                           pspan);
   }
 };
 template <int KK, int R1, int SRC, int N>
 struct TernRounds<KK, R1, SRC, N, N> {
   static __device__ __forceinline__ void run(uint32_t *, const TmaArgs &,
-                                             long long, bool, uint32_t,
+                                             long long, bool, bool, uint32_t,
                                              uint32_t) {}
 };
+
+// Wide stores of a tile's layers (a row pitch that is a multiple of 8
+// words and at least T0 rounded up to 8): each thread takes 8 positions of
+// one layer from the buffer (two 16-byte shared loads of packed lanes) and
+// stores each row's 8 words with one 16-byte store.  Positions from T0 to
+// the next multiple of 8 land in the row's padding.
+template <int KK, int R1>
+__device__ __forceinline__ void tern_copy_out(const uint32_t *work,
+                                              const TmaArgs &a, long long r0,
+                                              bool two) {
+  constexpr int T0 = P<3, KK>::v;
+  constexpr int WS = (T0 + 31) / 32 * 32;
+  constexpr int C8 = (T0 + 7) / 8;
+  static_assert(C8 * 8 <= WS, "the buffer covers the rounded row");
+  const int n = a.lout * C8;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int d = i / C8, m = (i - d * C8) * 8;
+    const uint4 x = *reinterpret_cast<const uint4 *>(work + d * WS + m);
+    const uint4 y = *reinterpret_cast<const uint4 *>(work + d * WS + m + 4);
+    uint16_t *q = a.layers16 + d * a.plane + r0 * a.pitch + m;
+    __stcs(reinterpret_cast<uint4 *>(q),
+           make_uint4(__byte_perm(x.x, x.y, 0x5410),
+                      __byte_perm(x.z, x.w, 0x5410),
+                      __byte_perm(y.x, y.y, 0x5410),
+                      __byte_perm(y.z, y.w, 0x5410)));
+    if (two)
+      __stcs(reinterpret_cast<uint4 *>(q + a.pitch),
+             make_uint4(__byte_perm(x.x, x.y, 0x7632),
+                        __byte_perm(x.z, x.w, 0x7632),
+                        __byte_perm(y.x, y.y, 0x7632),
+                        __byte_perm(y.z, y.w, 0x7632)));
+  }
+}
 
 // SRC 0: the cnt predicate (gain, loss); 1: the sorted code (a recount),
 // the tile's slice [bounds[t], bounds[t+1]) counted into layer 0 first
@@ -727,6 +768,10 @@ tern_first(const TmaArgs a) {
                        : a.pmode == kPredCrit ? (uint32_t)a.mu
                        : (uint32_t)a.ptarget;
   const uint32_t pspan = phi - plo;
+  constexpr int C8 = (T0 + 7) / 8;
+  const bool wide = (a.pitch & 7) == 0 && a.pitch >= C8 * 8 &&
+                    (a.plane & 7) == 0 &&
+                    (reinterpret_cast<uintptr_t>(a.layers16) & 15) == 0;
   for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const long long r0 = 2 * t;
     const bool two = r0 + 1 < a.rows;
@@ -743,7 +788,11 @@ tern_first(const TmaArgs a) {
       }
       __syncthreads();
     }
-    TernRounds<KK, R1, SRC, 0, NR>::run(work, a, r0, two, plo, pspan);
+    TernRounds<KK, R1, SRC, 0, NR>::run(work, a, r0, two, wide, plo, pspan);
+    if (wide) {
+      tern_copy_out<KK, R1>(work, a, r0, two);
+      __syncthreads();                  // the buffer is the next tile's
+    }
   }
 }
 
