@@ -74,6 +74,12 @@ int occupancy_grid(const GroupPlan &p) {
   return (int)std::max<long long>(1, grid);
 }
 
+// streamed launches sized once, at planning, not at every launch
+void size_streamed(std::vector<GroupPlan> &groups) {
+  for (auto &gp : groups)
+    if (gp.a.tma && gp.grid < 1) gp.grid = occupancy_grid(gp);
+}
+
 // Distance layers that can be nonzero after axes 0..j-1: each Hamming axis
 // adds at most 1 to the distance, each Lee axis at most floor(a/2).
 int live_layers(const Geometry &g, const AxisRange &r, int j) {
@@ -389,6 +395,7 @@ bool pad_plan(std::vector<GroupPlan> &groups, const Geometry &g,
     f = tern_first_variant(fv, 256);
   groups.resize(1);
   groups.insert(groups.end(), later.begin(), later.end());
+  size_streamed(groups);
   return true;
 }
 
@@ -415,6 +422,7 @@ void stream_groups(std::vector<GroupPlan> &groups, int R1) {
         }
       }
   }
+  size_streamed(groups);
 }
 
 // Algorithmic HBM bytes of one group launch: every word of the space read
@@ -482,6 +490,8 @@ bool u8_plan(std::vector<GroupPlan> &groups, int R1, long long room16) {
   if (!done) return false;
   groups[0] = f8;
   groups[1] = n8;
+  groups[0].grid = groups[1].grid = 0;
+  size_streamed(groups);
   return true;
 }
 

@@ -30,7 +30,9 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstring>
 #include <mutex>
+#include <unordered_map>
 
 #include "engine.h"
 
@@ -1255,6 +1257,49 @@ int launch_tma_first(const GroupPlan &p, cudaStream_t s) {
   return 0;
 }
 
+namespace {
+
+// tensor-map parameters of one streamed launch (the map is a pure function
+// of them)
+struct MapKey {
+  const void *base;
+  cuuint64_t dims[4], strides[3];
+  cuuint32_t box[4];
+  int dt;
+  bool operator==(const MapKey &o) const {
+    return std::memcmp(this, &o, sizeof(MapKey)) == 0;
+  }
+};
+struct MapKeyHash {
+  size_t operator()(const MapKey &k) const {
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(&k);
+    size_t h = 1469598103934665603ULL;
+    for (size_t i = 0; i < sizeof(MapKey); i++) {
+      h ^= b[i];
+      h *= 1099511628211ULL;
+    }
+    return h;
+  }
+};
+std::mutex g_map_mu;
+std::unordered_map<MapKey, CUtensorMap, MapKeyHash> g_maps;
+
+bool map_cache_get(const MapKey &k, CUtensorMap *m) {
+  std::lock_guard<std::mutex> g(g_map_mu);
+  auto it = g_maps.find(k);
+  if (it == g_maps.end()) return false;
+  *m = it->second;
+  return true;
+}
+
+void map_cache_put(const MapKey &k, const CUtensorMap &m) {
+  std::lock_guard<std::mutex> g(g_map_mu);
+  if (g_maps.size() >= 4096) g_maps.clear();   // freed planes' stale keys
+  g_maps[k] = m;
+}
+
+}  // namespace
+
 int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   if (p.a.tma == 3) return launch_tern_first(p, s);
   if (p.a.tma == 2) return launch_tma_first(p, s);
@@ -1285,17 +1330,27 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   void *gbase = a.in8 ? (void *)(reinterpret_cast<uint8_t *>(a.layers16) +
                                  a.off8)
                       : (void *)a.layers16;
-  const CUresult cr = enc(&map, a.in8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
-                                      : CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
-                          gbase, dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (cr != CUDA_SUCCESS) {
-    fprintf(stderr, "coldcore_b200: tensor map encode failed (%d)\n",
-            (int)cr);
-    return -9;
+  // the encoded maps of earlier launches, by their parameters: a plan's
+  // launches repeat every transform, and the encode is host work
+  MapKey key{};
+  key.base = gbase;
+  key.dt = a.in8 ? 1 : 2;
+  for (int i = 0; i < 4; i++) key.dims[i] = dims[i], key.box[i] = box[i];
+  for (int i = 0; i < 3; i++) key.strides[i] = strides[i];
+  if (!map_cache_get(key, &map)) {
+    const CUresult cr = enc(&map, a.in8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                        : CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+                            gbase, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) {
+      fprintf(stderr, "coldcore_b200: tensor map encode failed (%d)\n",
+              (int)cr);
+      return -9;
+    }
+    map_cache_put(key, map);
   }
   TmaArgs t{};
   t.layers16 = a.layers16;
