@@ -78,8 +78,18 @@ __global__ void k_batch_bounds(const BoundsJob *jobs) {
 // Cells of at least 2^16 words whose axes all have one size with a
 // register-blocked kernel run as their own launches (captured on forked
 // streams of the same graph); smaller cells share the persistent kernel.
-constexpr long long kBigCell = 1LL << 16;
-constexpr long long kItemWords = 32768;   // words per work item (at least)
+// (CC_BATCH_BIG: log2 of that threshold; CC_BATCH_ITEM: the words of one
+// work item of the persistent kernel, at least)
+long long big_cell_words() {
+  const char *e = getenv("CC_BATCH_BIG");
+  const int lg = e ? atoi(e) : 16;
+  return 1LL << (lg < 8 ? 8 : lg > 40 ? 40 : lg);
+}
+long long item_words() {
+  const char *e = getenv("CC_BATCH_ITEM");
+  const long long w = e ? atoll(e) : 32768;
+  return w < 256 ? 256 : w;
+}
 // side streams the big cells are spread over (CC_BATCH_STREAMS, 1..16,
 // default 4: 4, 8 and 16 timed within 3% of each other on the 256-cell
 // campaign), largest cells first onto the least loaded stream
@@ -407,7 +417,7 @@ int make_schedule(Batch *b) {
     for (int pid : lv) {
       const GroupArgs &a = b->passes[pid];
       const long long tw = (long long)a.Bo * a.mid * a.W;
-      const long long per = std::max<long long>(1, kItemWords / tw);
+      const long long per = std::max<long long>(1, item_words() / tw);
       for (long long t = 0; t < a.ntiles; t += per)
         items.push_back(make_int4(pid, (int)t,
                                   (int)std::min<long long>(per, a.ntiles - t),
@@ -621,7 +631,7 @@ int dct_batch_add(long long h, int problem, int n, const int *ax, int R,
   bool homog = true;
   for (int i = 1; i < n; i++) homog &= ax[i] == ax[0];
   int bm = 0;
-  c.big = c.g.space >= kBigCell && homog &&
+  c.big = c.g.space >= big_cell_words() && homog &&
           pick_group_kernel(problem, ax[0], c.R1, &bm) >= 0;
   b->cells.push_back(std::move(c));
   return (int)b->cells.size() - 1;
