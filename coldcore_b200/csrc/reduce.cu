@@ -43,8 +43,23 @@ k_cnt_reduce(const uint16_t *cnt, long long N, int mode, int target, int mu,
   const long long gs = (long long)gridDim.x * blockDim.x;
   const uint4 *v = reinterpret_cast<const uint4 *>(cnt);
   long long acc = 0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-       i < nvec; i += gs) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // four independent 16-byte loads in flight per thread, then the rest
+  for (; i + 3 * gs < nvec; i += 4 * gs) {
+    uint4 q[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) q[u] = v[i + u * gs];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t w4[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+#pragma unroll
+      for (int h = 0; h < 8; h++)
+        acc += cnt_term(mode,
+                        (int)((w4[h >> 1] >> (16 * (h & 1))) & 0xFFFFu),
+                        target, mu);
+    }
+  }
+  for (; i < nvec; i += gs) {
     const uint4 q = v[i];
     const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
@@ -65,8 +80,16 @@ k_max(const int32_t *A, long long N, long long *out) {
   const long long gs = (long long)gridDim.x * blockDim.x;
   const int4 *v = reinterpret_cast<const int4 *>(A);
   int32_t m = 0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-       i < nvec; i += gs) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * gs < nvec; i += 4 * gs) {
+    int4 q[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) q[u] = v[i + u * gs];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      m = max(m, max(max(q[u].x, q[u].y), max(q[u].z, q[u].w)));
+  }
+  for (; i < nvec; i += gs) {
     const int4 q = v[i];
     m = max(m, max(max(q.x, q.y), max(q.z, q.w)));
   }
