@@ -79,8 +79,9 @@ def measure(axes=None, R=3, budget_gb=8.0, code_words=100000, reps=3):
             "link_measured_GBps": rates,
             "link_floor_ms": round(floor_ms, 3),
             "frac_of_link_floor": round(floor_ms / best, 3),
+            # the K_10(10,5) link bytes at this leg's achieved link rate
             "projection_K10_10_5_s": round(
-                k10_link / (plan["link_bytes"] / best / 1e3), 1),
+                k10_link / (plan["link_bytes"] / (best * 1e-3)), 2),
             "reference_K10_10_5_s": "73-110 (GH200, C2C)"}
 
 
