@@ -565,6 +565,15 @@ int run_transform(int init_mode, int out_mode) {
   return 0;
 }
 
+// CC_TUNE_LOG=1: every timed variant of the per-launch tuning on stderr
+bool tune_log() {
+  static const bool on = [] {
+    const char *e = getenv("CC_TUNE_LOG");
+    return e && atoi(e) == 1;
+  }();
+  return on;
+}
+
 // Per-launch tuning of plan P with its grouping fixed: every register block
 // size, row width, prefetching form and CTA width of each launch, each
 // timed alone (three launches after a warm one).  A launch run again works
@@ -607,6 +616,12 @@ int tune_launches(Plan &P, int init_mode, int out_mode, cudaEvent_t e0,
       float ms = 0;
       CC_CK(cudaEventElapsedTime(&ms, e0, e1));
       if (ms < bv) { bv = ms; bi = vi; }
+      if (tune_log())
+        fprintf(stderr, "CC_TUNE_LOG transform(%d,%d) group %zu variant %zu: "
+                "kernel %d tma %d stages %d W %d threads %d grid %d smem %zu "
+                "pipe %d in8 %d out8 %d: %.4f ms\n", init_mode, out_mode, gi,
+                vi, p.kernel, p.a.tma, p.a.stages, p.a.W, p.threads, p.grid,
+                p.smem, p.a.pipe, p.a.in8, p.a.out8, ms / 3);
     }
     P.groups[gi] = vars[bi];
   }
