@@ -41,6 +41,7 @@ struct Cell {
   int first_pass = 0, npass = 0;     // global pass range (small cells)
   bool big = false;                  // own register-blocked launches
   int side = 0;                      // its side stream (big cells)
+  bool tuned = false;                // fast[] tuned (big cells)
   std::vector<GroupPlan> fast[3];    // recount, gain, loss (big cells)
   // codes may be replaced between launches (dct_batch_set_code): the
   // device buffer holds code_cap words, its length lives on the device
@@ -251,6 +252,72 @@ void release(Batch *b) {
 }
 
 // passes + level-ordered work table for the current tile budget
+// Per-launch tuning of the cells with their own launches, as the singleton
+// tunes its plan: every variant group_variants offers for a launch (register
+// block, row width, prefetching, streamed form, CTA width) is timed on the
+// batch stream (three launches after a warm one) and the fastest is kept.
+// Cells of at least 2^CC_BATCH_TUNE words (default 20; 0 turns it off, as
+// does CC_TUNE=0), once per batch.  A variant run again works in place on
+// the cell's planes, which only scrambles values; every step recomputes
+// from the code.
+int tune_big_cells(Batch *b) {
+  const char *te = getenv("CC_TUNE");
+  if (te && atoi(te) == 0) return 0;
+  const char *be = getenv("CC_BATCH_TUNE");
+  const int lg = be ? atoi(be) : 20;
+  if (lg <= 0) return 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CC_CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    cudaGetLastError();
+    return -1;
+  }
+  int rc = 0;
+  for (Cell &c : b->cells) {
+    if (rc) break;
+    if (!c.big || c.tuned || c.g.space < (1LL << lg) || c.fast[0].empty())
+      continue;
+    // the recount's first group reads its code slices: bounds for its tiles
+    const GroupArgs &a0 = c.fast[0][0].a;
+    rc = launch_code_bounds(c.dcode, (long long)c.code.size(),
+                            (long long)a0.Bo * a0.mid * a0.inner, a0.ntiles,
+                            c.bounds, b->stream);
+    for (int t = 0; t < 3 && !rc; t++)
+      for (size_t gi = 0; gi < c.fast[t].size() && !rc; gi++) {
+        const std::vector<GroupPlan> vars =
+            group_variants(c.fast[t][gi], c.R1, 220 << 10);
+        if (vars.size() < 2) continue;
+        float bv = 1e30f;
+        size_t bi = 0;
+        for (size_t vi = 0; vi < vars.size() && !rc; vi++) {
+          const GroupPlan &v = vars[vi];
+          if ((rc = prepare_group(v))) break;
+          rc = launch_group(v, b->stream);
+          if (rc == -9) { rc = 0; continue; }   // a form the launcher refused
+          if (rc) break;
+          if (cudaEventRecord(e0, b->stream) != cudaSuccess) { rc = -1; break; }
+          for (int r = 0; r < 3 && !rc; r++) rc = launch_group(v, b->stream);
+          if (rc) break;
+          float ms = 0;
+          if (cudaEventRecord(e1, b->stream) != cudaSuccess ||
+              cudaEventSynchronize(e1) != cudaSuccess ||
+              cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = -1;
+            break;
+          }
+          if (ms < bv) { bv = ms; bi = vi; }
+        }
+        if (!rc) c.fast[t][gi] = vars[bi];
+      }
+    c.tuned = !rc;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc == -1) cudaGetLastError();
+  return rc;
+}
+
 int make_schedule(Batch *b) {
   b->passes.clear();
   b->dep.clear();
@@ -263,6 +330,7 @@ int make_schedule(Batch *b) {
     Cell &c = b->cells[i];
     c.first_pass = (int)b->passes.size();
     c.npass = 0;
+    if (c.big && c.tuned) continue;     // its tuned launches stand
     if (c.big) {
       // 16-bit planes between launches (and packed pairs where the
       // planner can) when every layer value stays below 2^16: always for
@@ -381,6 +449,10 @@ int make_schedule(Batch *b) {
     if (c.big)
       for (int t = 0; t < 3; t++)
         for (auto &gp : c.fast[t]) gp.a.code_bounds = c.bounds;
+  }
+  {
+    const int rc = tune_big_cells(b);
+    if (rc) return rc;
   }
   // the bounds job of every cell (its first group's tiles)
   std::vector<BoundsJob> jobs;
