@@ -534,9 +534,22 @@ int run_big_cell(Batch *b, size_t i, cudaStream_t s) {
   Cell &c = b->cells[i];
   int rc = 0;
   for (int t = 0; t < 3; t++) {
-    for (const auto &gp : c.fast[t])
-      if ((rc = launch_group(gp, s))) return rc;
     long long *slot = b->d_scal + 3 * i + t;
+    // the deficit count (recount) or the map maximum folded into the last
+    // launch where its kernel reduces what it writes (a register kernel or
+    // a streamed strided group); else a separate reduction pass
+    bool folded = false;
+    for (size_t k = 0; k < c.fast[t].size(); k++) {
+      GroupPlan gp = c.fast[t][k];
+      if (k + 1 == c.fast[t].size() && gp.a.dst != kDstLayers &&
+          (gp.a.tma == 1 || (gp.a.tma == 0 && gp.kernel >= 0))) {
+        gp.a.red = slot;
+        gp.a.red_mode = t == 0 ? 1 : 2;
+        folded = true;
+      }
+      if ((rc = launch_group(gp, s))) return rc;
+    }
+    if (folded) continue;
     rc = t == 0 ? launch_cnt_reduce(c.cnt, c.g.space, kPredDef, 0, c.g.mu,
                                     slot, s)
                 : launch_max(t == 1 ? c.gain : c.loss, c.g.space, slot, s);

@@ -85,7 +85,8 @@ struct GroupArgs {
   // first group of a binary Hamming cell: axis 0 is the word pair itself
   // (inner = 2), applied once as a swap-add inside each packed lane
   int pair_axis;
-  long long *red;         // epilogue reduction target (generic tiles)
+  long long *red;         // epilogue reduction target (generic tiles, the
+                          // register kernels and the streamed groups)
   int red_mode;           // 0 none, 1 deficit of the cnt written, 2 map max
   // streamed form (transform_tma.cu): tensor loads into `stages` shared
   // memory stages, W = 2 x lanes inner words a tile (tma 1); the first
@@ -126,6 +127,9 @@ struct TmaArgs {
   long long rows;
   // 8-bit layer planes (tma_first OUT 5): their byte offset from layers16
   long long off8;
+  // epilogue reduction of a map or cnt written (GroupArgs::red_mode)
+  long long *red;
+  int red_mode;
 };
 
 struct GroupPlan {

@@ -224,12 +224,39 @@ enum RoundIo { kIoSmem = 0, kIoLayers = 1, kIoCnt = 2, kIoCode = 3,
 // 2^16 (the planner's 16-bit bound) and the inner stride is even, so a pair
 // never straddles a row; the group's HBM sides are u16 planes (one 32-bit
 // access per pair), the int32 map and the u16 cnt (unpacked at the store).
+// Epilogue reductions of a launch's output (GroupArgs::red_mode): 2 the
+// maximum of the map written (0 when no value is positive), 1 the deficit
+// sum max(0, mu - c) of the cnt written.  Per thread, then per warp, one
+// 64-bit atomic.
+__device__ __forceinline__ void red_map(long long *acc, long long a,
+                                        long long b) {
+  const long long m = a > b ? a : b;
+  if (m > *acc) *acc = m;
+}
+__device__ __forceinline__ void red_def(long long *acc, int mu, int c0,
+                                        int c1) {
+  *acc += (c0 < mu ? mu - c0 : 0) + (c1 < mu ? mu - c1 : 0);
+}
+__device__ __forceinline__ void red_flush(const GroupArgs &g, long long acc) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long other = __shfl_down_sync(0xffffffffu, acc, o);
+    acc = g.red_mode == 2 ? (other > acc ? other : acc) : acc + other;
+  }
+  if ((threadIdx.x & 31) == 0 && acc) {
+    if (g.red_mode == 2)
+      atomicMax((unsigned long long *)g.red, (unsigned long long)acc);
+    else
+      atomicAdd((unsigned long long *)g.red, (unsigned long long)acc);
+  }
+}
+
 template <int OP, int Q, int R1, int BM, bool FULL, bool PACK = false>
 __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
                                           int SD, long long o0, long long i0,
                                           int rb, int S, int src, int dst,
                                           int nl = R1,
-                                          const uint16_t *cs = nullptr) {
+                                          const uint16_t *cs = nullptr,
+                                          long long *racc = nullptr) {
   constexpr int QB = IPow<Q, BM>::v;
   int ne = QB;
   if (!FULL) { ne = 1; for (int t = 0; t < rb; t++) ne *= Q; }
@@ -395,6 +422,7 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
           for (int d = 0; d < R1; d++) s += (uint32_t)v[d][e];
           __stcs(reinterpret_cast<int2 *>(p),
                  make_int2((int)(s & 0xFFFFu), (int)(s >> 16)));
+          if (racc) red_map(racc, (long long)(s & 0xFFFFu), (long long)(s >> 16));
           p += gstep;
         }
       } else if (PACK) {                         // cnt: both halves at once
@@ -406,6 +434,7 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
 #pragma unroll
           for (int d = 0; d < R1; d++) s += (uint32_t)v[d][e];
           *reinterpret_cast<uint32_t *>(p) = s;
+          if (racc) red_def(racc, g.mu, (int)(s & 0xFFFFu), (int)(s >> 16));
           p += gstep;
         }
       } else if (dst == kIoLayers && g.out16) {
@@ -447,6 +476,7 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
 #pragma unroll
           for (int d = 0; d < R1; d++) s += v[d][e];
           __stcs(p, s);
+          if (racc) red_map(racc, (long long)s, 0);
           p += gstep;
         }
       } else {
@@ -458,6 +488,7 @@ __device__ __forceinline__ void run_round(const GroupArgs &g, int32_t *sm,
 #pragma unroll
           for (int d = 0; d < R1; d++) s += v[d][e];
           *p = (uint16_t)(s > 65535 ? 65535 : s);
+          if (racc) red_def(racc, g.mu, s > 65535 ? 65535 : s, g.mu);
           p += gstep;
         }
       }
@@ -483,20 +514,21 @@ template <int OP, int Q, int R1, int B, bool PACK = false>
 struct RoundSel {
   static __device__ __forceinline__ void run(
       const GroupArgs &g, int32_t *sm, int SD, long long o0, long long i0,
-      int rb, int S, int src, int dst, int nl, const uint16_t *cs) {
+      int rb, int S, int src, int dst, int nl, const uint16_t *cs,
+      long long *racc = nullptr) {
     if (rb == B)
       run_round<OP, Q, R1, B, true, PACK>(g, sm, SD, o0, i0, B, S, src, dst,
-                                          nl, cs);
+                                          nl, cs, racc);
     else
       RoundSel<OP, Q, R1, B - 1, PACK>::run(g, sm, SD, o0, i0, rb, S, src,
-                                            dst, nl, cs);
+                                            dst, nl, cs, racc);
   }
 };
 template <int OP, int Q, int R1, bool PACK>
 struct RoundSel<OP, Q, R1, 0, PACK> {
   static __device__ __forceinline__ void run(
       const GroupArgs &, int32_t *, int, long long, long long, int, int, int,
-      int, int, const uint16_t *) {}
+      int, int, const uint16_t *, long long * = nullptr) {}
 };
 
 template <int OP, int Q, int R1, int BM>
@@ -511,6 +543,8 @@ group_kernel(const GroupArgs g) {
                         : g.src == kSrcCnt ? kIoCnt : kIoCode;
   const int last_dst = g.dst == kDstLayers ? kIoLayers
                        : g.dst == kDstMap ? kIoMap : kIoCntOut;
+  long long acc = 0;                    // epilogue reduction (red_mode)
+  long long *racc = g.red_mode && g.dst != kDstLayers ? &acc : nullptr;
   for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
     const long long o0 = (tile / g.nchunk) * g.Bo;
     const long long i0 = (tile % g.nchunk) * W;
@@ -531,13 +565,15 @@ group_kernel(const GroupArgs g) {
       const int dst = r == g.nrounds - 1 ? last_dst : kIoSmem;
       if (g.pack)
         RoundSel<OP, Q, R1, BM, true>::run(g, sm, SD, o0, i0, g.rb[r],
-                                           g.rs[r], src, dst, R1, nullptr);
+                                           g.rs[r], src, dst, R1, nullptr,
+                                           racc);
       else
         RoundSel<OP, Q, R1, BM>::run(g, sm, SD, o0, i0, g.rb[r], g.rs[r],
-                                     src, dst, R1, nullptr);
+                                     src, dst, R1, nullptr, racc);
       __syncthreads();
     }
   }
+  if (racc) red_flush(g, acc);
 }
 
 // --------------------------------------------------------- pipelined kernel
@@ -658,6 +694,8 @@ group_kernel_pipe(const GroupArgs g) {
   uint16_t *const cb1 = cb0 + cbw;
   const int last_dst = g.dst == kDstLayers ? kIoLayers
                        : g.dst == kDstMap ? kIoMap : kIoCntOut;
+  long long acc = 0;                    // epilogue reduction (red_mode)
+  long long *racc = g.red_mode && g.dst != kDstLayers ? &acc : nullptr;
   int off0 = 0, off1 = 0;
   long long tile = blockIdx.x;
   if (tile < g.ntiles) {
@@ -692,14 +730,16 @@ group_kernel_pipe(const GroupArgs g) {
       const int nl = r > 0 ? R1 : g.lin;
       if (pk)
         RoundSel<OP, Q, R1, BM, kPackable>::run(g, buf, SD, o0, i0, g.rb[r],
-                                                g.rs[r], src, dst, nl, cs);
+                                                g.rs[r], src, dst, nl, cs,
+                                                racc);
       else
         RoundSel<OP, Q, R1, BM>::run(g, buf, SD, o0, i0, g.rb[r], g.rs[r],
-                                     src, dst, nl, cs);
+                                     src, dst, nl, cs, racc);
       __syncthreads();
     }
   }
   cp_wait_all();
+  if (racc) red_flush(g, acc);
 }
 
 // ------------------------------------------------------------ generic kernel

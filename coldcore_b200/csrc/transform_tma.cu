@@ -146,6 +146,20 @@ struct RoundAxes {
                            : (P<Q, 2>::v * R1 <= 64) ? 2 : 1;
 };
 
+// Epilogue reductions of a streamed launch's output (TmaArgs::red_mode): 2
+// the map maximum, 1 the deficit sum max(0, mu - c) of the cnt written; a
+// packed lane's two words, each only where it is a word of the cell.
+__device__ __forceinline__ void tma_red(long long *acc, const TmaArgs &a,
+                                        int w0, int w1, bool ok0, bool ok1) {
+  if (a.red_mode == 2) {
+    if (ok0 && w0 > *acc) *acc = w0;
+    if (ok1 && w1 > *acc) *acc = w1;
+  } else {
+    if (ok0 && w0 < a.mu) *acc += a.mu - w0;
+    if (ok1 && w1 < a.mu) *acc += a.mu - w1;
+  }
+}
+
 // ------------------------------------------------------------ one round
 // Round over axes [A, A + B) of the group on a stage of L lanes x MID mid
 // positions x R1 layers (32-bit packed lanes, layer-major as the tensor
@@ -155,7 +169,8 @@ template <int Q, int K, int R1, int L, int OUT, int A, int B, bool FIRST,
           bool LAST, bool IN8 = false>
 __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
                                           long long o, long long i0,
-                                          const uint16_t *s8 = nullptr) {
+                                          const uint16_t *s8 = nullptr,
+                                          long long *racc = nullptr) {
   constexpr int MID = P<Q, K>::v;
   constexpr int QB = P<Q, B>::v;
   constexpr int QA = P<Q, A>::v;
@@ -219,6 +234,8 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
                  make_int2((int)(s & 0xFFFFu), (int)(s >> 16)));
         else
           *reinterpret_cast<unsigned *>(a.cnt + x0 + e * step) = s;
+        if (racc)
+          tma_red(racc, a, (int)(s & 0xFFFFu), (int)(s >> 16), true, true);
       }
     } else {
       // OUT 3 (map) / 4 (cnt) of a padded plan: the pair's words j', j'+1
@@ -241,6 +258,7 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
           if (ok0) a.cnt[x] = (uint16_t)(s & 0xFFFFu);
           if (ok1) a.cnt[x + 1] = (uint16_t)(s >> 16);
         }
+        if (racc) tma_red(racc, a, (int)(s & 0xFFFFu), (int)(s >> 16), ok0, ok1);
       }
     }
   }
@@ -254,19 +272,21 @@ struct Rounds {
   static constexpr int B = (K - A) < BM ? (K - A) : BM;
   static __device__ __forceinline__ void run(uint32_t *st, const TmaArgs &a,
                                              long long o, long long i0,
-                                             const uint16_t *s8 = nullptr) {
+                                             const uint16_t *s8 = nullptr,
+                                             long long *racc = nullptr) {
     tma_round<Q, K, R1, L, OUT, A, B, A == 0, A + B == K, IN8>(st, a, o, i0,
-                                                              s8);
+                                                              s8, racc);
     if (A + B < K) __syncthreads();
     Rounds<Q, K, R1, L, OUT, (A + B < K ? A + B : K), IN8>::run(st, a, o, i0,
-                                                                s8);
+                                                                s8, racc);
   }
 };
 template <int Q, int K, int R1, int L, int OUT, bool IN8>
 struct Rounds<Q, K, R1, L, OUT, K, IN8> {
   static __device__ __forceinline__ void run(uint32_t *, const TmaArgs &,
                                              long long, long long,
-                                             const uint16_t *) {}
+                                             const uint16_t *,
+                                             long long * = nullptr) {}
 };
 
 // stage stride: the tile's words rounded up to 1 KB (tensor loads land on
@@ -301,6 +321,8 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
       base + (size_t)S * SB + (IN8 ? (size_t)SW * 4 : 0));
   volatile int *stop = reinterpret_cast<volatile int *>(bar + kTmaMaxStages);
   const uint32_t bytes = (uint32_t)(2 * L * (IN8 ? 1 : 2)) * MID * a.lin;
+  long long acc = 0;                    // epilogue reduction (red_mode)
+  long long *racc = (OUT != 0 && a.red_mode) ? &acc : nullptr;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; s++) mbar_init(&bar[s]);
     *stop = 0;
@@ -336,10 +358,11 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
     if (IN8)
       Rounds<Q, K, R1, L, OUT, 0, IN8>::run(
           work, a, o, i0,
-          reinterpret_cast<const uint16_t *>(stage + (size_t)s * SB));
+          reinterpret_cast<const uint16_t *>(stage + (size_t)s * SB), racc);
     else
       Rounds<Q, K, R1, L, OUT, 0>::run(
-          reinterpret_cast<uint32_t *>(stage + (size_t)s * SB), a, o, i0);
+          reinterpret_cast<uint32_t *>(stage + (size_t)s * SB), a, o, i0,
+          nullptr, racc);
     __syncthreads();                          // stage s is free again
     if (threadIdx.x == 0) {
       const long long nt = t + S * grid;
@@ -360,6 +383,18 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
       const long long tk = blockIdx.x + k * grid;
       if (tk >= a.ntiles) break;
       mbar_wait(&bar[k % S], (uint32_t)((k / S) & 1), kTmaDrainNs);
+    }
+  }
+  if (racc) {
+    for (int o2 = 16; o2 > 0; o2 >>= 1) {
+      const long long other = __shfl_down_sync(0xffffffffu, acc, o2);
+      acc = a.red_mode == 2 ? (other > acc ? other : acc) : acc + other;
+    }
+    if ((threadIdx.x & 31) == 0 && acc) {
+      if (a.red_mode == 2)
+        atomicMax((unsigned long long *)a.red, (unsigned long long)acc);
+      else
+        atomicAdd((unsigned long long *)a.red, (unsigned long long)acc);
     }
   }
 }
@@ -1367,6 +1402,9 @@ int launch_tma_group(const GroupPlan &p, cudaStream_t s) {
   t.pitch = a.pitch;
   t.t0 = a.t0;
   t.inner_c = a.pitch ? a.inner / a.pitch * a.t0 : a.inner;
+  t.mu = a.mu;
+  t.red = a.red;
+  t.red_mode = a.dst != kDstLayers && a.red ? a.red_mode : 0;
   const size_t smem = tma_smem_bytes(q, a.k, a.R + 1, lanes, a.stages,
                                      a.in8);
   int grid = p.grid;
