@@ -347,12 +347,13 @@ int make_schedule(Batch *b) {
         ptr.layers16 = reinterpret_cast<uint16_t *>(c.layers + c.plane);
         const int src = t == 0 ? kSrcCode : kSrcCnt;
         const int dst = t == 0 ? kDstCnt : kDstMap;
-        c.fast[t] = plan_groups(c.g, c.R1, ptr, src, dst, kn);
+        const Geometry tg = transform_geometry(c.g);
+        c.fast[t] = plan_groups(tg, c.R1, ptr, src, dst, kn);
         // the streamed forms where they apply (CC_TMA=0 keeps the
         // register kernels): a ternary cell's padded plan, else every
         // group a streamed form serves
         if (!streams_off && kn.half &&
-            !pad_plan(c.fast[t], c.g, ptr, dst, c.R1,
+            !pad_plan(c.fast[t], tg, ptr, dst, c.R1,
                       (long long)(c.R1 - 1) * c.plane * 2)) {
           stream_groups(c.fast[t], c.R1);
           u8_plan(c.fast[t], c.R1, (long long)(c.R1 - 1) * c.plane * 2);

@@ -169,6 +169,17 @@ std::vector<GroupPlan> plan_groups(const Geometry &g, int R1,
                                    Knobs kn, AxisRange range = AxisRange());
 // distance reach of one axis: 1 for Hamming, floor(a/2) for Lee
 inline long long axis_reach(int prob, int a) { return prob == kLee ? a / 2 : 1; }
+// The transform geometry of a cell: Lee distance on axes of size 2 or 3 is
+// the Hamming distance (every nonzero digit difference has weight
+// min(d, q - d) = 1), so such a cell plans and runs as Hamming, with the
+// Hamming kernels' streamed forms.
+inline Geometry transform_geometry(Geometry g) {
+  if (g.prob != kLee) return g;
+  for (int j = 0; j < g.n; j++)
+    if (g.ax[j] > 3) return g;
+  g.prob = kHamming;
+  return g;
+}
 
 // launchers (transform_*.cu)
 int launch_group(const GroupPlan &p, cudaStream_t s);

@@ -348,7 +348,7 @@ Plan build_group_plan(int src, int dst, Knobs kn) {
   PlanPtrs ptr{S.layers, S.plane, S.cnt, S.d_code, S.codeM, nullptr};
   kn.half = half_planes_ok(src, dst) ? 1 : 0;
   ptr.layers16 = reinterpret_cast<uint16_t *>(S.layers + S.plane);
-  Geometry g = S.g;
+  Geometry g = transform_geometry(S.g);
   g.mu = g_mu;
   P.groups = plan_groups(g, S.R1, ptr, src, dst, kn);
   if (kn.pad) {
@@ -1683,6 +1683,7 @@ int dct_b200_plan_probe(int problem, int n, const int *ax, int R,
     g.pw[i + 1] = g.pw[i] * ax[i];
   }
   g.space = g.pw[n];
+  g = transform_geometry(g);                  // as a cell would plan it
   bool wide = false;
   for (int i = 0; i < n; i++) wide = wide || ax[i] > 16;
   if (!layered && wide) return 0;             // window passes, not groups

@@ -56,6 +56,10 @@ def live_layers(problem, axes, j, R):
 
 def check_plan(plan, problem, axes, R, mode, budget_kb, pipe, half):
     layered = problem in ("hamming", "lee")
+    # Lee distance on axes of size 2 or 3 is the Hamming distance: such a
+    # cell is planned as Hamming (transform_geometry)
+    if problem == "lee" and max(axes) <= 3:
+        problem = "hamming"
     R1 = R + 1 if layered else 1
     n = len(axes)
     space = math.prod(axes)
