@@ -659,7 +659,9 @@ int autotune(int init_mode, int out_mode) {
                                 {100 << 10, 2}, {100 << 10, 3},
                                 {200 << 10, 3}, {160 << 10, 2},
                                 {200 << 10, 2},
-                                // padded plans (ternary cells)
+                                // padded plans (ternary cells); 32 KB
+                                // gives a six-axis first group
+                                {32 << 10, 1, 0, 1, 1},
                                 {64 << 10, 1, 0, 1, 1},
                                 {100 << 10, 1, 0, 1, 1},
                                 {160 << 10, 1, 0, 1, 1},
@@ -694,6 +696,14 @@ int autotune(int init_mode, int out_mode) {
     CC_CK(cudaEventSynchronize(e1));
     float ms = 0;
     CC_CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (tune_log()) {
+      fprintf(stderr, "CC_TUNE_LOG transform(%d,%d) plan budget %zu KB pipe "
+              "%d pad %d u8 %d axes", init_mode, out_mode, kn.budget >> 10,
+              kn.pipe, kn.pad, kn.u8);
+      for (const auto &gp : P.groups)
+        fprintf(stderr, " %d", gp.a.k + gp.a.pair_axis);
+      fprintf(stderr, ": %.4f ms\n", ms / 2);
+    }
     if (ms < best) { best = ms; keep = P; }
   }
   if (rc) return rc;
