@@ -659,11 +659,7 @@ int autotune(int init_mode, int out_mode) {
                                 {100 << 10, 2}, {100 << 10, 3},
                                 {200 << 10, 3}, {160 << 10, 2},
                                 {200 << 10, 2},
-                                // padded plans (ternary cells); 34 KB
-                                // (four layers) and 42 KB (five) give a
-                                // six-axis first group
-                                {34 << 10, 0, 0, 1, 1},
-                                {42 << 10, 0, 0, 1, 1},
+                                // padded plans (ternary cells)
                                 {64 << 10, 1, 0, 1, 1},
                                 {100 << 10, 1, 0, 1, 1},
                                 {160 << 10, 1, 0, 1, 1},

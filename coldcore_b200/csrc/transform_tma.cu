@@ -885,7 +885,7 @@ const FirstEntry kFirst[] = {FE(9, 4), FE(10, 4), FE(11, 4), FE(12, 4),
 struct TernEntry { int src, kk, r1; FirstFn fn; };
 #define TF(KK, R1) {0, KK, R1, tern_first<KK, R1, 0>},                     \
                    {1, KK, R1, tern_first<KK, R1, 1>}
-const TernEntry kTern[] = {TF(6, 4), TF(7, 4), TF(6, 5), TF(7, 5)};
+const TernEntry kTern[] = {TF(7, 4), TF(7, 5)};
 #undef TF
 
 const TernEntry *find_tern(int src, int kk, int r1) {

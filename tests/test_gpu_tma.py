@@ -132,3 +132,38 @@ def test_byte_planes_after_the_first_group(monkeypatch, axes, R, mu):
             forms = b.plan_forms(im, om)
             assert forms[0] & BYTE8 and forms[1] & BYTE8, (im, forms)
         assert not (b.plan_forms(0, 2) & BYTE8).any()
+
+
+@pytest.mark.parametrize("axes,R,budget", [
+    ([3] * 14, 3, "34"), ([3] * 13, 4, "42"), ([3] * 12, 3, "34")])
+def test_six_axis_ternary_first_group(monkeypatch, axes, R, budget):
+    """The padded plan with a six-axis first group (a 729-word row padded
+    to 768, two rows a tile in the register kernel) and the later axes in
+    two streamed groups: recount, gain and loss equal the oracle's over
+    three codes, one a multiset."""
+    monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_TUNE", "0")
+    monkeypatch.setenv("CC_PIPE", "0")
+    monkeypatch.setenv("CC_SMEM_BUDGET_KB", budget)
+    size = int(np.prod(axes))
+    rng = np.random.default_rng(size % 983 + R)
+    o = OracleBackend(axes, R, mu=2)
+    with GpuBackend(axes, R, mu=2) as b:
+        for step in range(3):
+            if step == 2:
+                code = np.sort(rng.integers(0, size, size // 70))
+            else:
+                code = np.sort(rng.choice(size, size=size // (80 + 50 * step),
+                                          replace=False))
+            b.recount(code)
+            o.recount(code)
+            assert np.array_equal(b.read_cnt(), o.read_cnt()), step
+            b.gain_map()
+            o.gain_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            b.loss_map()
+            o.loss_map()
+            assert np.array_equal(b.map_all(), o.map), step
+        plan = b.plan(1, 1)
+        assert int(plan[0][1]) == 6, plan
+        assert (b.plan_forms(1, 1)[1:] & TMA).all()
