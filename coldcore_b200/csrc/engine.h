@@ -81,6 +81,8 @@ struct GroupArgs {
   // read).
   int in8, out8;
   long long off8;
+  // streamed group: axes per register round (0: RoundAxes, the default)
+  int tbm;
   int pack;               // two inner words per 32-bit lane (group_kernel)
   // first group of a binary Hamming cell: axis 0 is the word pair itself
   // (inner = 2), applied once as a swap-add inside each packed lane

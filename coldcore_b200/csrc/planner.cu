@@ -253,14 +253,21 @@ std::vector<GroupPlan> group_variants(const GroupPlan &p, int R1,
   }
   for (int lanes : {16, 32})
     for (int stages : {1, 2, 3, 4})
-      if (!tma_off && (stages < 4 || p.a.in8) &&
-          tma_group_ok(tma_variant(p, lanes, stages, 256).a, q, R1, lanes,
-                       stages))
+      for (int tbm : {0, 3}) {
+        if (tma_off || (stages == 4 && !p.a.in8)) continue;
+        GroupPlan t = p;
+        t.a.tbm = tbm;
+        if (!tma_group_ok(tma_variant(t, lanes, stages, 256).a, q, R1, lanes,
+                          stages))
+          continue;
+        // three-axis rounds have twice the blocks: 512 threads only
         for (int th : {256, 512}) {
-          GroupPlan v = tma_variant(p, lanes, stages, th);
+          if (tbm == 3 && th != 512) continue;
+          GroupPlan v = tma_variant(t, lanes, stages, th);
           v.grid = occupancy_grid(v);
           out.push_back(v);
         }
+      }
   // a padded plan's later groups run streamed only (the register kernels
   // address the canonical layout)
   if (p.a.pitch && p.a.tma == 1) return out;
@@ -404,9 +411,23 @@ bool pad_plan(std::vector<GroupPlan> &groups, const Geometry &g,
 // strided group as tensor loads (64-word rows first, three stages where
 // they fit).
 void stream_groups(std::vector<GroupPlan> &groups, int R1) {
+  // CC_TMA_BM=3: three-axis register rounds (512 threads) where they exist
+  const char *be = getenv("CC_TMA_BM");
+  const int tbm = be && atoi(be) == 3 ? 3 : 0;
   for (auto &p : groups) {
     if (p.kernel < 0 || p.a.nrounds <= 0) continue;
     bool done = false;
+    for (int lanes : {16, 32})
+      for (int stages : {3, 2}) {
+        if (done || !tbm) break;
+        GroupPlan t = p;
+        t.a.tbm = tbm;
+        GroupPlan v = tma_variant(t, lanes, stages, 512);
+        if (tma_group_ok(v.a, p.a.rq[0], R1, lanes, stages)) {
+          p = v;
+          done = true;
+        }
+      }
     for (int stages : {3, 2, 0})
       if (!done && tma_first_ok(p.a, R1, stages)) {
         p = tma_first_variant(p, stages, 256);

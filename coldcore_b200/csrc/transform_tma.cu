@@ -264,11 +264,13 @@ __device__ __forceinline__ void tma_round(uint32_t *st, const TmaArgs &a,
   }
 }
 
-// The rounds of a K-axis group: RoundAxes-sized rounds from axis 0 up, the
-// remainder last.
-template <int Q, int K, int R1, int L, int OUT, int A, bool IN8 = false>
+// The rounds of a K-axis group: RoundAxes-sized rounds from axis 0 up (or
+// BMX axes a round: smaller register blocks, twice the blocks a round, for
+// twice the threads), the remainder last.
+template <int Q, int K, int R1, int L, int OUT, int A, bool IN8 = false,
+          int BMX = 0>
 struct Rounds {
-  static constexpr int BM = RoundAxes<Q, R1>::v;
+  static constexpr int BM = BMX ? BMX : RoundAxes<Q, R1>::v;
   static constexpr int B = (K - A) < BM ? (K - A) : BM;
   static __device__ __forceinline__ void run(uint32_t *st, const TmaArgs &a,
                                              long long o, long long i0,
@@ -277,12 +279,12 @@ struct Rounds {
     tma_round<Q, K, R1, L, OUT, A, B, A == 0, A + B == K, IN8>(st, a, o, i0,
                                                               s8, racc);
     if (A + B < K) __syncthreads();
-    Rounds<Q, K, R1, L, OUT, (A + B < K ? A + B : K), IN8>::run(st, a, o, i0,
-                                                                s8, racc);
+    Rounds<Q, K, R1, L, OUT, (A + B < K ? A + B : K), IN8, BMX>::run(
+        st, a, o, i0, s8, racc);
   }
 };
-template <int Q, int K, int R1, int L, int OUT, bool IN8>
-struct Rounds<Q, K, R1, L, OUT, K, IN8> {
+template <int Q, int K, int R1, int L, int OUT, bool IN8, int BMX>
+struct Rounds<Q, K, R1, L, OUT, K, IN8, BMX> {
   static __device__ __forceinline__ void run(uint32_t *, const TmaArgs &,
                                              long long, long long,
                                              const uint16_t *,
@@ -302,7 +304,8 @@ struct Stage8 {
   static constexpr int bytes = (R1 * P<Q, K>::v * 2 * L + 1023) / 1024 * 1024;
 };
 
-template <int Q, int K, int R1, int L, int OUT, bool IN8 = false>
+template <int Q, int K, int R1, int L, int OUT, bool IN8 = false,
+          int BMX = 0>
 __global__ void __launch_bounds__(512)
 tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
   extern __shared__ __align__(128) uint8_t dyn[];
@@ -356,11 +359,11 @@ tma_group(const __grid_constant__ CUtensorMap map, const TmaArgs a) {
     const long long o = t / a.nchunk;
     const long long i0 = (t % a.nchunk) * (2 * L);
     if (IN8)
-      Rounds<Q, K, R1, L, OUT, 0, IN8>::run(
+      Rounds<Q, K, R1, L, OUT, 0, IN8, BMX>::run(
           work, a, o, i0,
           reinterpret_cast<const uint16_t *>(stage + (size_t)s * SB), racc);
     else
-      Rounds<Q, K, R1, L, OUT, 0>::run(
+      Rounds<Q, K, R1, L, OUT, 0, false, BMX>::run(
           reinterpret_cast<uint32_t *>(stage + (size_t)s * SB), a, o, i0,
           nullptr, racc);
     __syncthreads();                          // stage s is free again
@@ -836,7 +839,8 @@ tern_first(const TmaArgs a) {
 // ------------------------------------------------------------ dispatch
 typedef void (*TmaFn)(const CUtensorMap, const TmaArgs);
 
-struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; int in8 = 0; };
+struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; int in8 = 0;
+                  int bm = 0; };
 
 #define TE(Q, K, R1, L)                                                     \
   {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0>},                              \
@@ -844,6 +848,12 @@ struct TmaEntry { int q, k, r1, lanes, out; TmaFn fn; int in8 = 0; };
   {Q, K, R1, L, 2, tma_group<Q, K, R1, L, 2>}
 // ternary groups run only in the padded layout: OUT 0 (layers), 3 (map)
 // and 4 (cnt), the last two back to the canonical index
+// three axes a register round (8-word blocks): 512 blocks a round on
+// 16-lane rows of an 8-axis group, one for each of 512 threads
+#define TB(Q, K, R1, L, I8)                                                 \
+  {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0, I8, 3>, I8 ? 1 : 0, 3},        \
+  {Q, K, R1, L, 1, tma_group<Q, K, R1, L, 1, I8, 3>, I8 ? 1 : 0, 3},        \
+  {Q, K, R1, L, 2, tma_group<Q, K, R1, L, 2, I8, 3>, I8 ? 1 : 0, 3}
 // the launch after an 8-bit first group: its planes staged as bytes
 #define TE8(Q, K, R1, L)                                                    \
   {Q, K, R1, L, 0, tma_group<Q, K, R1, L, 0, true>, 1},                     \
@@ -862,10 +872,12 @@ const TmaEntry kTma[] = {
     TE3(3, 3, 5, 32), TE3(3, 4, 5, 32),
     TE8(2, 5, 4, 16), TE8(2, 6, 4, 16), TE8(2, 7, 4, 16), TE8(2, 8, 4, 16),
     TE8(2, 5, 4, 32), TE8(2, 6, 4, 32), TE8(2, 7, 4, 32),
+    TB(2, 8, 4, 16, false), TB(2, 8, 4, 16, true),
 };
 #undef TE
 #undef TE3
 #undef TE8
+#undef TB
 
 typedef void (*FirstFn)(const TmaArgs);
 // src 0: the cnt predicate (tma_first), 1: the sorted code (code_first)
@@ -908,10 +920,10 @@ int out_code(const GroupArgs &a) {
 }
 
 const TmaEntry *find_tma(int q, int k, int r1, int lanes, int out,
-                         int in8 = 0) {
+                         int in8 = 0, int bm = 0) {
   for (const auto &e : kTma)
     if (e.q == q && e.k == k && e.r1 == r1 && e.lanes == lanes &&
-        e.out == out && e.in8 == (in8 ? 1 : 0))
+        e.out == out && e.in8 == (in8 ? 1 : 0) && e.bm == bm)
       return &e;
   return nullptr;
 }
@@ -988,7 +1000,7 @@ bool tma_group_ok(const GroupArgs &a, int q, int r1, int lanes, int stages) {
   // the other CTA's rounds
   if (stages < 1 || stages > kTmaMaxStages || !encode_fn()) return false;
   const int out = out_code(a);
-  if (!find_tma(q, a.k, r1, lanes, out, a.in8)) return false;
+  if (!find_tma(q, a.k, r1, lanes, out, a.in8, a.tbm)) return false;
   if (a.prob != kHamming || !a.pack || !a.in16 || a.pair_axis ||
       a.src != kSrcLayers || a.R + 1 != r1)
     return false;
@@ -1148,7 +1160,7 @@ const TmaEntry *entry_of(const GroupPlan &p) {
   const GroupArgs &a = p.a;
   const int out = out_code(a);
   return find_tma(a.rq[0] ? a.rq[0] : a.qax[0], a.k, a.R + 1, a.W / 2, out,
-                  a.in8);
+                  a.in8, a.tbm);
 }
 
 // opt every streamed kernel in to the largest dynamic shared memory once

@@ -167,3 +167,35 @@ def test_six_axis_ternary_first_group(monkeypatch, axes, R, budget):
         plan = b.plan(1, 1)
         assert int(plan[0][1]) == 6, plan
         assert (b.plan_forms(1, 1)[1:] & TMA).all()
+
+
+@pytest.mark.parametrize("axes,R,mu,u8", [
+    ([2] * 20, 3, 1, "1"), ([2] * 23, 3, 2, "1"), ([2] * 23, 3, 1, "0")])
+def test_three_axis_rounds_in_the_eight_axis_group(monkeypatch, axes, R, mu,
+                                                   u8):
+    """The eight-axis streamed group with three-axis register rounds (8-word
+    blocks, 512 threads), over 16-bit or 8-bit planes: fields equal the
+    oracle's.  A 64 KB tile budget gives the 12 | 8 | ... grouping."""
+    monkeypatch.setenv("CC_TMA", "1")
+    monkeypatch.setenv("CC_TMA_BM", "3")
+    monkeypatch.setenv("CC_U8", u8)
+    monkeypatch.setenv("CC_TUNE", "0")
+    monkeypatch.setenv("CC_SMEM_BUDGET_KB", "64")
+    size = int(np.prod(axes))
+    rng = np.random.default_rng(size % 977 + mu)
+    o = OracleBackend(axes, R, mu=mu)
+    with GpuBackend(axes, R, mu=mu) as b:
+        for step in range(2):
+            code = np.sort(rng.choice(size, size=size // (170 + 30 * step),
+                                      replace=False))
+            b.recount(code)
+            o.recount(code)
+            assert np.array_equal(b.read_cnt(), o.read_cnt()), step
+            b.gain_map()
+            o.gain_map()
+            assert np.array_equal(b.map_all(), o.map), step
+            b.loss_map()
+            o.loss_map()
+            assert np.array_equal(b.map_all(), o.map), step
+        plan = b.plan(1, 1)
+        assert [int(r[1]) for r in plan[:2]] == [12, 8], plan
