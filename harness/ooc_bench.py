@@ -44,6 +44,17 @@ def link_rates(nbytes=1 << 30, reps=3):
     return out
 
 
+# the reference's K_10(10,5): (R+1) = 6 planes of 10^10 words at 2 bytes,
+# each crossing the link once a phase (two phases)
+K10_LINK_BYTES = 2 * 6 * 10 ** 10 * 2
+
+
+def link_projection_s(link_bytes, best_ms, target_bytes=K10_LINK_BYTES):
+    """Seconds that `target_bytes` of link traffic take at the rate a
+    transform achieved (`link_bytes` crossed in `best_ms` milliseconds)."""
+    return target_bytes / (link_bytes / (best_ms * 1e-3))
+
+
 def measure(axes=None, R=3, budget_gb=8.0, code_words=100000, reps=3):
     import torch
     from coldcore_b200.outofcore import ooc_plan, ooc_transform
@@ -66,9 +77,6 @@ def measure(axes=None, R=3, budget_gb=8.0, code_words=100000, reps=3):
     # phase 1 is device-to-host bound, phase 2 host-to-device bound
     half = plan["link_bytes"] / 2
     floor_ms = half / (rates["d2h"] * 1e6) + half / (rates["h2d"] * 1e6)
-    # the reference's K_10(10,5): (R+1) planes of 10^10 words at 2 bytes,
-    # each crossing the link once a phase
-    k10_link = 2 * 6 * 10 ** 10 * 2
     return {"cell": f"binary Hamming n={len(axes)}, R={R}", "words": X,
             "device_budget_GB": budget_gb, "code_words": int(len(code)),
             "plan": {k: plan[k] for k in ("split", "n_slabs", "n_cols",
@@ -81,7 +89,7 @@ def measure(axes=None, R=3, budget_gb=8.0, code_words=100000, reps=3):
             "frac_of_link_floor": round(floor_ms / best, 3),
             # the K_10(10,5) link bytes at this leg's achieved link rate
             "projection_K10_10_5_s": round(
-                k10_link / (plan["link_bytes"] / (best * 1e-3)), 2),
+                link_projection_s(plan["link_bytes"], best), 2),
             "reference_K10_10_5_s": "73-110 (GH200, C2C)"}
 
 

@@ -51,3 +51,12 @@ def test_traffic_covers_every_h2_grouping():
 def test_peak_fallback_or_measured():
     peak, kind = bench.peaks()
     assert kind in ("measured", "fallback") and peak > 1000
+
+
+def test_out_of_hbm_projection_is_in_seconds():
+    """17.18 GB crossed in 310.9 ms is 55.3 GB/s; the reference's K_10(10,5)
+    link traffic (240 GB) at that rate takes 4.34 s."""
+    from harness.ooc_bench import K10_LINK_BYTES, link_projection_s
+    assert K10_LINK_BYTES == 240 * 10 ** 9
+    s = link_projection_s(17179869184, 310.907)
+    assert abs(s - 4.343) < 0.01
