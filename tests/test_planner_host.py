@@ -209,3 +209,16 @@ def test_planner_fuzz():
         check_plan(plan, problem, axes, R, mode, budget, pipe, half)
         checked += 1
     assert checked > N_FUZZ * 0.8
+
+
+@pytest.mark.parametrize("axes,R", [([2] * 20, 2), ([3] * 12, 3),
+                                    ([2, 3] * 6, 2)])
+def test_lee_on_small_axes_plans_as_hamming(axes, R):
+    """A Lee cell whose axes are all of size 2 or 3 gets the Hamming cell's
+    launches (the distances are the same); one axis of size 4 keeps Lee."""
+    for mode in MODES:
+        assert plan_probe("lee", axes, R, *mode) == \
+            plan_probe("hamming", axes, R, *mode)
+    wider = [4] + axes[1:]
+    assert plan_probe("lee", wider, R, 1, 1) != \
+        plan_probe("hamming", wider, R, 1, 1)
